@@ -1,0 +1,361 @@
+/*
+ * rockfit_b200.h -- C ABI of the B200-native bonded-particle DEM engine.
+ *
+ * Every entry point returns an rf_status and takes plain pointers, sizes and
+ * scalars. Device pointers are CUDA device memory on the current device;
+ * host pointers are ordinary host memory. Streams are cudaStream_t passed as
+ * an opaque pointer (NULL = the legacy default stream).
+ *
+ * Two families of entry points:
+ *
+ *  md_*  -- drop-in replacements for the RockFit-DEM hot-path kernels and step
+ *           operations. They work IN PLACE on buffers laid out exactly as the
+ *           reference's md_data_types.h lays them out:
+ *             particle vectors R, V, W, F, M : float[3N], planes x | y | z at 0, N, 2N
+ *             cell arrays  CI[N], CIs[2N] (sorted cell keys, then particle ids),
+ *                          pnC[2*CN] (first particle of each cell, then count)
+ *             neighbour rows IL[N*K] (uint_fast32_t ids, empty = UINT_FAST32_MAX),
+ *                          ILtype[N*K] (uint8: 1 = bond, 0 = contact/none),
+ *                          _1d_iL[N*K] (1 / initial bond length),
+ *                          Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd : rf_float3[N*K]
+ *           Ids use uint_fast32_t, the reference's own id type, so a caller
+ *           built with the same compiler sees the same struct and array sizes.
+ *
+ *  rf_*  -- the fused engine: a whole quasi-static or explicit test run with its
+ *           own device-resident layout (slot-major bond rows, packed particle
+ *           vectors, device-side load reduction, CUDA-graph step loop).
+ *
+ * Units follow the reference (md_phys_constants.h:5-14): length mm, mass mg,
+ * time us; stress therefore in units of 1e9 Pa.
+ */
+#ifndef ROCKFIT_B200_H
+#define ROCKFIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rf_status {
+    RF_OK = 0,
+    RF_ERR_INVALID = 1,        /* bad argument (null pointer, zero size, inconsistent sizes) */
+    RF_ERR_CUDA = 2,           /* a CUDA runtime call failed; see rf_last_error_string() */
+    RF_ERR_ROW_OVERFLOW = 3,   /* a neighbour row needed more than K slots; rows left unmodified past K */
+    RF_ERR_CELL_RANGE = 4,     /* a particle or neighbour cell fell outside the cell grid */
+    RF_ERR_NOT_CONVERGED = 5,  /* FIRE reached its iteration limit */
+    RF_ERR_CAPACITY = 6,       /* an internal fixed-capacity table (candidate list) overflowed */
+    RF_ERR_NO_DEVICE = 7,      /* no usable CUDA device */
+    RF_ERR_STATE = 8           /* call made on an engine in the wrong state */
+} rf_status;
+
+typedef void* rf_stream;                       /* cudaStream_t */
+typedef struct rf_float3 { float x, y, z; } rf_float3;       /* layout of CUDA float3 */
+typedef struct rf_uint3 { unsigned int x, y, z; } rf_uint3;  /* layout of CUDA uint3 */
+typedef struct rf_double3 { double x, y, z; } rf_double3;    /* layout of CUDA double3 */
+
+#define RF_EMPTY_SLOT ((uint_fast32_t)UINT_FAST32_MAX)
+
+/* Text of the last error raised on this host thread (CUDA error name or argument check). */
+const char* rf_last_error_string(void);
+/* Library version, and sizeof(uint_fast32_t) the library was built with. */
+int rf_version(void);
+int rf_id_bytes(void);
+
+/* ------------------------------------------------------------------------ */
+/* Scalar state of a test: the numbers md_task_data carries                 */
+/* (md_data_types.h:78-323). rf_task_prepare() fills the derived fields with  */
+/* the reference's own formulas and type conversions; a caller migrating from */
+/* the reference may instead copy them over from its md_task_data.           */
+/* ------------------------------------------------------------------------ */
+
+typedef enum rf_test_kind { RF_TEST_UNIAXIAL = 0, RF_TEST_BRAZIL = 1 } rf_test_kind;
+
+typedef struct rf_potential {              /* potential_data, md_data_types.h:146-186 */
+    /* inputs */
+    double m_E, m_nu, m_Ec, m_Gc, m_ro, b_r, b_d, p_r, p_e, p_mu, p_mur, a_farcut;
+    /* derived by potential_data::CalculateParameters (md_data_types.h:153-185) */
+    double m_G, b_S, p_V, p_m, b_dd, p_1d_m, p_I, hm_E, hm_G, p_A, aa_farcut,
+           Trayleigh, Tsim, dt, D, a, _1d_a, aa, dt_d_m, dt_d_I;
+} rf_potential;
+
+typedef struct rf_sample {                 /* sample_data, md_data_types.h:78-122 */
+    rf_double3 A_real, B_real, size_real, center_real;
+    double Vext;
+    rf_float3 L, A, B, axis, center, size, sized2, hidenpoint, spacesize, spacesized2;
+    float R0, H0, Vgenmax;
+} rf_sample;
+
+typedef struct rf_cells {                  /* cell_data, md_data_types.h:24-56 */
+    rf_uint3 Nr;
+    uint64_t N;                            /* number of cells CN */
+    float a, _1d_a;
+    rf_float3 _1d_Nr;
+} rf_cells;
+
+typedef struct rf_compression {            /* compression_data, md_data_types.h:188-294 */
+    int32_t Loading, Fracture;
+    rf_float3 center, size, sized2;
+    rf_double3 size_d, center_d;
+    float R, RR, Hd2, C, mu, Area, _1d_Area;
+    double V, VLoad, Top, Bottom, TopR, BottomR, FractureStress, FractureStrain,
+           MinStress, ZeroStress, Stress, Strain, MaxStrain, Size0;
+} rf_compression;
+
+typedef struct rf_task {
+    rf_test_kind kind;
+    uint64_t N;                            /* particles (particle_data::N) */
+    uint32_t K;                            /* slots per particle (interaction_list_data::IonP) */
+    float acut, aacut;                     /* interaction_list_data::CalculateParameters */
+    rf_potential Po;
+    rf_sample S;
+    rf_cells C;
+    rf_compression Compress;
+    uint64_t bloks;                        /* additional_data::bloks = N/1024 + 1 */
+    double sz0;                            /* result_data::sz0 = Compress.size.z at the start (md_results.cu:21) */
+} rf_task;
+
+/*
+ * Fill the derived fields of *t from its inputs, following
+ *   potential_data::CalculateParameters   md_data_types.h:153-185
+ *   sample_data::SetSpaceSizeSi / SetLSi / CalculateParameters   md_data_types.h:86-121
+ *   cell_data::CalculateParameters        md_data_types.h:42-55
+ *   interaction_list_data::CalculateParameters md_data_types.h:137-143
+ *   compression_data::CalculateUParameters / CalculateBParameters md_data_types.h:196-271
+ * Inputs: t->kind, t->N, t->K, t->Po (inputs), space_size_si / specimen_size_si
+ * (metres, as SetSpaceSizeSi / SetLSi take them), v_load, min_stress, max_strain.
+ * cell_a is C.a (the reference sets it to 2 * a_farcut, mp_determineconjgradient.cu:32).
+ */
+rf_status rf_task_prepare(rf_task* t, const double space_size_si[3], const double specimen_size_si[3],
+                          double cell_a, double v_load, double min_stress, double max_strain);
+
+/* compression_data::CompressU / CompressB (md_data_types.h:223-293): advance the platen one step. */
+rf_status md_CompressU(rf_task* t, double pressure);
+rf_status md_CompressB(rf_task* t, double pressure);
+
+/*
+ * SumForcesULoading / SumForcesBLoading (md_results.cu:34-117): reduce the platen
+ * partial sums FL[2*nblocks] (host copy), update Stress, Loading, FractureStress,
+ * FractureStrain, Fracture. sz0 is R.sz0, Compress.size.z when the run started
+ * (md_results.cu:21). curve (may be NULL) receives (strain, stress_bottom,
+ * stress_top) when step % dNsave == 0, as R.h_sFL does; *nsaved is advanced.
+ */
+rf_status md_SumForcesULoading(rf_task* t, const float* h_FL, uint64_t nblocks, uint64_t step,
+                               uint64_t dNsave, double sz0, double* curve, uint64_t* nsaved);
+
+/* ------------------------------------------------------------------------ */
+/* md_* device step operations (reference layout, in place, on `stream`).    */
+/* ------------------------------------------------------------------------ */
+
+/* d_CalculateCellIndex, md_calculate_cell.cu:28-53 */
+rf_status md_CalculateCellIndex(const float* R, uint_fast32_t N, uint_fast32_t* CI, float _1d_a,
+                                rf_uint3 cN, rf_stream stream);
+
+/* Scratch bytes md_CellDistribution needs for N particles and CN cells. */
+size_t md_CellDistributionScratchBytes(uint_fast32_t N, uint_fast32_t CN);
+
+/*
+ * CellDistribution, md_cell_distribution.cu:52-101: cell index per particle,
+ * stable sort of (cell, id) into CIs, and per-cell (start, count) into pnC
+ * (cells without particles get 0, 0). The sort here is a counting sort; its
+ * output equals the reference's stable cub radix sort of (CI, 0..N-1).
+ * scratch: device buffer of md_CellDistributionScratchBytes(N, CN) bytes.
+ */
+rf_status md_CellDistribution(const float* R, uint_fast32_t N, uint_fast32_t* CI, uint_fast32_t* CIs,
+                              uint_fast32_t* pnC, uint_fast32_t CN, float _1d_a, rf_uint3 cN,
+                              void* scratch, size_t scratch_bytes, rf_stream stream);
+
+/*
+ * InteractionListConstruct + d_ConstructInteractionList,
+ * md_interaction_list_construction.cu:163-168, md_interaction_list_construct.cu:13-98:
+ * clear IL to empty and fill each row from the 8 octant cells in the reference's
+ * visiting order. A row that would exceed K slots is cut at K and the call returns
+ * RF_ERR_ROW_OVERFLOW (the reference writes past the row).
+ */
+rf_status md_InteractionListConstruct(const float* R, uint_fast32_t N, const uint_fast32_t* CIs,
+                                      const uint_fast32_t* pnC, uint_fast32_t* IL, uint_fast32_t K,
+                                      float a, float _1d_a, float aacut, rf_uint3 cN, uint_fast32_t CN,
+                                      rf_stream stream);
+
+/*
+ * InteractionListReConstructBPM + d_ReConstructInteractionListbpm,
+ * md_interaction_list_construction.cu:176-180, md_interaction_list_reconstructbpm.cu:13-46,80-139:
+ * add every neighbour within sqrt(aacut) not yet in the row, at the first free slot,
+ * as type 0. A full row returns RF_ERR_ROW_OVERFLOW and is left unchanged.
+ */
+rf_status md_InteractionListReConstructBPM(const float* R, uint_fast32_t N, const uint_fast32_t* CIs,
+                                           const uint_fast32_t* pnC, uint_fast32_t* IL, uint8_t* ILtype,
+                                           uint_fast32_t K, float a, float _1d_a, float aacut,
+                                           rf_uint3 cN, uint_fast32_t CN, rf_stream stream);
+
+/* d_DeleteFarLinks, md_interaction_list_reconstructbpm.cu:141-186 */
+rf_status md_DeleteFarLinks(const float* R, uint_fast32_t N, uint_fast32_t* IL, uint8_t* ILtype,
+                            float* _1d_iL, rf_float3* Rij, rf_float3* Oijt, rf_float3* Fijn,
+                            rf_float3* Fijt, rf_float3* Mijn, rf_float3* Mijt, rf_float3* Mijadd,
+                            uint_fast32_t K, float aacut, rf_stream stream);
+
+/* d_ConstructBoundInteractions, md_boundinteractions_construct.cu:35-106 */
+rf_status md_ConstructBoundInteractions(const float* R, const float* V, const float* W,
+                                        const uint_fast32_t* IL, uint8_t* ILtype, float* _1d_iL,
+                                        rf_float3* Rij, rf_float3* Oijt, rf_float3* Fijn, rf_float3* Fijt,
+                                        rf_float3* Mijn, rf_float3* Mijt, rf_float3* Mijadd,
+                                        uint_fast32_t N, uint_fast32_t K, float aa_create, float b_r,
+                                        rf_stream stream);
+
+/* d_CalculateForcesDEM_22 (bond force, moment and break check), md_calculateforcesdem3.cu:424-483 */
+rf_status md_CalculateForcesDEM_22(const float* R, const float* V, const float* W,
+                                   const uint_fast32_t* IL, uint8_t* ILtype, const float* _1d_iL,
+                                   rf_float3* Rij, rf_float3* Oijt, rf_float3* Mijn, rf_float3* Mijt,
+                                   float* F, float* M, uint_fast32_t N, uint_fast32_t K, float dt,
+                                   float m_E, float m_G, float b_r, float m_Gcritn, float m_Gcritt,
+                                   rf_stream stream);
+
+/* d_CalculateForcesDEM_21 (Hertz-Mindlin contacts), md_calculateforcesdem3.cu:338-422 */
+rf_status md_CalculateForcesDEM_21(const float* R, const float* V, const float* W,
+                                   const uint_fast32_t* IL, uint8_t* ILtype, const float* _1d_iL,
+                                   rf_float3* Rij, rf_float3* Oijt, float* F, float* M,
+                                   uint_fast32_t N, uint_fast32_t K, float dt, float m_E, float m_G,
+                                   float p_A, float m_mu, float m_muroll, float mP, float rP,
+                                   rf_stream stream);
+
+/* d_CalculateIncrementsDEM, md_calculateincrementsdem.cu:19-49 */
+rf_status md_CalculateIncrementsDEM(const float* F, float* V, float* R, const float* M, float* W,
+                                    uint_fast32_t N, float _1d_Mass_m_dt, float dt, float _1d_I_m_dt,
+                                    rf_stream stream);
+
+/*
+ * d_braziltest_simple2, md_braziltest_simple2.cu:19-151. Platen contact, friction and
+ * clamp; the reaction sums go to FL as the reference lays them out: FL[0..nblocks)
+ * bottom partials then FL[nblocks..2*nblocks) top partials, so the reference's
+ * SumForcesULoading reads the same totals. Here the totals sit in FL[0] and
+ * FL[nblocks]; the other partials are 0.
+ */
+rf_status md_braziltest_simple2(float* R, float* V, float* F, float* FL, uint_fast32_t N,
+                                rf_float3 c, float RR, float Yt, float Yb, float Ytr, float Ybr,
+                                float vt, float Zcut, uint64_t nblocks, rf_stream stream);
+
+/* d_UniaxialCompression3_simple, md_uniaxialcompression3_simple.cu:19-136 (FL as above) */
+rf_status md_UniaxialCompression3_simple(float* R, float* V, float* F, float* FL, uint_fast32_t N,
+                                         rf_float3 c, float RR, float Zt, float Zb, float Ztr, float Zbr,
+                                         float vt, float Zcut, uint64_t nblocks, rf_stream stream);
+
+/* d_ParallelepipedCutRestriction, md_parallelepipedrestriction.cu:73-159 */
+rf_status md_ParallelepipedCutRestriction(float* R, float* V, float* F, uint_fast32_t N,
+                                          rf_float3 center, rf_float3 sized2, rf_float3 hp,
+                                          rf_stream stream);
+
+/* FIRE pieces, md_firerelaxation.cu:18-70 and :372-490 */
+rf_status md_CalculateIncrementsFIRE(const float* F, float* V, float* R, uint_fast32_t N,
+                                     float _1d_Mass_m_dt, float dt, float F_alpha, rf_stream stream);
+rf_status md_CalculateDecrementsHalfStepFIRE(const float* V, float* R, uint_fast32_t N, float dt_d2,
+                                             rf_stream stream);
+/* d_FdotVEntire: P = sum_i F_i . V_i as nblocks per-block partial sums (device doubles,
+   FdotV[0..nblocks)); the caller adds them in order, as CalculateGPUStepsContractRelaxFIRE
+   adds the reference's partials (md_firerelaxation.cu:239-245). */
+rf_status md_FdotVEntire(const float* V, const float* F, double* FdotV, uint64_t nblocks, uint_fast32_t N,
+                         rf_stream stream);
+
+/* ------------------------------------------------------------------------ */
+/* Whole-test drivers (h_CalculationBrazilTest / h_CalculationUniaxialCompression). */
+/* ------------------------------------------------------------------------ */
+
+typedef struct rf_run_result {
+    uint64_t steps;                /* explicit steps taken */
+    double FractureStress, FractureStrain, Stress, Strain;
+    int32_t Fracture;
+    uint64_t broken_bonds;         /* directed bond slots that broke */
+    uint64_t bonds_initial;        /* directed bond slots after bond construction */
+    rf_status error;               /* first device-side error seen (RF_OK if none) */
+} rf_run_result;
+
+/*
+ * h_CalculationBrazilTest / h_CalculationUniaxialCompression
+ * (md_calculationbraziltest.cu:113-214, md_calculationuniaxialcompression.cu:113-216):
+ * copy h_R in, build cells, rows and bonds, and step until Strain >= MaxStrain,
+ * fracture, or max_steps (0 = no limit). t->Compress is updated as the reference
+ * updates mdTD.Compress. curve (may be NULL) receives up to curve_cap records of
+ * (strain, stress_bottom, stress_top) per step. h_R_out (may be NULL) receives the
+ * final positions, float[3N] planar.
+ */
+rf_status md_CalculationBrazilTest(rf_task* t, const float* h_R, uint64_t max_steps,
+                                   double* curve, uint64_t curve_cap, float* h_R_out,
+                                   rf_run_result* result);
+rf_status md_CalculationUniaxialCompression(rf_task* t, const float* h_R, uint64_t max_steps,
+                                            double* curve, uint64_t curve_cap, float* h_R_out,
+                                            rf_run_result* result);
+
+/* ------------------------------------------------------------------------ */
+/* Fused engine                                                              */
+/* ------------------------------------------------------------------------ */
+
+typedef struct rf_engine rf_engine;
+
+/*
+ * Create an engine for task *t (prepared) on the current device, copy the
+ * particle positions h_R (float[3N] planar, host) in, build rows and bonds
+ * (md_calculationbraziltest.cu:132-144). V, W start at zero.
+ */
+rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out);
+rf_status rf_engine_destroy(rf_engine* e);
+
+/* Advance nsteps explicit steps (stops early, on device, at fracture / max strain). */
+rf_status rf_engine_step(rf_engine* e, uint64_t nsteps);
+/* Same, with positions uploaded from host first and results read back after:
+   the end-to-end path through host buffers. */
+rf_status rf_engine_step_host(rf_engine* e, const float* h_R_in, uint64_t nsteps, float* h_R_out);
+/* Block until queued work finishes; copy the scalar test state out. */
+rf_status rf_engine_sync(rf_engine* e, rf_task* t_out, rf_run_result* r_out);
+
+/*
+ * Export the state in the reference layout (host buffers, any may be NULL):
+ * R, V, W : float[3N]; IL : uint_fast32_t[N*K]; ILtype : uint8[N*K];
+ * _1d_iL : float[N*K]; Rij, Oijt, Mijn, Mijt : rf_float3[N*K].
+ */
+rf_status rf_engine_export(rf_engine* e, float* R, float* V, float* W, uint_fast32_t* IL,
+                           uint8_t* ILtype, float* _1d_iL, rf_float3* Rij, rf_float3* Oijt,
+                           rf_float3* Mijn, rf_float3* Mijt);
+/* Import full state (reference layout, host buffers, all required) -- resume. */
+rf_status rf_engine_import(rf_engine* e, const float* R, const float* V, const float* W,
+                           const uint_fast32_t* IL, const uint8_t* ILtype, const float* _1d_iL,
+                           const rf_float3* Rij, const rf_float3* Oijt, const rf_float3* Mijn,
+                           const rf_float3* Mijt);
+
+/* Copy the load curve recorded so far: up to cap records of (strain, stress_bottom, stress_top). */
+rf_status rf_engine_curve(rf_engine* e, double* curve, uint64_t cap, uint64_t* n);
+
+/* Engine counters: [0] steps, [1] candidate-list rebuilds, [2] live bond slots,
+   [3] live contact slots, [4] occupied slots; all as of the last sync. */
+rf_status rf_engine_counters(rf_engine* e, uint64_t* out, int n);
+
+/* Kernel launches the engine issues per explicit step when no rebuild runs. */
+int rf_engine_launches_per_step(void);
+/* The stream the engine launches on (cudaStream_t), for callers that time or order work. */
+rf_stream rf_engine_stream(rf_engine* e);
+/* Whether the device-driven CUDA graph loop is in use (1) or plain stream launches (0). */
+int rf_engine_uses_graph(rf_engine* e);
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic specimens                                                */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Deterministic seeded specimen: particles of radius p_r on a jittered cubic
+ * lattice of spacing 2*p_r*(1+gap_frac), cut to a cylinder (axis z, diameter d,
+ * height h) centred at center (mm). jitter is the uniform half-width of the
+ * per-coordinate jitter, in units of p_r. The count goes to *n; with R == NULL
+ * nothing else is written, otherwise cap must be >= *n and R receives the
+ * positions planar (x | y | z at 0, n, 2n). Order is lattice order (x fastest).
+ */
+rf_status rf_specimen_lattice_cylinder(uint64_t seed, double p_r, double gap_frac, double jitter,
+                                       double d, double h, const double center[3],
+                                       float* R, uint64_t cap, uint64_t* n);
+/* Same, cut to a Brazilian disc: axis z, diameter d, thickness h. */
+rf_status rf_specimen_lattice_disc(uint64_t seed, double p_r, double gap_frac, double jitter,
+                                   double d, double h, const double center[3],
+                                   float* R, uint64_t cap, uint64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ROCKFIT_B200_H */

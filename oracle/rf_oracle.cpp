@@ -1,0 +1,957 @@
+// ORACLE -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of the RockFit-DEM hot path (one thread per particle, serial,
+// in the reference's own order of operations). It is the checker for the CUDA
+// engine: only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg
+// may load it. Nothing in the product links or calls it.
+//
+// Built with -O2 -ffp-contract=off (no FMA contraction, SSE arithmetic), so every
+// float operation below is one IEEE-754 round-to-nearest operation in source order.
+// Each function is instantiated for T = float (the reference's precision; the
+// engine's reference mode must match it bit for bit) and T = double (the FP64
+// oracle used to report error). Reference citations are file:line in
+// MSMS-LAB/RockFit-DEM.
+//
+// CUDA intrinsics the reference calls are restated as:
+//   __fmul_rn(a,b)  -> a*b                      (IEEE product)
+//   __frcp_rn(x)    -> 1/x                      (IEEE quotient)
+//   __fsqrt_rn(x)   -> sqrt(x)                  (IEEE square root)
+//   __frsqrt_rn(x)  -> correctly rounded 1/sqrt(x), computed in double and
+//                      rounded once (exhaustively checked against the device)
+//   norm3df(x,y,z)  -> sqrt(x*x + y*y + z*z)    (the engine uses the same formula;
+//                      the reference's library norm may differ in the last bit)
+// Quirks of the reference that are reproduced are marked "QUIRK".
+// Where the reference reads or writes out of bounds, the oracle stops at the
+// bound and reports a status instead (marked "BOUND").
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdio>
+#include <vector>
+#include <algorithm>
+#include <limits>
+
+#include "../include/rockfit_b200.h"
+
+namespace rfo {
+
+typedef uint64_t id_t;                        // uint_fast32_t on Linux glibc
+static const id_t EMPTY = std::numeric_limits<id_t>::max();
+
+enum { ST_OK = 0, ST_ROW_OVERFLOW = 3, ST_CELL_RANGE = 4 };
+
+template <class T> struct V3 { T x, y, z; };
+
+// float -> unsigned conversion as the device does it (saturating, NaN -> 0).
+static inline uint32_t f2u_sat(double v) {
+    if (!(v > 0.0)) return 0u;
+    if (v >= 4294967295.0) return 0xFFFFFFFFu;
+    return (uint32_t)v;
+}
+
+template <class T> static inline T rsqrt_rn(T x);
+template <> inline float rsqrt_rn<float>(float x) { return (float)(1.0 / std::sqrt((double)x)); }
+template <> inline double rsqrt_rn<double>(double x) { return 1.0 / std::sqrt(x); }
+
+template <class T> static inline T floor_t(T x);
+template <> inline float floor_t<float>(float x) { return std::floor(x); }
+template <> inline double floor_t<double>(double x) { return std::floor(x); }
+
+// ---------------------------------------------------------------------------
+// Cells: d_CalculateCellIndex (md_calculate_cell.cu:28-53)
+// ---------------------------------------------------------------------------
+template <class T>
+static inline uint64_t cell_of(const T* R, uint64_t N, uint64_t i, T inv_a, const rf_uint3& cN,
+                               uint32_t* ix, uint32_t* iy, uint32_t* iz) {
+    uint32_t x = f2u_sat((double)floor_t<T>(R[i] * inv_a));
+    uint32_t y = f2u_sat((double)floor_t<T>(R[i + N] * inv_a));
+    uint32_t z = f2u_sat((double)floor_t<T>(R[i + 2 * N] * inv_a));
+    if (ix) { *ix = x; *iy = y; *iz = z; }
+    // iindx = indx.x + indx.y*cN.x + indx.z*cN.y*cN.x, in unsigned int then widened
+    // to uint_fast32_t (md_calculate_cell.cu:47).
+    uint32_t c = x + y * cN.x + z * cN.y * cN.x;
+    return (uint64_t)c;
+}
+
+template <class T>
+int cell_index(const T* R, uint64_t N, id_t* CI, T inv_a, rf_uint3 cN) {
+    int st = ST_OK;
+    for (uint64_t i = 0; i < N; ++i) {
+        uint32_t x, y, z;
+        CI[i] = cell_of(R, N, i, inv_a, cN, &x, &y, &z);
+        if (x > cN.x - 1 || y > cN.y - 1 || z > cN.z - 1) st = ST_CELL_RANGE;  // pre_debugtest check :42-46
+    }
+    return st;
+}
+
+// CellDistribution (md_cell_distribution.cu:52-101): stable sort of (CI, 0..N-1)
+// (cub radix sort is stable; values are the identity filled by d_FillIndex), then
+// d_DetermineCellPointer (md_calculate_cell.cu:55-80) after a zero fill of pnC.
+template <class T>
+int cell_distribution(const T* R, uint64_t N, id_t* CI, id_t* CIs, id_t* pnC, uint64_t CN,
+                      T inv_a, rf_uint3 cN) {
+    int st = cell_index(R, N, CI, inv_a, cN);
+    std::vector<id_t> ids(N);
+    for (uint64_t i = 0; i < N; ++i) ids[i] = i;
+    std::stable_sort(ids.begin(), ids.end(), [&](id_t a, id_t b) { return CI[a] < CI[b]; });
+    for (uint64_t i = 0; i < N; ++i) { CIs[i] = CI[ids[i]]; CIs[N + i] = ids[i]; }
+    std::memset(pnC, 0, sizeof(id_t) * 2 * CN);
+    for (uint64_t i = 0; i < N; ++i) {
+        id_t c = CIs[i];
+        if (i == 0 || CIs[i - 1] != c) {
+            if (c >= CN) { st = ST_CELL_RANGE; continue; }          // BOUND
+            pnC[c] = i;
+            uint64_t n = 1;
+            // QUIRK (md_calculate_cell.cu:72): the run scan does not stop at N and
+            // continues into the id half of CIs; ids are distinct, so at most one
+            // extra match (CIs[N] == c) can extend the last run.
+            while (i + n < 2 * N && CIs[i + n] == c) ++n;
+            pnC[c + CN] = n;
+        }
+    }
+    return st;
+}
+
+// The 8 octant cells in the order the reference visits them
+// (md_interaction_list_construct.cu:59-85, md_interaction_list_reconstructbpm.cu:107-134).
+template <class T>
+static inline void octant_cells(const T* R, uint64_t N, uint64_t i, T a, T inv_a, const rf_uint3& cN,
+                                int64_t cells[8]) {
+    uint32_t ix, iy, iz;
+    uint64_t c = cell_of(R, N, i, inv_a, cN, &ix, &iy, &iz);
+    // indxx = copysignf(1, R - __fmul_rn(indx + 0.5f, a)); indx + 0.5f is float math
+    T hx = (T)((T)ix + (T)0.5f), hy = (T)((T)iy + (T)0.5f), hz = (T)((T)iz + (T)0.5f);
+    int sx = std::signbit(R[i] - hx * a) ? -1 : 1;
+    int sy = std::signbit(R[i + N] - hy * a) ? -1 : 1;
+    int sz = std::signbit(R[i + 2 * N] - hz * a) ? -1 : 1;
+    int64_t ox = sx, oy = (int64_t)sy * cN.x, oz = (int64_t)sz * cN.y * cN.x;
+    int64_t b = (int64_t)c;
+    cells[0] = b;
+    cells[1] = b + ox;
+    cells[2] = b + oy;
+    cells[3] = b + oz;
+    cells[4] = b + ox + oy;
+    cells[5] = b + ox + oz;
+    cells[6] = b + oy + oz;
+    cells[7] = b + ox + oy + oz;
+}
+
+template <class T>
+static inline T dist2_rn(const T* R, uint64_t N, uint64_t i, uint64_t j) {
+    // rr = __fmul_rn(dx,dx) + __fmul_rn(dy,dy) + __fmul_rn(dz,dz)
+    T dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
+    return dx * dx + dy * dy + dz * dz;
+}
+
+// InteractionListConstruct: memset IL to 0xFF, then d_ConstructInteractionList
+// (md_interaction_list_construction.cu:163-168, md_interaction_list_construct.cu:13-98).
+template <class T>
+int construct_list(const T* R, uint64_t N, const id_t* CIs, const id_t* pnC, id_t* IL, uint64_t K,
+                   T a, T inv_a, T aacut, rf_uint3 cN, uint64_t CN) {
+    int st = ST_OK;
+    for (uint64_t k = 0; k < N * K; ++k) IL[k] = EMPTY;
+    for (uint64_t i = 0; i < N; ++i) {
+        int64_t cells[8];
+        octant_cells(R, N, i, a, inv_a, cN, cells);
+        uint64_t n = 0;
+        for (int c = 0; c < 8; ++c) {
+            if (cells[c] < 0 || (uint64_t)cells[c] >= CN) { st = ST_CELL_RANGE; continue; }  // BOUND
+            uint64_t start = pnC[cells[c]], cnt = pnC[cells[c] + CN];
+            for (uint64_t m = 0; m < cnt; ++m) {
+                if (start + m >= N) break;                                          // BOUND
+                id_t j = CIs[start + m + N];
+                if (j >= N) continue;                                               // BOUND
+                T rr = dist2_rn(R, N, i, j);
+                if (rr < aacut && j != i) {                                         // :26
+                    if (n < K) IL[i * K + n] = j; else st = ST_ROW_OVERFLOW;        // BOUND (:89-92)
+                    ++n;
+                }
+            }
+        }
+    }
+    return st;
+}
+
+// d_ReConstructInteractionListbpm + addnewlinkbpm (md_interaction_list_reconstructbpm.cu:13-46,80-139)
+template <class T>
+int reconstruct_bpm(const T* R, uint64_t N, const id_t* CIs, const id_t* pnC, id_t* IL, uint8_t* ILtype,
+                    uint64_t K, T a, T inv_a, T aacut, rf_uint3 cN, uint64_t CN) {
+    int st = ST_OK;
+    for (uint64_t i = 0; i < N; ++i) {
+        int64_t cells[8];
+        octant_cells(R, N, i, a, inv_a, cN, cells);
+        for (int c = 0; c < 8; ++c) {
+            if (cells[c] < 0 || (uint64_t)cells[c] >= CN) { st = ST_CELL_RANGE; continue; }  // BOUND
+            uint64_t start = pnC[cells[c]], cnt = pnC[cells[c] + CN];
+            for (uint64_t m = 0; m < cnt; ++m) {
+                if (start + m >= N) break;                                          // BOUND
+                id_t j = CIs[start + m + N];
+                if (j >= N) continue;                                               // BOUND
+                T rr = dist2_rn(R, N, i, j);
+                if (rr < aacut && rr > 1e-10) {                                     // :28
+                    // QUIRK (:30-36): kdxfree == 0 doubles as "no free slot found", so for
+                    // particle 0 a free slot 0 is passed over while a later free slot exists.
+                    uint64_t kdxfree = 0;
+                    uint64_t s;
+                    for (s = 0; s < K; ++s) {
+                        id_t kj = IL[i * K + s];
+                        if (kdxfree == 0 && kj == EMPTY) kdxfree = i * K + s;
+                        if (kj == j) break;
+                    }
+                    if (s == K) {
+                        // BOUND: with no free slot the reference writes IL[0]; here the row
+                        // is left unchanged and overflow is reported.
+                        bool has_free = false;
+                        for (uint64_t q = 0; q < K; ++q) if (IL[i * K + q] == EMPTY) has_free = true;
+                        if (!has_free) { st = ST_ROW_OVERFLOW; continue; }
+                        IL[kdxfree] = j;
+                        ILtype[kdxfree] = 0;
+                    }
+                }
+            }
+        }
+    }
+    return st;
+}
+
+// d_DeleteFarLinks (md_interaction_list_reconstructbpm.cu:141-186).
+// QUIRK: the reference's "_1d_iL = 0;" clears its own pointer, not the element, so
+// 1/L0 of a deleted slot is left as it was.
+template <class T>
+void delete_far_links(const T* R, uint64_t N, id_t* IL, uint8_t* ILtype, V3<T>* Rij, V3<T>* Oijt,
+                      V3<T>* Mijn, V3<T>* Mijt, uint64_t K, T aacut) {
+    for (uint64_t i = 0; i < N; ++i)
+        for (uint64_t s = 0; s < K; ++s) {
+            uint64_t k = i * K + s;
+            id_t j = IL[k];
+            if (j == EMPTY) continue;
+            if (j >= N) continue;                                                   // BOUND
+            T rr = dist2_rn(R, N, i, j);
+            if (rr > aacut || rr < 1e-10) {
+                IL[k] = EMPTY;
+                ILtype[k] = 0;
+                Rij[k] = {0, 0, 0};
+                Oijt[k] = {0, 0, 0};
+                Mijn[k] = {0, 0, 0};
+                Mijt[k] = {0, 0, 0};
+                // Fijn, Fijt, Mijadd are zeroed too; the live path never makes them non-zero.
+            }
+        }
+}
+
+// d_ConstructBoundInteractions (md_boundinteractions_construct.cu:35-106).
+// rm2 = r.x*r.x + r.y*r.y + r.z*r.z is restated with the FMA contraction nvcc applies
+// to that expression in the reference build: fma(z, z, fma(x, x, y*y)).
+template <class T>
+static inline T rm2_bond(T x, T y, T z) { return std::fma(z, z, std::fma(x, x, y * y)); }
+
+template <class T>
+void construct_bonds(const T* R, uint64_t N, const id_t* IL, uint8_t* ILtype, T* iL, V3<T>* Rij,
+                     V3<T>* Oijt, V3<T>* Mijn, V3<T>* Mijt, uint64_t K, T aa_create) {
+    for (uint64_t i = 0; i < N; ++i)
+        for (uint64_t s = 0; s < K; ++s) {
+            uint64_t k = i * K + s;
+            id_t j = IL[k];
+            if (j == EMPTY) continue;
+            if (j >= N) continue;                                                   // BOUND
+            T rx = R[j] - R[i], ry = R[j + N] - R[i + N], rz = R[j + 2 * N] - R[i + 2 * N];
+            T rm2 = rm2_bond(rx, ry, rz);
+            if (rm2 < aa_create && rm2 > 1e-18) {
+                iL[k] = rsqrt_rn(rm2);
+                ILtype[k] = 1;
+            } else {
+                ILtype[k] = 0;
+            }
+            Rij[k] = {0, 0, 0};   // QUIRK Q2: the unit bond direction is overwritten with 0*r (:69-80)
+            Oijt[k] = {0, 0, 0};
+            Mijn[k] = {0, 0, 0};
+            Mijt[k] = {0, 0, 0};
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Forces (md_calculateforcesdem3.cu)
+// ---------------------------------------------------------------------------
+template <class T> struct FP {
+    // kernel scalar arguments as the drivers pass them (floats for T = float)
+    T dt, m_E, m_G, b_r, m_Gcritn, m_Gcritt;          // _22
+    T hm_E, hm_G, p_A, m_mu, m_muroll, mP, rP;        // _21
+};
+
+template <class T> static inline T pi_t() { return (T)3.14159265358979f; }   // MCf_pi
+template <class T> static inline T two_thirds_t() { return (T)0.6666666667f; }  // MCf_2d3
+
+template <class T>
+static inline T norm3(T x, T y, T z) { return std::sqrt(x * x + y * y + z * z); }
+
+// d_CalculateForcesDEM_22 (:424-483) with dd_Calculate_rijm_nij_2 (:38-52),
+// dd_Calculate_fijn_bpm_2 (:91-103), dd_Calculate_M123_bpm_2 (:54-89),
+// dd_Calculate_mijn_bpm_2 (:105-129), dd_Calculate_mijt_bpm_2 (:131-152),
+// dd_Calculate_fijt_mijunsym_bpm_2 (:154-197), dd_CheckBreakConditionDEM_2 (:20-36).
+// F and M are accumulated (+=), as the kernel does after the driver's memset.
+template <class T>
+void forces_22(const T* R, const T* V, const T* W, const id_t* IL, uint8_t* ILtype, const T* iL,
+               V3<T>* Rij, V3<T>* Oijt, V3<T>* Mijn, V3<T>* Mijt, T* F, T* M, uint64_t N, uint64_t K,
+               const FP<T>& p, uint8_t* broke /* may be null: 1 where a bond broke */) {
+    const T PI = pi_t<T>();
+    for (uint64_t i = 0; i < N; ++i) {
+        T fsx = 0, fsy = 0, fsz = 0, msx = 0, msy = 0, msz = 0;
+        T Sc = 0, Mc = 0;
+        for (uint64_t s = 0; s < K; ++s) {
+            uint64_t k = i * K + s;
+            id_t j = IL[k];
+            if (!(j != EMPTY && ILtype[k] == 1)) continue;
+            // rijm, nij
+            T rx = R[j] - R[i], ry = R[j + N] - R[i + N], rz = R[j + 2 * N] - R[i + 2 * N];
+            T rijm = norm3(rx, ry, rz);
+            T inv_rm = (T)1 / rijm;
+            T nx = rx * inv_rm, ny = ry * inv_rm, nz = rz * inv_rm;
+            // normal force
+            T il = iL[k];
+            T cef = p.m_E * (rijm - (T)1 / il) * il;
+            Sc = cef;
+            cef *= p.b_r * p.b_r * PI;
+            fsx += nx * cef; fsy += ny * cef; fsz += nz * cef;
+            // rotation-increment matrix
+            V3<T> rp = Rij[k];
+            T tx = rp.y * nz - rp.z * ny;
+            T ty = rp.z * nx - rp.x * nz;
+            T tz = rp.x * ny - rp.y * nx;
+            T wsx = W[j] + W[i], wsy = W[j + N] + W[i + N], wsz = W[j + 2 * N] + W[i + 2 * N];
+            T cphi = (wsx * nx + wsy * ny + wsz * nz) * p.dt * (T)0.5f;
+            T phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
+            Rij[k] = {nx, ny, nz};
+            T M1x = (T)1.0f + tz * phz + ty * phy;
+            T M1y = phz - tz - ty * phx;
+            T M1z = -phy - tz * phx + ty;
+            T M2x = tz - phz - tx * phy;
+            T M2y = tz * phz + (T)1.0f + tx * phx;
+            T M2z = -tz * phy + phx - tx;
+            T M3x = -ty - tx * phz + phy;
+            T M3y = -ty * phz + tx - phx;
+            T M3z = ty * phy + tx * phx + (T)1.0f;
+            T dwx = W[j] - W[i], dwy = W[j + N] - W[i + N], dwz = W[j + 2 * N] - W[i + 2 * N];
+            // torsion moment
+            {
+                T c1 = nx * dwx + ny * dwy + nz * dwz;
+                c1 *= p.dt * (T)0.5f * p.m_G * il;
+                V3<T> o = Mijn[k];
+                T mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
+                T my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
+                T mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
+                Mijn[k] = {mx, my, mz};
+                c1 = PI * p.b_r * p.b_r * p.b_r * p.b_r;
+                msx += mx * c1; msy += my * c1; msz += mz * c1;
+            }
+            // bending moment (QUIRK Q1: the summed moment carries dt*E/(4 L0) twice)
+            {
+                T c1 = nx * dwx + ny * dwy + nz * dwz;
+                T c2 = p.dt * (T)0.25f * p.m_E * il;
+                V3<T> o = Mijt[k];
+                T mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
+                T my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
+                T mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
+                Mijt[k] = {mx, my, mz};
+                c2 *= PI * p.b_r * p.b_r * p.b_r * p.b_r;
+                msx += mx * c2; msy += my * c2; msz += mz * c2;
+            }
+            // shear force and asymmetric moment
+            {
+                T hx = (T)0.5f * wsx, hy = (T)0.5f * wsy, hz = (T)0.5f * wsz;
+                T vx = V[j] - V[i] - hy * rz + hz * ry;
+                T vy = V[j + N] - V[i + N] - hz * rx + hx * rz;
+                T vz = V[j + 2 * N] - V[i + 2 * N] - hx * ry + hy * rx;
+                T c = nx * vx + ny * vy + nz * vz;
+                V3<T> o = Oijt[k];
+                T ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c) * p.dt;
+                T oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (vy - ny * c) * p.dt;
+                T oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (vz - nz * c) * p.dt;
+                c = p.m_G * il;
+                Mc = c;
+                c *= p.b_r * p.b_r * PI;
+                fsx += ox * c; fsy += oy * c; fsz += oz * c;
+                Oijt[k] = {ox, oy, oz};
+                msx += (T)0.5f * (ry * oz - rz * oy) * c;
+                msy += (T)0.5f * (rz * ox - rx * oz) * c;
+                msz += (T)0.5f * (rx * oy - ry * ox) * c;
+            }
+            // break check
+            {
+                V3<T> o = Oijt[k], mt = Mijt[k], mn = Mijn[k];
+                Mc *= norm3(o.x, o.y, o.z);
+                Sc += norm3(mt.x, mt.y, mt.z) * (T)4.0f * p.b_r;
+                Mc += norm3(mn.x, mn.y, mn.z) * (T)2.0f * p.b_r;
+                if ((Sc > p.m_Gcritn) || (Mc > p.m_Gcritt)) {
+                    ILtype[k] = 0;
+                    Oijt[k] = {0, 0, 0};
+                    Mijn[k] = {0, 0, 0};
+                    Mijt[k] = {0, 0, 0};
+                    if (broke) broke[k] = 1;
+                }
+            }
+        }
+        F[i] += fsx; F[i + N] += fsy; F[i + 2 * N] += fsz;
+        M[i] += msx; M[i + N] += msy; M[i + 2 * N] += msz;
+    }
+}
+
+// d_CalculateForcesDEM_21 (:338-422) with dd_Calculate_fijn_ppHM_2 (:199-253),
+// dd_Calculate_fijtmijt_ppHM_2 (:255-314), dd_Calculate_mijroll_ppHM_2 (:316-336).
+template <class T>
+void forces_21(const T* R, const T* V, const T* W, const id_t* IL, const uint8_t* ILtype,
+               V3<T>* Oijt, T* F, T* M, uint64_t N, uint64_t K, const FP<T>& p) {
+    const T m_E = p.hm_E, m_G = p.hm_G, rP = p.rP, mP = p.mP;
+    for (uint64_t i = 0; i < N; ++i) {
+        T fsx = 0, fsy = 0, fsz = 0, msx = 0, msy = 0, msz = 0;
+        for (uint64_t s = 0; s < K; ++s) {
+            uint64_t k = i * K + s;
+            id_t j = IL[k];
+            if (j != EMPTY && ILtype[k] == 0) {
+                T rx = R[j] - R[i], ry = R[j + N] - R[i + N], rz = R[j + 2 * N] - R[i + 2 * N];
+                T rijm = norm3(rx, ry, rz);
+                T inv_rm = (T)1 / rijm;
+                T nx = rx * inv_rm, ny = ry * inv_rm, nz = rz * inv_rm;
+                if (rijm < (T)2.0f * rP) {
+                    // normal force with damping
+                    T c1 = std::sqrt(rP * std::fabs(rP - (T)0.5f * rijm));
+                    T Kn = (T)2.0f * m_E * c1;
+                    T Kt = (T)8.0f * m_G * c1;
+                    T wsx = W[j] + W[i], wsy = W[j + N] + W[i + N], wsz = W[j + 2 * N] + W[i + 2 * N];
+                    T vx = V[j] - V[i] + rP * (ny * wsz - nz * wsy);
+                    T vy = V[j + N] - V[i + N] + rP * (nz * wsx - nx * wsz);
+                    T vz = V[j + 2 * N] - V[i + 2 * N] + rP * (nx * wsy - ny * wsx);
+                    T vn = nx * vx + ny * vy + nz * vz;
+                    T fn = (rijm - (T)2.0f * rP) * Kn * two_thirds_t<T>();
+                    c1 = (T)-1.8257f * p.p_A * vn * std::sqrt(Kn * (T)0.5f * mP);
+                    fsx += nx * (fn + c1); fsy += ny * (fn + c1); fsz += nz * (fn + c1);
+                    T vtx = vx - nx * vn, vty = vy - ny * vn, vtz = vz - nz * vn;
+                    // tangential spring, Coulomb cap, damping
+                    V3<T> o = Oijt[k];
+                    T c = nx * o.x + ny * o.y + nz * o.z;
+                    T ox = o.x - nx * c, oy = o.y - ny * c, oz = o.z - nz * c;
+                    c = ox * ox + oy * oy + oz * oz;
+                    if (c > 1e-18) {
+                        c = (T)1 / c;
+                        c *= o.x * o.x + o.y * o.y + o.z * o.z;
+                        c = std::sqrt(c);
+                        ox *= c; oy *= c; oz *= c;
+                    }
+                    ox += vtx * p.dt; oy += vty * p.dt; oz += vtz * p.dt;
+                    T ftx = ox * Kt, fty = oy * Kt, ftz = oz * Kt;
+                    T ftm = ftx * ftx + fty * fty + ftz * ftz;
+                    if (ftm > p.m_mu * p.m_mu * fn * fn) {
+                        c = p.m_mu * std::fabs(fn) * rsqrt_rn(ftm);
+                        ftx *= c; fty *= c; ftz *= c;
+                        c = (T)1 / Kt;
+                        ox = ftx * c; oy = fty * c; oz = ftz * c;
+                    } else {
+                        c = (T)-1.8257f * p.p_A * std::sqrt(Kt * (T)0.5f * mP);
+                        ftx += vtx * c; fty += vty * c; ftz += vtz * c;
+                    }
+                    Oijt[k] = {ox, oy, oz};
+                    fsx += ftx; fsy += fty; fsz += ftz;
+                    msx += (ny * ftz - nz * fty) * rP;
+                    msy += (nz * ftx - nx * ftz) * rP;
+                    msz += (nx * fty - ny * ftx) * rP;
+                    // rolling friction; QUIRK: a (near-)zero spin clears the whole moment sum
+                    T wx = W[i], wy = W[i + N], wz = W[i + 2 * N];
+                    T wim = wx * wx + wy * wy + wz * wz;
+                    if (wim > 1e-18) {
+                        T cr = -p.m_muroll * std::fabs(fn) * rsqrt_rn(wim);
+                        msx += wx * cr; msy += wy * cr; msz += wz * cr;
+                    } else {
+                        msx = 0; msy = 0; msz = 0;
+                    }
+                } else {
+                    Oijt[k] = {0, 0, 0};
+                }
+            } else if (j == EMPTY) {
+                Oijt[k] = {0, 0, 0};
+            }
+        }
+        F[i] += fsx; F[i + N] += fsy; F[i + 2 * N] += fsz;
+        M[i] += msx; M[i + N] += msy; M[i + 2 * N] += msz;
+    }
+}
+
+// d_CalculateIncrementsDEM (md_calculateincrementsdem.cu:19-49)
+template <class T>
+void increments(const T* F, T* V, T* R, const T* M, T* W, uint64_t N, T dt_d_m, T dt, T dt_d_I) {
+    for (uint64_t i = 0; i < N; ++i)
+        for (int c = 0; c < 3; ++c) {
+            uint64_t q = i + c * N;
+            V[q] += F[q] * dt_d_m;
+            R[q] += V[q] * dt;
+            W[q] += M[q] * dt_d_I;
+        }
+}
+
+// d_braziltest_simple2 (md_braziltest_simple2.cu:19-151). The reaction sums are
+// returned in double in particle order (the reference sums per-thread floats in a
+// block tree, then block partials in double on the host).
+template <class T>
+void brazil_platen(T* R, T* V, T* F, uint64_t N, V3<T> c, T RR, T Yt, T Yb, T Ytr, T Ybr, T vt, T Zcut,
+                   double* sfb_out, double* sft_out) {
+    double sfb = 0, sft = 0;
+    for (uint64_t i = 0; i < N; ++i) {
+        T rx = R[i] - c.x, ry = R[i + N], rz = R[i + 2 * N] - c.z;
+        if (rx * rx + rz * rz < RR && rz < Zcut) {
+            if (ry - Ytr > -1e-9) {
+                T fy = F[i + N];
+                if (fy > 0) {
+                    sft += (double)fy;
+                    T iv = V[i] * V[i] + V[i + 2 * N] * V[i + 2 * N];
+                    if (iv > 1e-9) {
+                        iv = rsqrt_rn(iv);
+                        F[i] -= (T)0.45f * fy * V[i] * iv;
+                        F[i + 2 * N] -= (T)0.45f * fy * V[i + 2 * N] * iv;
+                    }
+                }
+                if (ry - Yt > -1e-9) { R[i + N] = Yt; V[i + N] = vt; F[i + N] = 0; }
+            }
+            if (ry - Ybr < 1e-9) {
+                T fy = F[i + N];
+                if (fy < 0) {
+                    sfb += (double)fy;
+                    T iv = V[i] * V[i] + V[i + 2 * N] * V[i + 2 * N];
+                    if (iv > 1e-9) {
+                        iv = rsqrt_rn(iv);
+                        F[i] += (T)0.45f * fy * V[i] * iv;
+                        F[i + 2 * N] += (T)0.45f * fy * V[i + 2 * N] * iv;
+                    }
+                }
+                if (ry - Yb < 1e-9) { R[i + N] = Yb; V[i + N] = 0; F[i + N] = 0; }
+            }
+        }
+    }
+    *sfb_out = sfb; *sft_out = sft;
+}
+
+// d_UniaxialCompression3_simple (md_uniaxialcompression3_simple.cu:19-136)
+template <class T>
+void uniaxial_platen(T* R, T* V, T* F, uint64_t N, V3<T> c, T RR, T Zt, T Zb, T Ztr, T Zbr, T vt, T Zcut,
+                     double* sfb_out, double* sft_out) {
+    double sfb = 0, sft = 0;
+    for (uint64_t i = 0; i < N; ++i) {
+        T rx = R[i] - c.x, ry = R[i + N] - c.y, rz = R[i + 2 * N];
+        if (rx * rx + ry * ry < RR && rz < Zcut) {
+            if (rz - Ztr > -1e-9) {
+                T fz = F[i + 2 * N];
+                if (fz > 0) sft += (double)fz;
+                if (rz - Zt > -1e-9) { R[i + 2 * N] = Zt; V[i + 2 * N] = vt; F[i + 2 * N] = 0; }
+            }
+            if (rz - Zbr < 1e-9) {
+                T fz = F[i + 2 * N];
+                if (fz < 0) sfb += (double)fz;
+                if (rz - Zb < 1e-9) { R[i + 2 * N] = Zb; V[i + 2 * N] = 0; F[i + 2 * N] = 0; }
+            }
+        }
+    }
+    *sfb_out = sfb; *sft_out = sft;
+}
+
+// d_ParallelepipedCutRestriction (md_parallelepipedrestriction.cu:73-159)
+template <class T>
+void cut_restriction(T* R, T* V, T* F, uint64_t N, V3<T> center, V3<T> sized2, V3<T> hp) {
+    for (uint64_t i = 0; i < N; ++i) {
+        T dx = R[i] - center.x, dy = R[i + N] - center.y, dz = R[i + 2 * N] - center.z;
+        bool out = (dx - sized2.x > 0) || (dx + sized2.x < 0) || (dy - sized2.y > 0) ||
+                   (dy + sized2.y < 0) || (dz - sized2.z > 0) || (dz + sized2.z < 0);
+        if (out) {
+            R[i] = hp.x; R[i + N] = hp.y; R[i + 2 * N] = hp.z;
+            V[i] = 0; V[i + N] = 0; V[i + 2 * N] = 0;
+            F[i] = 0; F[i + N] = 0; F[i + 2 * N] = 0;
+        }
+    }
+}
+
+}  // namespace rfo
+
+// ===========================================================================
+// Host scalar logic, restated from md_data_types.h and md_results.cu.
+// ===========================================================================
+namespace rfo {
+static const double MC_pi = 3.1415926535897932384626433832795;   // md_math_constants.h:44
+static const double MC_1d3 = 1.0 / 3.0;                           // md_math_constants.h:15
+static const double length_const = 1e-3;                          // md_phys_constants.h:5
+
+// potential_data::CalculateParameters (md_data_types.h:153-185)
+static void potential_params(rf_potential& P) {
+    P.m_G = 0.5 * P.m_E / (1.0 + P.m_nu);
+    P.b_S = MC_pi * P.b_r * P.b_r;
+    P.p_V = 4.0 * MC_1d3 * MC_pi * P.p_r * P.p_r * P.p_r;
+    P.p_m = P.m_ro * P.p_V;
+    P.b_dd = P.b_d * P.b_d;
+    P.p_1d_m = 1.0 / P.p_m;
+    P.p_I = 0.4 * P.p_m * P.p_r * P.p_r;
+    P.hm_E = 0.5 * P.m_E / (1.0 - P.m_nu * P.m_nu);
+    P.hm_G = 0.5 * P.m_G / (2.0 - P.m_nu);
+    P.p_A = std::log(P.p_e) / std::sqrt(MC_pi * MC_pi + std::log(P.p_e) * std::log(P.p_e));
+    P.aa_farcut = P.a_farcut * P.a_farcut;
+    P.Trayleigh = MC_pi * P.p_r * std::sqrt(2.0 * P.m_ro * (1.0 + P.m_nu)) /
+                  (std::sqrt(P.m_E) * (0.163 * P.m_nu + 0.8766));
+    double t0 = P.m_E * P.b_S / (2.0 * P.p_r), t1 = P.m_G * P.b_S / (2.0 * P.p_r);
+    P.Tsim = (t0 > t1) ? 2.0 * std::sqrt(P.p_m / t0) : 2.0 * std::sqrt(P.p_m / t1);
+    P.dt = (P.Trayleigh < P.Tsim) ? 0.1 * P.Trayleigh : 0.1 * P.Tsim;
+    P.D = 1e-15 * P.m_E * P.b_S / (2.0 * P.p_r);
+    P.a = (2.0 + 0 * 1e-6) * P.p_r;
+    P._1d_a = 1.0 / P.a;
+    P.aa = P.a * P.a;
+    P.dt_d_m = P.p_1d_m * P.dt;
+    P.dt_d_I = P.dt / P.p_I;
+}
+
+static int prepare(rf_task* t, const double ss[3], const double ls[3], double cell_a, double vload,
+                   double minstress, double maxstrain) {
+    rf_potential& P = t->Po;
+    potential_params(P);
+    rf_sample& S = t->S;
+    rf_cells& C = t->C;
+    C.a = (float)cell_a;
+    // sample_data::SetSpaceSizeSi (:86-93), SetLSi (:94-100), CalculateParameters (:105-121)
+    S.spacesize = {(float)(ss[0] / length_const), (float)(ss[1] / length_const), (float)(ss[2] / length_const)};
+    S.spacesized2 = {(float)(0.5 * S.spacesize.x), (float)(0.5 * S.spacesize.y), (float)(0.5 * S.spacesize.z)};
+    S.L = {(float)(ls[0] / length_const - 2.0 * P.p_r), (float)(ls[1] / length_const - 2.0 * P.p_r),
+           (float)(ls[2] / length_const - 2.0 * P.p_r)};
+    S.axis = {0.f, 0.f, 1.f};
+    double C_a = (double)C.a, p_r = P.p_r;
+    S.A = {(float)(1.01 * C_a), (float)(1.01 * C_a), (float)(1.01 * C_a)};
+    S.B = {S.A.x + S.spacesize.x, S.A.y + S.spacesize.y, S.A.z + S.spacesize.z};
+    S.center = {(float)(0.5 * (S.A.x + S.B.x)), (float)(0.5 * (S.A.y + S.B.y)), (float)(0.5 * (S.A.z + S.B.z))};
+    S.size = S.L;
+    S.sized2 = {(float)(0.5 * S.L.x), (float)(0.5 * S.L.y), (float)(0.5 * S.L.z)};
+    S.R0 = (float)(0.5 * S.L.x);
+    S.H0 = (float)(0.5 * S.L.z);
+    S.Vext = MC_pi * (0.5 * S.L.x + p_r) * (0.5 * S.L.x + p_r) * (S.L.z + 2.0 * p_r);
+    S.hidenpoint.x = (float)(S.A.x + 0.5 * S.spacesize.x);
+    S.hidenpoint.y = (float)(S.A.y + 0.5 * S.spacesize.y);
+    {
+        float fl = std::floor((float)((double)S.B.z / C_a));
+        float f3 = fl + 3.0f;
+        S.hidenpoint.z = (float)(((double)f3 - 0.5) * C_a);
+    }
+    S.A_real = {(double)(float)(S.center.x - S.sized2.x), (double)(float)(S.center.y - S.sized2.y),
+                (double)(float)(S.center.z - S.sized2.z)};
+    S.B_real = {(double)(float)(S.center.x + S.sized2.x), (double)(float)(S.center.y + S.sized2.y),
+                (double)(float)(S.center.z + S.sized2.z)};
+    S.size_real = {S.B_real.x - S.A_real.x, S.B_real.y - S.A_real.y, S.B_real.z - S.A_real.z};
+    S.center_real = {0.5 * (S.B_real.x + S.A_real.x), 0.5 * (S.B_real.y + S.A_real.y),
+                     0.5 * (S.B_real.z + S.A_real.z)};
+    S.Vgenmax = 0.f;
+    // interaction_list_data::CalculateParameters (:137-143)
+    t->acut = (float)P.a_farcut;
+    t->aacut = t->acut * t->acut;
+    // cell_data::CalculateParameters (:42-55), called with S.B (md_calculationbraziltest.cu:118)
+    C._1d_a = (float)(1.0 / (double)C.a);
+    C.Nr.x = (unsigned)(std::floor((float)((double)S.B.x * (double)C._1d_a)) + 1.0f);
+    C.Nr.y = (unsigned)(std::floor((float)((double)S.B.y * (double)C._1d_a)) + 1.0f);
+    C.Nr.z = (unsigned)(std::floor((float)((double)S.B.z * (double)C._1d_a)) + 3.0f);
+    C.N = (uint64_t)C.Nr.x * C.Nr.y * C.Nr.z;
+    C._1d_Nr = {(float)(1.0 / (double)C.Nr.x), (float)(1.0 / (double)C.Nr.y), (float)(1.0 / (double)C.Nr.z)};
+    t->bloks = t->N / 1024 + 1;
+    // compression_data::CalculateUParameters / CalculateBParameters (:196-271)
+    rf_compression& K = t->Compress;
+    std::memset(&K, 0, sizeof(K));
+    K.VLoad = vload;
+    K.size_d = S.size_real;
+    K.size = {(float)K.size_d.x, (float)K.size_d.y, (float)K.size_d.z};
+    K.sized2 = {(float)(0.5 * K.size_d.x), (float)(0.5 * K.size_d.y), (float)(0.5 * K.size_d.z)};
+    K.center_d = S.center_real;
+    K.center = {(float)K.center_d.x, (float)K.center_d.y, (float)K.center_d.z};
+    K.Hd2 = K.sized2.z;
+    K.C = (float)(P.m_E * P.b_S / (4.0 * P.p_r));
+    K.mu = (float)P.p_mu;
+    K.MinStress = minstress;
+    K.MaxStrain = maxstrain;
+    if (t->kind == RF_TEST_UNIAXIAL) {
+        K.Size0 = K.size_d.z;
+        K.Bottom = K.center_d.z - 0.5 * K.size_d.z;
+        K.BottomR = K.Bottom + P.p_r;
+        K.Top = K.center_d.z + 0.5 * K.size_d.z;
+        K.TopR = K.Top - P.p_r;
+        K.R = (float)(1.5 * K.sized2.x);
+        K.Area = (float)(MC_pi * (K.sized2.x + P.p_r) * (K.sized2.x + P.p_r));
+        K.ZeroStress = 0.33 * K.MinStress;
+    } else {
+        K.Size0 = K.size_d.y;
+        K.Bottom = K.center_d.y - 0.5 * K.size_d.y;
+        K.BottomR = K.Bottom + P.p_r;
+        K.Top = K.center_d.y + 0.5 * K.size_d.y;
+        K.TopR = K.Top - P.p_r;
+        K.R = (K.sized2.x > K.sized2.z) ? K.sized2.x : (float)(1.05 * K.sized2.z);
+        K.Area = (float)(0.5 * 2 * MC_pi * (K.sized2.x + P.p_r) * (K.size.z + 2.0 * P.p_r));
+        K.ZeroStress = 0.5 * K.MinStress;
+    }
+    K.RR = K.R * K.R;
+    K._1d_Area = (float)(1.0 / (double)K.Area);
+    // V and Strain are read before the driver first sets them; they start at 0 here.
+    K.V = 0.0;
+    K.Strain = 0.0;
+    t->sz0 = (double)K.size.z;
+    return 0;
+}
+
+// compression_data::CompressU / CompressB (md_data_types.h:223-293)
+static void compress(rf_task* t, double pressure) {
+    rf_compression& K = t->Compress;
+    const rf_potential& P = t->Po;
+    K.V = (pressure < 1e-9) ? 10.0 * K.VLoad : K.VLoad;
+    if (t->kind == RF_TEST_UNIAXIAL) {
+        K.size_d.z += K.V * P.dt;
+        K.Top += K.V * P.dt;
+        K.TopR = K.Top - 2.0 * P.p_r;
+        K.size.z = (float)K.size_d.z;
+        K.sized2.z = (float)(0.5 * K.size_d.z);
+        K.center_d.z += K.V * P.dt;
+        K.center.z = (float)K.center_d.z;
+        K.Hd2 = K.sized2.z;
+        K.Strain = (K.size_d.z - K.Size0) / K.Size0;
+    } else {
+        K.size_d.y += K.V * P.dt;
+        K.Top += K.V * P.dt;
+        K.TopR = K.Top - 2.0 * P.p_r;
+        K.size.y = (float)K.size_d.y;
+        K.sized2.y = (float)(0.5 * K.size_d.y);
+        K.center_d.y += K.V * P.dt;
+        K.center.y = (float)K.center_d.y;
+        K.Hd2 = K.sized2.y;
+        K.Strain = (K.size_d.y - K.Size0) / K.Size0;
+    }
+}
+
+// SumForcesULoading (md_results.cu:34-74) given the two reaction sums; sz0 = R.sz0.
+static void sum_forces(rf_task* t, double sfb, double sft, double sz0, double* curve, uint64_t cap,
+                       uint64_t* nsaved) {
+    rf_compression& K = t->Compress;
+    if (curve && *nsaved < cap) {
+        curve[3 * *nsaved + 0] = (K.size_d.z - sz0) / sz0;
+        curve[3 * *nsaved + 1] = sfb * (double)K._1d_Area;
+        curve[3 * *nsaved + 2] = sft * (double)K._1d_Area;
+    }
+    if (curve) ++*nsaved;
+    K.Stress = 0.5 * (std::fabs(sfb) + std::fabs(sft)) * (double)K._1d_Area;
+    if (!K.Loading && K.Stress > K.MinStress) K.Loading = 1;
+    if (K.FractureStress < K.Stress) {
+        K.FractureStress = K.Stress;
+        K.FractureStrain = (sz0 - K.size_d.z) / sz0;
+    }
+    if (K.Loading && K.Stress < K.ZeroStress) K.Fracture = 1;
+}
+
+// One whole test (h_CalculationBrazilTest md_calculationbraziltest.cu:113-214 /
+// h_CalculationUniaxialCompression md_calculationuniaxialcompression.cu:113-216).
+// State vectors are passed in and out so a run can be split and compared step by step.
+template <class T>
+struct Run {
+    rf_task* t;
+    uint64_t N, K, CN;
+    std::vector<T> R, V, W, F, M, iL;
+    std::vector<id_t> IL, CI, CIs, pnC;
+    std::vector<uint8_t> type, broke;
+    std::vector<V3<T>> Rij, Oijt, Mijn, Mijt;
+    double sz0;
+    int status;
+    uint64_t steps, broken;
+
+    void init(const float* R0) {
+        N = t->N; K = t->K; CN = t->C.N;
+        R.assign(3 * N, 0); V.assign(3 * N, 0); W.assign(3 * N, 0); F.assign(3 * N, 0); M.assign(3 * N, 0);
+        for (uint64_t q = 0; q < 3 * N; ++q) R[q] = (T)R0[q];
+        iL.assign(N * K, 0); IL.assign(N * K, EMPTY); type.assign(N * K, 0); broke.assign(N * K, 0);
+        Rij.assign(N * K, {0, 0, 0}); Oijt = Rij; Mijn = Rij; Mijt = Rij;
+        CI.assign(N, 0); CIs.assign(2 * N, 0); pnC.assign(2 * CN, 0);
+        sz0 = t->sz0 != 0.0 ? t->sz0 : (double)t->Compress.size.z;   // R.sz0 (md_results.cu:21)
+        status = 0; steps = 0; broken = 0;
+        T inv_a = (T)t->C._1d_a, a = (T)t->C.a, aacut = (T)t->aacut;
+        int s = cell_distribution<T>(R.data(), N, CI.data(), CIs.data(), pnC.data(), CN, inv_a, t->C.Nr);
+        if (s) status = s;
+        s = construct_list<T>(R.data(), N, CIs.data(), pnC.data(), IL.data(), K, a, inv_a, aacut, t->C.Nr, CN);
+        if (s) status = s;
+        construct_bonds<T>(R.data(), N, IL.data(), type.data(), iL.data(), Rij.data(), Oijt.data(), Mijn.data(),
+                           Mijt.data(), K, (T)(float)t->Po.b_dd);
+        delete_far_links<T>(R.data(), N, IL.data(), type.data(), Rij.data(), Oijt.data(), Mijn.data(), Mijt.data(),
+                            K, (T)(float)t->Po.aa_farcut);
+    }
+
+    FP<T> fparams() const {
+        FP<T> p;
+        const rf_potential& P = t->Po;
+        p.dt = (T)(float)P.dt; p.m_E = (T)(float)P.m_E; p.m_G = (T)(float)P.m_G; p.b_r = (T)(float)P.b_r;
+        p.m_Gcritn = (T)(float)P.m_Ec; p.m_Gcritt = (T)(float)P.m_Gc;
+        p.hm_E = (T)(float)P.hm_E; p.hm_G = (T)(float)P.hm_G; p.p_A = (T)(float)P.p_A;
+        p.m_mu = (T)(float)P.p_mu; p.m_muroll = (T)(float)P.p_mur; p.mP = (T)(float)P.p_m; p.rP = (T)(float)P.p_r;
+        return p;
+    }
+
+    bool running() const {
+        return t->Compress.Strain < t->Compress.MaxStrain && !t->Compress.Fracture;
+    }
+
+    // One pass of the loop body (md_calculationbraziltest.cu:170-190).
+    void step(double* curve, uint64_t cap, uint64_t* nsaved) {
+        const rf_potential& P = t->Po;
+        rf_compression& Kc = t->Compress;
+        T inv_a = (T)t->C._1d_a, a = (T)t->C.a, aacut = (T)t->aacut;
+        int s = cell_distribution<T>(R.data(), N, CI.data(), CIs.data(), pnC.data(), CN, inv_a, t->C.Nr);
+        if (s && !status) status = s;
+        s = reconstruct_bpm<T>(R.data(), N, CIs.data(), pnC.data(), IL.data(), type.data(), K, a, inv_a, aacut,
+                               t->C.Nr, CN);
+        if (s && !status) status = s;
+        std::fill(F.begin(), F.end(), (T)0);
+        std::fill(M.begin(), M.end(), (T)0);
+        FP<T> p = fparams();
+        forces_22<T>(R.data(), V.data(), W.data(), IL.data(), type.data(), iL.data(), Rij.data(), Oijt.data(),
+                     Mijn.data(), Mijt.data(), F.data(), M.data(), N, K, p, broke.data());
+        forces_21<T>(R.data(), V.data(), W.data(), IL.data(), type.data(), Oijt.data(), F.data(), M.data(), N, K, p);
+        double sfb = 0, sft = 0;
+        V3<T> c = {(T)Kc.center.x, (T)Kc.center.y, (T)Kc.center.z};
+        if (t->kind == RF_TEST_BRAZIL) {
+            T Zcut = (T)(float)((double)t->S.center.y + (double)t->S.spacesized2.y);
+            brazil_platen<T>(R.data(), V.data(), F.data(), N, c, (T)Kc.RR, (T)(float)Kc.Top, (T)(float)Kc.Bottom,
+                             (T)(float)Kc.TopR, (T)(float)Kc.BottomR, (T)(float)Kc.V, Zcut, &sfb, &sft);
+        } else {
+            T Zcut = (T)(float)((double)t->S.center.z + (double)t->S.spacesized2.z);
+            uniaxial_platen<T>(R.data(), V.data(), F.data(), N, c, (T)Kc.RR, (T)(float)Kc.Top, (T)(float)Kc.Bottom,
+                               (T)(float)Kc.TopR, (T)(float)Kc.BottomR, (T)(float)Kc.V, Zcut, &sfb, &sft);
+        }
+        sum_forces(t, sfb, sft, sz0, curve, cap, nsaved);
+        increments<T>(F.data(), V.data(), R.data(), M.data(), W.data(), N, (T)(float)P.dt_d_m, (T)(float)P.dt,
+                      (T)(float)P.dt_d_I);
+        const rf_sample& S = t->S;
+        cut_restriction<T>(R.data(), V.data(), F.data(), N, {(T)S.center.x, (T)S.center.y, (T)S.center.z},
+                           {(T)S.spacesized2.x, (T)S.spacesized2.y, (T)S.spacesized2.z},
+                           {(T)S.hidenpoint.x, (T)S.hidenpoint.y, (T)S.hidenpoint.z});
+        delete_far_links<T>(R.data(), N, IL.data(), type.data(), Rij.data(), Oijt.data(), Mijn.data(), Mijt.data(),
+                            K, (T)(float)P.aa_farcut);
+        compress(t, Kc.Stress);
+        ++steps;
+    }
+};
+}  // namespace rfo
+
+extern "C" {
+int rfo_task_prepare(rf_task* t, const double ss[3], const double ls[3], double cell_a, double vload,
+                     double minstress, double maxstrain) {
+    return rfo::prepare(t, ss, ls, cell_a, vload, minstress, maxstrain);
+}
+void rfo_compress(rf_task* t, double pressure) { rfo::compress(t, pressure); }
+void rfo_sum_forces(rf_task* t, double sfb, double sft, double sz0) {
+    uint64_t n = 0;
+    rfo::sum_forces(t, sfb, sft, sz0, nullptr, 0, &n);
+}
+
+// Full run in FP32 (reference precision). State in/out arrays are the reference
+// layout; R_io holds the initial positions on entry and final ones on exit.
+// Returns the number of steps taken; *status gets the first bound/overflow status.
+uint64_t rfo_run_f(rf_task* t, float* R_io, uint64_t max_steps, float* V_out, float* W_out,
+                   uint64_t* IL_out, uint8_t* type_out, float* iL_out, float* Rij_out, float* Oijt_out,
+                   float* Mijn_out, float* Mijt_out, uint8_t* broke_out, double* curve, uint64_t cap,
+                   uint64_t* nsaved, int* status) {
+    rfo::Run<float> r;
+    r.t = t;
+    r.init(R_io);
+    uint64_t ns = 0;
+    while (r.running() && (max_steps == 0 || r.steps < max_steps)) r.step(curve, cap, &ns);
+    if (nsaved) *nsaved = ns;
+    uint64_t N = r.N, K = r.K;
+    std::memcpy(R_io, r.R.data(), sizeof(float) * 3 * N);
+    if (V_out) std::memcpy(V_out, r.V.data(), sizeof(float) * 3 * N);
+    if (W_out) std::memcpy(W_out, r.W.data(), sizeof(float) * 3 * N);
+    if (IL_out) std::memcpy(IL_out, r.IL.data(), sizeof(uint64_t) * N * K);
+    if (type_out) std::memcpy(type_out, r.type.data(), N * K);
+    if (iL_out) std::memcpy(iL_out, r.iL.data(), sizeof(float) * N * K);
+    if (Rij_out) std::memcpy(Rij_out, r.Rij.data(), sizeof(float) * 3 * N * K);
+    if (Oijt_out) std::memcpy(Oijt_out, r.Oijt.data(), sizeof(float) * 3 * N * K);
+    if (Mijn_out) std::memcpy(Mijn_out, r.Mijn.data(), sizeof(float) * 3 * N * K);
+    if (Mijt_out) std::memcpy(Mijt_out, r.Mijt.data(), sizeof(float) * 3 * N * K);
+    if (broke_out) std::memcpy(broke_out, r.broke.data(), N * K);
+    if (status) *status = r.status;
+    return r.steps;
+}
+
+// Same run in FP64 (the FP64 oracle): positions, velocities, forces and all
+// parameters in double. Outputs are rounded to float for comparison.
+uint64_t rfo_run_d(rf_task* t, const float* R_in, uint64_t max_steps, double* R_out, double* curve,
+                   uint64_t cap, uint64_t* nsaved, uint8_t* type_out, int* status) {
+    rfo::Run<double> r;
+    r.t = t;
+    r.init(R_in);
+    uint64_t ns = 0;
+    while (r.running() && (max_steps == 0 || r.steps < max_steps)) r.step(curve, cap, &ns);
+    if (nsaved) *nsaved = ns;
+    if (R_out) std::memcpy(R_out, r.R.data(), sizeof(double) * 3 * r.N);
+    if (type_out) std::memcpy(type_out, r.type.data(), r.N * r.K);
+    if (status) *status = r.status;
+    return r.steps;
+}
+}  // extern "C"
+// ===========================================================================
+// C ABI for the tests (ctypes). Suffix _f = float instance, _d = double instance.
+// Slot state arrays are float3/double3 AoS, ids uint64 (uint_fast32_t on Linux).
+// ===========================================================================
+extern "C" {
+
+int rfo_cell_distribution_f(const float* R, uint64_t N, uint64_t* CI, uint64_t* CIs, uint64_t* pnC,
+                            uint64_t CN, float inv_a, rf_uint3 cN) {
+    return rfo::cell_distribution<float>(R, N, CI, CIs, pnC, CN, inv_a, cN);
+}
+int rfo_construct_list_f(const float* R, uint64_t N, const uint64_t* CIs, const uint64_t* pnC, uint64_t* IL,
+                         uint64_t K, float a, float inv_a, float aacut, rf_uint3 cN, uint64_t CN) {
+    return rfo::construct_list<float>(R, N, CIs, pnC, IL, K, a, inv_a, aacut, cN, CN);
+}
+int rfo_reconstruct_bpm_f(const float* R, uint64_t N, const uint64_t* CIs, const uint64_t* pnC, uint64_t* IL,
+                          uint8_t* ILtype, uint64_t K, float a, float inv_a, float aacut, rf_uint3 cN,
+                          uint64_t CN) {
+    return rfo::reconstruct_bpm<float>(R, N, CIs, pnC, IL, ILtype, K, a, inv_a, aacut, cN, CN);
+}
+void rfo_delete_far_links_f(const float* R, uint64_t N, uint64_t* IL, uint8_t* ILtype, float* Rij, float* Oijt,
+                            float* Mijn, float* Mijt, uint64_t K, float aacut) {
+    typedef rfo::V3<float> v;
+    rfo::delete_far_links<float>(R, N, IL, ILtype, (v*)Rij, (v*)Oijt, (v*)Mijn, (v*)Mijt, K, aacut);
+}
+void rfo_construct_bonds_f(const float* R, uint64_t N, const uint64_t* IL, uint8_t* ILtype, float* iL,
+                           float* Rij, float* Oijt, float* Mijn, float* Mijt, uint64_t K, float aa_create) {
+    typedef rfo::V3<float> v;
+    rfo::construct_bonds<float>(R, N, IL, ILtype, iL, (v*)Rij, (v*)Oijt, (v*)Mijn, (v*)Mijt, K, aa_create);
+}
+void rfo_forces_22_f(const float* R, const float* V, const float* W, const uint64_t* IL, uint8_t* ILtype,
+                     const float* iL, float* Rij, float* Oijt, float* Mijn, float* Mijt, float* F, float* M,
+                     uint64_t N, uint64_t K, float dt, float m_E, float m_G, float b_r, float m_Gcritn,
+                     float m_Gcritt, uint8_t* broke) {
+    typedef rfo::V3<float> v;
+    rfo::FP<float> p{};
+    p.dt = dt; p.m_E = m_E; p.m_G = m_G; p.b_r = b_r; p.m_Gcritn = m_Gcritn; p.m_Gcritt = m_Gcritt;
+    rfo::forces_22<float>(R, V, W, IL, ILtype, iL, (v*)Rij, (v*)Oijt, (v*)Mijn, (v*)Mijt, F, M, N, K, p, broke);
+}
+void rfo_forces_21_f(const float* R, const float* V, const float* W, const uint64_t* IL, const uint8_t* ILtype,
+                     float* Oijt, float* F, float* M, uint64_t N, uint64_t K, float dt, float m_E, float m_G,
+                     float p_A, float m_mu, float m_muroll, float mP, float rP) {
+    typedef rfo::V3<float> v;
+    rfo::FP<float> p{};
+    p.dt = dt; p.hm_E = m_E; p.hm_G = m_G; p.p_A = p_A; p.m_mu = m_mu; p.m_muroll = m_muroll; p.mP = mP; p.rP = rP;
+    rfo::forces_21<float>(R, V, W, IL, ILtype, (v*)Oijt, F, M, N, K, p);
+}
+void rfo_increments_f(const float* F, float* V, float* R, const float* M, float* W, uint64_t N, float dt_d_m,
+                      float dt, float dt_d_I) {
+    rfo::increments<float>(F, V, R, M, W, N, dt_d_m, dt, dt_d_I);
+}
+void rfo_brazil_platen_f(float* R, float* V, float* F, uint64_t N, rf_float3 c, float RR, float Yt, float Yb,
+                         float Ytr, float Ybr, float vt, float Zcut, double* sums) {
+    rfo::brazil_platen<float>(R, V, F, N, {c.x, c.y, c.z}, RR, Yt, Yb, Ytr, Ybr, vt, Zcut, &sums[0], &sums[1]);
+}
+void rfo_uniaxial_platen_f(float* R, float* V, float* F, uint64_t N, rf_float3 c, float RR, float Zt, float Zb,
+                           float Ztr, float Zbr, float vt, float Zcut, double* sums) {
+    rfo::uniaxial_platen<float>(R, V, F, N, {c.x, c.y, c.z}, RR, Zt, Zb, Ztr, Zbr, vt, Zcut, &sums[0], &sums[1]);
+}
+void rfo_cut_restriction_f(float* R, float* V, float* F, uint64_t N, rf_float3 center, rf_float3 sized2,
+                           rf_float3 hp) {
+    rfo::cut_restriction<float>(R, V, F, N, {center.x, center.y, center.z}, {sized2.x, sized2.y, sized2.z},
+                                {hp.x, hp.y, hp.z});
+}
+float rfo_rsqrt_rn_f(float x) { return rfo::rsqrt_rn<float>(x); }
+void rfo_rsqrt_rn_array_f(const float* x, float* y, uint64_t n) {
+    for (uint64_t i = 0; i < n; ++i) y[i] = rfo::rsqrt_rn<float>(x[i]);
+}
+
+}  // extern "C"

@@ -1,0 +1,1122 @@
+// Fused B200 engine for the explicit BPM test loop.
+//
+// One explicit step of the reference (md_calculationbraziltest.cu:170-190:
+// CellDistribution, InteractionListReConstructBPM, F=M=0, _22, _21, platen,
+// SumForcesULoading, increments, cut, DeleteFarLinks, CompressB/U) is ONE kernel
+// here, one thread per particle:
+//
+//   delete  -- DeleteFarLinks of the previous step, with this step's positions
+//              (the reference runs it at the end of the previous step on the same
+//              positions, so the result is identical);
+//   add     -- new neighbours inside a_farcut, taken from a Verlet candidate list
+//              (cutoff a_farcut + skin, rebuilt only when some particle has moved
+//              more than 0.45*skin since the last build) instead of re-binning every
+//              step. New links are inserted in the order the reference would insert
+//              them: by (octant-cell rank, id), computed from the same float cell
+//              arithmetic, into the first free slot;
+//   bonds   -- bond slots in slot order (same sums, same rounding as _22);
+//   contacts-- contact slots in slot order (as _21), F = (0 + F_bond) + F_contact;
+//   platen, increments, cut -- per particle, into the other position buffer;
+//   load    -- per-block FP64 partial sums, the last block finishes the scalar
+//              step (SumForcesULoading, CompressB/U, fracture, load curve) on device.
+//
+// Layout in HBM: particle vectors as float4 (x, y, z, 0), double-buffered; rows
+// slot-major (ids[k*N + i]) so a warp reading slot k of 32 particles is one
+// coalesced 128-byte access; per-slot state as 12 float planes (Rij, Oijt, Mijn,
+// Mijt); per-particle 32-bit masks for occupied slots, bond slots and contacts
+// with non-zero tangential overlap (so empty and idle slots cost no state reads).
+//
+// The step loop is a CUDA graph: WHILE(continue) { IF(rebuild) {bin, scan,
+// scatter, candidates}; step }, with both conditions set on device by the step
+// kernel, so one graph launch advances many steps without host round trips.
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include "rf_physics.cuh"
+
+namespace rf {
+
+// Scalar state of the run, device resident (compression_data + result bookkeeping).
+struct DevScalars {
+    double V, VLoad, Top, Bottom, TopR, BottomR, FractureStress, FractureStrain, MinStress, ZeroStress, Stress,
+        Strain, MaxStrain, Size0;
+    double size_d[3], center_d[3];
+    double sz0;
+    float center[3], size[3], sized2[3];
+    float RR, _1d_Area, Hd2;
+    int32_t Loading, Fracture;
+    unsigned long long steps, target, rebuilds, curve_n, broken;
+    uint32_t done, err, rebuild, moved, block_counter, pad;
+};
+
+struct Consts {
+    uint32_t N, K, KC;
+    int kind;
+    double dt_d, p_r_d;
+    BondParams bp;
+    ContactParams cp;
+    float dtm, dt, dtI;
+    float aacut, aa_farcut;
+    RefGrid g;
+    float zcut;
+    rf_float3 box_c, box_h, hp;
+    // candidate grid
+    float cg_inv_h;
+    float cg_ox, cg_oy, cg_oz;
+    uint32_t cg_nx, cg_ny, cg_nz, cg_cells;
+    float rc2, disp2;
+    unsigned long long curve_cap;
+    cudaGraphConditionalHandle h_loop, h_rebuild;
+    int use_graph;
+};
+
+struct Dev {
+    float4* pos[2];
+    float4* vel[2];
+    float4* ang[2];
+    uint32_t* ids;      // [K][N]
+    float* il;          // [K][N]
+    float* st;          // [12][K][N]
+    uint32_t* live;     // [N]
+    uint32_t* bond;     // [N]
+    uint32_t* cmask;    // [N]
+    uint32_t* cand;     // [KC][N]
+    uint32_t* cand_n;   // [N]
+    unsigned long long* member;   // [N]
+    float4* pos_ref;    // [N]
+    uint32_t* cg_key;   // [N]
+    uint32_t* cg_count; // [cells+1]
+    uint32_t* cg_start; // [cells+1]
+    uint32_t* cg_fill;  // [cells+1]
+    uint32_t* cg_bsum;
+    uint32_t* cg_sorted;   // [N]
+    double2* partial;   // [blocks]
+    unsigned long long n_particles;
+    double* curve;      // [cap][3]
+    DevScalars* sc;
+};
+
+__device__ __forceinline__ f3 f4to3(const float4 v) { return mk3(v.x, v.y, v.z); }
+__device__ __forceinline__ float* plane(const Dev& d, const Consts& c, int p, uint32_t k) {
+    return d.st + ((size_t)p * c.K + k) * c.N;
+}
+
+// ---------------------------------------------------------------------------
+// Candidate-list rebuild (runs only when the displacement flag is set)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool gate_closed(const Dev& d, const Consts& c) {
+    // In graph mode the IF node gates the rebuild; on a plain stream the kernels check.
+    return !c.use_graph && (d.sc->rebuild == 0 || d.sc->done);
+}
+
+__device__ __forceinline__ uint32_t cg_cell_of(const float4 x, const Consts& c) {
+    const float fx = floorf((x.x - c.cg_ox) * c.cg_inv_h);
+    const float fy = floorf((x.y - c.cg_oy) * c.cg_inv_h);
+    const float fz = floorf((x.z - c.cg_oz) * c.cg_inv_h);
+    if (!(fx >= 0.f && fy >= 0.f && fz >= 0.f)) return 0xFFFFFFFFu;
+    const uint32_t ix = (uint32_t)fx, iy = (uint32_t)fy, iz = (uint32_t)fz;
+    if (ix >= c.cg_nx || iy >= c.cg_ny || iz >= c.cg_nz) return 0xFFFFFFFFu;
+    return ix + c.cg_nx * (iy + c.cg_ny * iz);
+}
+
+__global__ void k_rb_zero(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= c.cg_cells; q += gridDim.x * blockDim.x) {
+        d.cg_count[q] = 0;
+        d.cg_fill[q] = 0;
+    }
+}
+
+__global__ void k_rb_bin(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    const float4* P = d.pos[d.sc->steps & 1];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        uint32_t key = cg_cell_of(P[i], c);
+        if (key == 0xFFFFFFFFu) key = c.cg_cells;          // parked or outside: tail bin, no candidates
+        d.cg_key[i] = key;
+        atomicAdd(&d.cg_count[key], 1u);
+    }
+}
+
+__global__ void k_rb_scan_sums(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    __shared__ uint32_t sh[32];
+    const size_t n = (size_t)c.cg_cells + 1, base = (size_t)blockIdx.x * 4096;
+    uint32_t s = 0;
+    for (int t = threadIdx.x; t < 4096; t += blockDim.x)
+        if (base + t < n) s += d.cg_count[base + t];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) d.cg_bsum[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_rb_scan_totals(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    const uint32_t nb = (c.cg_cells + 1 + 4095) / 4096;
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (uint32_t b = 0; b < nb; ++b) { uint32_t v = d.cg_bsum[b]; d.cg_bsum[b] = acc; acc += v; }
+    }
+}
+
+__global__ void k_rb_scan_apply(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    __shared__ uint32_t wsum[32];
+    const size_t n = (size_t)c.cg_cells + 1;
+    const size_t base = (size_t)blockIdx.x * 4096 + (size_t)threadIdx.x * 4;
+    uint32_t v[4], t = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { v[q] = (base + q < n) ? d.cg_count[base + q] : 0; t += v[q]; }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t incl = t;
+    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += y; }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t s = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0, si = s;
+        for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, si, o); if (lane >= o) si += y; }
+        wsum[lane] = si - s;
+    }
+    __syncthreads();
+    uint32_t run = d.cg_bsum[blockIdx.x] + wsum[w] + incl - t;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) { if (base + q < n) d.cg_start[base + q] = run; run += v[q]; }
+}
+
+__global__ void k_rb_scatter(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        const uint32_t key = d.cg_key[i];
+        d.cg_sorted[d.cg_start[key] + atomicAdd(&d.cg_fill[key], 1u)] = i;
+    }
+}
+
+// Candidates: every j != i within rc of i (27 cells), and which of them sit in i's row.
+__global__ void k_rb_cand(Dev d, Consts c) {
+    if (gate_closed(d, c)) return;
+    const float4* P = d.pos[d.sc->steps & 1];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        const float4 xi = P[i];
+        d.pos_ref[i] = xi;
+        const uint32_t key = d.cg_key[i];
+        uint32_t n = 0;
+        if (key < c.cg_cells) {
+            const int ix = key % c.cg_nx, iy = (key / c.cg_nx) % c.cg_ny, iz = key / (c.cg_nx * c.cg_ny);
+            for (int dz = -1; dz <= 1; ++dz) {
+                const int z = iz + dz;
+                if (z < 0 || z >= (int)c.cg_nz) continue;
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int y = iy + dy;
+                    if (y < 0 || y >= (int)c.cg_ny) continue;
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const int x = ix + dx;
+                        if (x < 0 || x >= (int)c.cg_nx) continue;
+                        const uint32_t cell = x + c.cg_nx * (y + c.cg_ny * z);
+                        const uint32_t s = d.cg_start[cell], e = s + d.cg_count[cell];
+                        for (uint32_t q = s; q < e; ++q) {
+                            const uint32_t j = d.cg_sorted[q];
+                            if (j == i) continue;
+                            const float4 xj = P[j];
+                            const float ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
+                            if (ddx * ddx + ddy * ddy + ddz * ddz < c.rc2) {
+                                if (n < c.KC) d.cand[(size_t)n * c.N + i] = j;
+                                else raise_status(&d.sc->err, RF_ERR_CAPACITY);
+                                ++n;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (n > c.KC) n = c.KC;
+        d.cand_n[i] = n;
+        // membership: candidates already in the row
+        unsigned long long mem = 0ull;
+        uint32_t live = d.live[i];
+        while (live) {
+            const uint32_t k = __ffs(live) - 1;
+            live &= live - 1;
+            const uint32_t j = d.ids[(size_t)k * c.N + i];
+            for (uint32_t q = 0; q < n; ++q)
+                if (d.cand[(size_t)q * c.N + i] == j) { mem |= 1ull << q; break; }
+        }
+        d.member[i] = mem;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&d.sc->rebuilds, 1ull);
+}
+
+// ---------------------------------------------------------------------------
+// The step kernel
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void zero_slot_state(const Dev& d, const Consts& c, uint32_t k, uint32_t i) {
+#pragma unroll
+    for (int p = 0; p < 12; ++p) plane(d, c, p, k)[i] = 0.f;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
+    DevScalars* sc = d.sc;
+    if (sc->done) return;
+    const uint32_t cur = (uint32_t)(sc->steps & 1ull), nxt = cur ^ 1u;
+    const float4* __restrict__ P = d.pos[cur];
+    const float4* __restrict__ Vv = d.vel[cur];
+    const float4* __restrict__ Wv = d.ang[cur];
+    const uint32_t N = c.N;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < N;
+    const uint32_t FULL = 0xffffffffu;
+
+    // platen arguments of this step, as the driver passes them (double -> float)
+    const float Top = (float)sc->Top, Bottom = (float)sc->Bottom, TopR = (float)sc->TopR,
+                BottomR = (float)sc->BottomR, vt = (float)sc->V, RR = sc->RR;
+    rf_float3 cc;
+    cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
+
+    f3 xi = mk3(0.f, 0.f, 0.f), vi = xi, wi = xi;
+    uint32_t live = 0, bond = 0, cm = 0;
+    unsigned long long mem = 0ull;
+    uint32_t ncand = 0;
+    if (valid) {
+        xi = f4to3(P[i]); vi = f4to3(Vv[i]); wi = f4to3(Wv[i]);
+        live = d.live[i]; bond = d.bond[i]; cm = d.cmask[i];
+        mem = d.member[i]; ncand = d.cand_n[i];
+    }
+    const uint32_t live0 = live, bond0 = bond, cm0 = cm;
+    const unsigned long long mem0 = mem;
+
+    // ---- delete: d_DeleteFarLinks (md_interaction_list_reconstructbpm.cu:141-186)
+    {
+        const uint32_t wl = __reduce_or_sync(FULL, live);
+        const uint32_t kend = 32u - __clz(wl);
+        for (uint32_t k = 0; k < kend; ++k) {
+            if (!((live >> k) & 1u)) continue;
+            const size_t s = (size_t)k * N + i;
+            const uint32_t j = d.ids[s];
+            const float rr = dist2_rn(xi, f4to3(P[j]));
+            if (rr > c.aa_farcut || (double)rr < 1e-10) {
+                d.ids[s] = EMPTY32;
+                zero_slot_state(d, c, k, i);
+                const uint32_t bit = 1u << k;
+                live &= ~bit; bond &= ~bit; cm &= ~bit;
+                for (uint32_t q = 0; q < ncand; ++q)
+                    if (d.cand[(size_t)q * N + i] == j) { mem &= ~(1ull << q); break; }
+            }
+        }
+    }
+
+    // ---- add: InteractionListReConstructBPM (md_interaction_list_reconstructbpm.cu:13-46,80-139)
+    if (valid) {
+        unsigned long long tried = mem;
+        bool have_cells = false;
+        int64_t cells[8];
+        for (;;) {
+            unsigned long long best = ~0ull;
+            uint32_t best_q = 0;
+            for (uint32_t q = 0; q < ncand; ++q) {
+                if ((tried >> q) & 1ull) continue;
+                const uint32_t j = d.cand[(size_t)q * N + i];
+                const f3 xj = f4to3(P[j]);
+                const float rr = dist2_rn(xi, xj);
+                if (!(rr < c.aacut && (double)rr > 1e-10)) continue;
+                if (!have_cells) { octant_cells(xi, c.g, cells); have_cells = true; }
+                const int rank = octant_rank(cells, ref_cell(xj, c.g));
+                if (rank < 0) continue;
+                const unsigned long long key = ((unsigned long long)rank << 32) | j;
+                if (key < best) { best = key; best_q = q; }
+            }
+            if (best == ~0ull) break;
+            tried |= 1ull << best_q;
+            const uint32_t free = ~live & (c.K >= 32 ? 0xffffffffu : ((1u << c.K) - 1u));
+            if (!free) { raise_status(&sc->err, RF_ERR_ROW_OVERFLOW); continue; }
+            uint32_t k;
+            if (i == 0 && (free & 1u) && (free & ~1u)) k = __ffs(free & ~1u) - 1;   // kdxfree==0 quirk
+            else k = __ffs(free) - 1;
+            d.ids[(size_t)k * N + i] = (uint32_t)(best & 0xffffffffull);
+            live |= 1u << k;
+            mem |= 1ull << best_q;
+        }
+    }
+
+    // ---- bonds: d_CalculateForcesDEM_22 (md_calculateforcesdem3.cu:424-483)
+    f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
+    uint32_t nbroken = 0;
+    {
+        const uint32_t wb = __reduce_or_sync(FULL, bond);
+        const uint32_t kend = 32u - __clz(wb);
+        for (uint32_t k = 0; k < kend; ++k) {
+            if (!((bond >> k) & 1u)) continue;
+            const size_t s = (size_t)k * N + i;
+            const uint32_t j = d.ids[s];
+            const f3 xj = f4to3(P[j]);
+            const f3 r = mk3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
+            float* p0 = d.st + (size_t)k * N + i;
+            const size_t ps = (size_t)c.K * N;
+            f3 rij = mk3(p0[0], p0[ps], p0[2 * ps]);
+            f3 oijt = mk3(p0[3 * ps], p0[4 * ps], p0[5 * ps]);
+            f3 mijn = mk3(p0[6 * ps], p0[7 * ps], p0[8 * ps]);
+            f3 mijt = mk3(p0[9 * ps], p0[10 * ps], p0[11 * ps]);
+            const bool broke = bond_slot(c.bp, r, vi, f4to3(Vv[j]), wi, f4to3(Wv[j]), d.il[s], rij, oijt, mijn, mijt,
+                                         fsb, msb);
+            p0[0] = rij.x; p0[ps] = rij.y; p0[2 * ps] = rij.z;
+            p0[3 * ps] = oijt.x; p0[4 * ps] = oijt.y; p0[5 * ps] = oijt.z;
+            p0[6 * ps] = mijn.x; p0[7 * ps] = mijn.y; p0[8 * ps] = mijn.z;
+            p0[9 * ps] = mijt.x; p0[10 * ps] = mijt.y; p0[11 * ps] = mijt.z;
+            if (broke) { bond &= ~(1u << k); ++nbroken; }
+        }
+    }
+
+    // ---- contacts: d_CalculateForcesDEM_21 (md_calculateforcesdem3.cu:338-422)
+    f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
+    {
+        const uint32_t ct = live & ~bond;
+        const uint32_t wc = __reduce_or_sync(FULL, ct);
+        const uint32_t kend = 32u - __clz(wc);
+        const size_t ps = (size_t)c.K * N;
+        for (uint32_t k = 0; k < kend; ++k) {
+            if (!((ct >> k) & 1u)) continue;
+            const size_t s = (size_t)k * N + i;
+            const uint32_t j = d.ids[s];
+            const f3 xj = f4to3(P[j]);
+            const f3 r = mk3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
+            float* o0 = d.st + 3 * ps + (size_t)k * N + i;
+            const uint32_t bit = 1u << k;
+            f3 o = (cm & bit) ? mk3(o0[0], o0[ps], o0[2 * ps]) : mk3(0.f, 0.f, 0.f);
+            if (contact_slot(c.cp, r, vi, f4to3(Vv[j]), wi, f4to3(Wv[j]), o, fsc, msc)) {
+                o0[0] = o.x; o0[ps] = o.y; o0[2 * ps] = o.z;
+                cm |= bit;
+            } else if (cm & bit) {
+                o0[0] = 0.f; o0[ps] = 0.f; o0[2 * ps] = 0.f;
+                cm &= ~bit;
+            }
+        }
+    }
+
+    double sfb = 0.0, sft = 0.0;
+    uint32_t moved = 0;
+    if (valid) {
+        if (live != live0) d.live[i] = live;
+        if (bond != bond0) d.bond[i] = bond;
+        if (cm != cm0) d.cmask[i] = cm;
+        if (mem != mem0) d.member[i] = mem;
+        // F = 0 after the memset, then += _22 sums, then += _21 sums
+        float Fx = 0.0f + fsb.x, Fy = 0.0f + fsb.y, Fz = 0.0f + fsb.z;
+        Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
+        float Mx = 0.0f + msb.x, My = 0.0f + msb.y, Mz = 0.0f + msb.z;
+        Mx += msc.x; My += msc.y; Mz += msc.z;
+        float Rx = xi.x, Ry = xi.y, Rz = xi.z, Vx = vi.x, Vy = vi.y, Vz = vi.z;
+        if (KIND == RF_TEST_BRAZIL)
+            brazil_particle(Rx, Ry, Rz, Vx, Vy, Vz, Fx, Fy, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, c.zcut, sfb, sft);
+        else
+            uniaxial_particle(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, c.zcut, sfb, sft);
+        // d_CalculateIncrementsDEM (md_calculateincrementsdem.cu:19-49)
+        Vx += __fmul_rn(Fx, c.dtm); Vy += __fmul_rn(Fy, c.dtm); Vz += __fmul_rn(Fz, c.dtm);
+        Rx += __fmul_rn(Vx, c.dt); Ry += __fmul_rn(Vy, c.dt); Rz += __fmul_rn(Vz, c.dt);
+        float Wx = wi.x + __fmul_rn(Mx, c.dtI), Wy = wi.y + __fmul_rn(My, c.dtI), Wz = wi.z + __fmul_rn(Mz, c.dtI);
+        // d_ParallelepipedCutRestriction (md_parallelepipedrestriction.cu:73-159)
+        if (outside_box(Rx, Ry, Rz, c.box_c, c.box_h)) {
+            Rx = c.hp.x; Ry = c.hp.y; Rz = c.hp.z;
+            Vx = 0.f; Vy = 0.f; Vz = 0.f;
+        }
+        d.pos[nxt][i] = make_float4(Rx, Ry, Rz, 0.f);
+        d.vel[nxt][i] = make_float4(Vx, Vy, Vz, 0.f);
+        d.ang[nxt][i] = make_float4(Wx, Wy, Wz, 0.f);
+        const float4 pr = d.pos_ref[i];
+        const float ex = Rx - pr.x, ey = Ry - pr.y, ez = Rz - pr.z;
+        moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+    }
+
+    // ---- block reductions (fixed tree: deterministic)
+    __shared__ double s_b[4], s_t[4];
+    __shared__ uint32_t s_n[4], s_m[4];
+    __shared__ bool s_last;
+    for (int o = 16; o; o >>= 1) {
+        sfb += __shfl_xor_sync(FULL, sfb, o);
+        sft += __shfl_xor_sync(FULL, sft, o);
+    }
+    const uint32_t wn = __reduce_add_sync(FULL, nbroken), wm = __reduce_or_sync(FULL, moved);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { s_b[w] = sfb; s_t[w] = sft; s_n[w] = wn; s_m[w] = wm; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double b = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
+        const double t = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
+        d.partial[blockIdx.x] = make_double2(b, t);
+        const uint32_t nb = s_n[0] + s_n[1] + s_n[2] + s_n[3];
+        if (nb) atomicAdd(&sc->broken, (unsigned long long)nb);
+        if (s_m[0] | s_m[1] | s_m[2] | s_m[3]) atomicOr(&sc->moved, 1u);
+        __threadfence();
+        const uint32_t ticket = atomicAdd(&sc->block_counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+
+    // ---- last block: SumForcesULoading (md_results.cu:34-74) and CompressB/U
+    __threadfence();
+    double pb = 0.0, pt = 0.0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const double2 v = __ldcg(&d.partial[b]);
+        pb += v.x; pt += v.y;
+    }
+    for (int o = 16; o; o >>= 1) {
+        pb += __shfl_xor_sync(FULL, pb, o);
+        pt += __shfl_xor_sync(FULL, pt, o);
+    }
+    __syncthreads();
+    if (l == 0) { s_b[w] = pb; s_t[w] = pt; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double sfb_all = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
+    const double sft_all = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
+    sc->block_counter = 0;
+    // curve record and stress
+    const double a1 = (double)sc->_1d_Area;
+    if (sc->curve_n < c.curve_cap) {
+        double* rec = d.curve + 3 * sc->curve_n;
+        rec[0] = (sc->size_d[2] - sc->sz0) / sc->sz0;
+        rec[1] = sfb_all * a1;
+        rec[2] = sft_all * a1;
+    }
+    sc->curve_n += 1;
+    sc->Stress = 0.5 * (fabs(sfb_all) + fabs(sft_all)) * a1;
+    if (!sc->Loading && sc->Stress > sc->MinStress) sc->Loading = 1;
+    if (sc->FractureStress < sc->Stress) {
+        sc->FractureStress = sc->Stress;
+        sc->FractureStrain = (sc->sz0 - sc->size_d[2]) / sc->sz0;
+    }
+    if (sc->Loading && sc->Stress < sc->ZeroStress) sc->Fracture = 1;
+    // CompressU / CompressB (md_data_types.h:223-293)
+    const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+    sc->V = (sc->Stress < 1e-9) ? 10.0 * sc->VLoad : sc->VLoad;
+    sc->size_d[ax] += sc->V * c.dt_d;
+    sc->Top += sc->V * c.dt_d;
+    sc->TopR = sc->Top - 2.0 * c.p_r_d;
+    sc->size[ax] = (float)sc->size_d[ax];
+    sc->sized2[ax] = (float)(0.5 * sc->size_d[ax]);
+    sc->center_d[ax] += sc->V * c.dt_d;
+    sc->center[ax] = (float)sc->center_d[ax];
+    sc->Hd2 = sc->sized2[ax];
+    sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
+    sc->steps += 1;
+    const bool running = (sc->Strain < sc->MaxStrain) && !sc->Fracture;
+    sc->done = running ? 0u : 1u;
+    const uint32_t mv = sc->moved;
+    sc->moved = 0;
+    sc->rebuild = mv;
+    if (c.use_graph) {
+        cudaGraphSetConditional(c.h_rebuild, mv ? 1u : 0u);
+        cudaGraphSetConditional(c.h_loop, (running && sc->steps < sc->target) ? 1u : 0u);
+    }
+}
+
+// Sets both graph conditions at the start of a launch.
+__global__ void k_prologue(Dev d, Consts c) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        DevScalars* sc = d.sc;
+        const bool go = !sc->done && sc->steps < sc->target;
+        if (c.use_graph) {
+            cudaGraphSetConditional(c.h_rebuild, (go && sc->rebuild) ? 1u : 0u);
+            cudaGraphSetConditional(c.h_loop, go ? 1u : 0u);
+        }
+    }
+}
+
+// On a plain stream: stop once the target step count is reached.
+__global__ void k_stream_gate(Dev d) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        DevScalars* sc = d.sc;
+        if (sc->steps >= sc->target) sc->done = sc->done | 2u;
+    }
+}
+__global__ void k_stream_ungate(Dev d) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) d.sc->done &= 1u;
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion (reference layout <-> engine layout)
+// ---------------------------------------------------------------------------
+__global__ void k_planar_to_f4(const float* __restrict__ R, uint32_t N, float4* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        out[i] = make_float4(R[i], R[i + N], R[i + 2 * (size_t)N], 0.f);
+}
+__global__ void k_f4_to_planar(const float4* __restrict__ in, uint32_t N, float* __restrict__ R) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float4 v = in[i];
+        R[i] = v.x; R[i + N] = v.y; R[i + 2 * (size_t)N] = v.z;
+    }
+}
+
+// Reference-layout rows (uint_fast32_t ids, AoS float3 state) -> engine rows.
+__global__ void k_rows_import(const uint_fast32_t* __restrict__ IL, const uint8_t* __restrict__ type,
+                              const float* __restrict__ iL, const rf_float3* __restrict__ Rij,
+                              const rf_float3* __restrict__ Oijt, const rf_float3* __restrict__ Mijn,
+                              const rf_float3* __restrict__ Mijt, Dev d, Consts c) {
+    const uint_fast32_t E = empty_id<uint_fast32_t>();
+    const size_t ps = (size_t)c.K * c.N;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        uint32_t live = 0, bond = 0, cm = 0;
+        for (uint32_t k = 0; k < c.K; ++k) {
+            const size_t r = (size_t)i * c.K + k, s = (size_t)k * c.N + i;
+            const uint_fast32_t j = IL[r];
+            d.ids[s] = (j == E || j >= c.N) ? EMPTY32 : (uint32_t)j;
+            d.il[s] = iL[r];
+            float* p0 = d.st + s;
+            p0[0] = Rij[r].x; p0[ps] = Rij[r].y; p0[2 * ps] = Rij[r].z;
+            p0[3 * ps] = Oijt[r].x; p0[4 * ps] = Oijt[r].y; p0[5 * ps] = Oijt[r].z;
+            p0[6 * ps] = Mijn[r].x; p0[7 * ps] = Mijn[r].y; p0[8 * ps] = Mijn[r].z;
+            p0[9 * ps] = Mijt[r].x; p0[10 * ps] = Mijt[r].y; p0[11 * ps] = Mijt[r].z;
+            if (j != E && j < c.N) {
+                live |= 1u << k;
+                if (type[r] == 1) bond |= 1u << k;
+                else if (Oijt[r].x != 0.f || Oijt[r].y != 0.f || Oijt[r].z != 0.f) cm |= 1u << k;
+            }
+        }
+        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm;
+    }
+}
+
+__global__ void k_rows_export(uint_fast32_t* __restrict__ IL, uint8_t* __restrict__ type, float* __restrict__ iL,
+                              rf_float3* __restrict__ Rij, rf_float3* __restrict__ Oijt, rf_float3* __restrict__ Mijn,
+                              rf_float3* __restrict__ Mijt, Dev d, Consts c) {
+    const uint_fast32_t E = empty_id<uint_fast32_t>();
+    const size_t ps = (size_t)c.K * c.N;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        const uint32_t live = d.live[i], bond = d.bond[i];
+        for (uint32_t k = 0; k < c.K; ++k) {
+            const size_t r = (size_t)i * c.K + k, s = (size_t)k * c.N + i;
+            IL[r] = ((live >> k) & 1u) ? (uint_fast32_t)d.ids[s] : E;
+            type[r] = (uint8_t)((bond >> k) & 1u);
+            iL[r] = d.il[s];
+            const float* p0 = d.st + s;
+            Rij[r].x = p0[0]; Rij[r].y = p0[ps]; Rij[r].z = p0[2 * ps];
+            Oijt[r].x = p0[3 * ps]; Oijt[r].y = p0[4 * ps]; Oijt[r].z = p0[5 * ps];
+            Mijn[r].x = p0[6 * ps]; Mijn[r].y = p0[7 * ps]; Mijn[r].z = p0[8 * ps];
+            Mijt[r].x = p0[9 * ps]; Mijt[r].y = p0[10 * ps]; Mijt[r].z = p0[11 * ps];
+        }
+    }
+}
+
+__global__ void k_counters(Dev d, Consts c, unsigned long long* out) {
+    unsigned long long nb = 0, nc = 0, nl = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        const uint32_t l = d.live[i], b = d.bond[i];
+        nl += __popc(l); nb += __popc(b); nc += __popc(d.cmask[i]);
+    }
+    atomicAdd(&out[0], nb); atomicAdd(&out[1], nc); atomicAdd(&out[2], nl);
+}
+
+
+__global__ void k_set_target(DevScalars* sc, unsigned long long n) { sc->target = sc->steps + n; }
+__global__ void k_force_rebuild(DevScalars* sc) { sc->rebuild = 1u; }
+__global__ void k_planar_to_cur(const float* __restrict__ R, Dev d) {
+    float4* out = d.pos[d.sc->steps & 1ull];
+    const uint32_t N = (uint32_t)(d.n_particles);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+        out[i] = make_float4(R[i], R[i + N], R[i + 2 * (size_t)N], 0.f);
+    if (blockIdx.x == 0 && threadIdx.x == 0) d.sc->rebuild = 1u;
+}
+__global__ void k_cur_to_planar(Dev d, float* __restrict__ R) {
+    const float4* in = d.pos[d.sc->steps & 1ull];
+    const uint32_t N = (uint32_t)(d.n_particles);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float4 v = in[i];
+        R[i] = v.x; R[i + N] = v.y; R[i + 2 * (size_t)N] = v.z;
+    }
+}
+
+}  // namespace rf
+
+using namespace rf;
+
+struct rf_engine {
+    rf_task task;
+    Dev d;
+    Consts c;
+    int device;
+    cudaStream_t stream;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    uint32_t nblocks;
+    uint32_t cg_nb;
+    bool graph_ok;
+    std::vector<void*> allocs;
+    unsigned long long* counters_dev;
+    float* staging;
+    uint64_t bonds_initial;
+};
+
+namespace {
+
+template <class T> rf_status dalloc(rf_engine* e, T** p, size_t n) {
+    void* q = nullptr;
+    RF_CUDA(cudaMalloc(&q, (n ? n : 1) * sizeof(T)));
+    e->allocs.push_back(q);
+    *p = (T*)q;
+    return RF_OK;
+}
+
+#define TRY(x) do { rf_status s__ = (x); if (s__ != RF_OK) return s__; } while (0)
+
+rf_status build_graph(rf_engine* e) {
+    cudaGraph_t g;
+    RF_CUDA(cudaGraphCreate(&g, 0));
+    e->graph = g;
+    RF_CUDA(cudaGraphConditionalHandleCreate(&e->c.h_loop, g, 0, 0));
+    RF_CUDA(cudaGraphConditionalHandleCreate(&e->c.h_rebuild, g, 0, 0));
+    e->c.use_graph = 1;
+    Dev d = e->d;
+    Consts c = e->c;
+    void* args[] = {&d, &c};
+    auto kparams = [&](void* fn, unsigned grid, unsigned block) {
+        cudaKernelNodeParams kp = {};
+        kp.func = fn; kp.gridDim = dim3(grid); kp.blockDim = dim3(block);
+        kp.sharedMemBytes = 0; kp.kernelParams = args; kp.extra = nullptr;
+        return kp;
+    };
+    // prologue -> WHILE
+    cudaGraphNode_t pro;
+    cudaKernelNodeParams kp = kparams((void*)k_prologue, 1, 32);
+    RF_CUDA(cudaGraphAddKernelNode(&pro, g, nullptr, 0, &kp));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = e->c.h_loop;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    RF_CUDA(cudaGraphAddNode(&wnode, g, &pro, 1, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    // IF(rebuild) inside the loop body
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = e->c.h_rebuild;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    RF_CUDA(cudaGraphAddNode(&inode, body, nullptr, 0, &ip));
+    cudaGraph_t rb = ip.conditional.phGraph_out[0];
+    const unsigned gN = (e->c.N + 255) / 256;
+    const unsigned gC = (e->c.cg_cells + 1 + 255) / 256;
+    struct { void* fn; unsigned grid, block; } seq[] = {
+        {(void*)k_rb_zero, gC, 256},      {(void*)k_rb_bin, gN, 256},
+        {(void*)k_rb_scan_sums, e->cg_nb, 1024}, {(void*)k_rb_scan_totals, 1, 32},
+        {(void*)k_rb_scan_apply, e->cg_nb, 1024}, {(void*)k_rb_scatter, gN, 256},
+        {(void*)k_rb_cand, (e->c.N + 127) / 128, 128},
+    };
+    cudaGraphNode_t prev = nullptr;
+    for (auto& s : seq) {
+        cudaGraphNode_t n;
+        kp = kparams(s.fn, s.grid, s.block);
+        RF_CUDA(cudaGraphAddKernelNode(&n, rb, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
+        prev = n;
+    }
+    cudaGraphNode_t step;
+    void* fn = (e->task.kind == RF_TEST_BRAZIL) ? (void*)k_step<RF_TEST_BRAZIL> : (void*)k_step<RF_TEST_UNIAXIAL>;
+    kp = kparams(fn, e->nblocks, 128);
+    RF_CUDA(cudaGraphAddKernelNode(&step, body, &inode, 1, &kp));
+    RF_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
+    return RF_OK;
+}
+
+rf_status launch_stream_steps(rf_engine* e, uint64_t nsteps) {
+    Dev d = e->d;
+    Consts c = e->c;
+    c.use_graph = 0;
+    const unsigned gN = (c.N + 255) / 256, gC = (c.cg_cells + 1 + 255) / 256;
+    cudaStream_t s = e->stream;
+    for (uint64_t q = 0; q < nsteps; ++q) {
+        k_stream_gate<<<1, 32, 0, s>>>(d);
+        k_rb_zero<<<gC, 256, 0, s>>>(d, c);
+        k_rb_bin<<<gN, 256, 0, s>>>(d, c);
+        k_rb_scan_sums<<<e->cg_nb, 1024, 0, s>>>(d, c);
+        k_rb_scan_totals<<<1, 32, 0, s>>>(d, c);
+        k_rb_scan_apply<<<e->cg_nb, 1024, 0, s>>>(d, c);
+        k_rb_scatter<<<gN, 256, 0, s>>>(d, c);
+        k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
+        if (e->task.kind == RF_TEST_BRAZIL) k_step<RF_TEST_BRAZIL><<<e->nblocks, 128, 0, s>>>(d, c);
+        else k_step<RF_TEST_UNIAXIAL><<<e->nblocks, 128, 0, s>>>(d, c);
+        k_stream_ungate<<<1, 32, 0, s>>>(d);
+    }
+    RF_CHECK_LAUNCH("engine stream steps");
+    return RF_OK;
+}
+
+}  // namespace
+
+// Host-side helpers from the md_* layer.
+extern "C" size_t md_CellDistributionScratchBytes(uint_fast32_t N, uint_fast32_t CN);
+
+extern "C" {
+
+rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) {
+    if (!t || !h_R || !out || t->N == 0 || t->K == 0) { set_error("rf_engine_create: bad arguments"); return RF_ERR_INVALID; }
+    if (t->K > 32) { set_error("rf_engine_create: the engine keeps slot masks in 32 bits (K <= 32), got K=%u", t->K); return RF_ERR_INVALID; }
+    if (t->N >= 0xFFFFFFFFull) { set_error("rf_engine_create: N too large"); return RF_ERR_INVALID; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("rf_engine_create: no CUDA device"); return RF_ERR_NO_DEVICE; }
+    rf_engine* e = new rf_engine();
+    std::memset(&e->d, 0, sizeof(e->d));
+    std::memset(&e->c, 0, sizeof(e->c));
+    e->task = *t;
+    e->graph = nullptr; e->exec = nullptr; e->graph_ok = false; e->staging = nullptr; e->bonds_initial = 0;
+    e->stream = nullptr; e->counters_dev = nullptr;
+    cudaGetDevice(&e->device);
+    rf_status st = RF_OK;
+    auto fail = [&](rf_status s) { rf_engine_destroy(e); return s; };
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(RF_ERR_CUDA);
+
+    const uint32_t N = (uint32_t)t->N, K = t->K;
+    Consts& c = e->c;
+    c.N = N; c.K = K; c.KC = 64; c.kind = t->kind;
+    const rf_potential& P = t->Po;
+    c.dt_d = P.dt; c.p_r_d = P.p_r;
+    c.bp = BondParams{(float)P.dt, (float)P.m_E, (float)P.m_G, (float)P.b_r, (float)P.m_Ec, (float)P.m_Gc};
+    c.cp = ContactParams{(float)P.dt, (float)P.hm_E, (float)P.hm_G, (float)P.p_A, (float)P.p_mu, (float)P.p_mur,
+                         (float)P.p_m, (float)P.p_r};
+    c.dtm = (float)P.dt_d_m; c.dt = (float)P.dt; c.dtI = (float)P.dt_d_I;
+    c.aacut = t->aacut; c.aa_farcut = (float)P.aa_farcut;
+    c.g.a = t->C.a; c.g.inv_a = t->C._1d_a; c.g.nx = t->C.Nr.x; c.g.ny = t->C.Nr.y; c.g.nz = t->C.Nr.z; c.g.CN = t->C.N;
+    c.zcut = (t->kind == RF_TEST_BRAZIL) ? (float)((double)t->S.center.y + (double)t->S.spacesized2.y)
+                                         : (float)((double)t->S.center.z + (double)t->S.spacesized2.z);
+    c.box_c = t->S.center; c.box_h = t->S.spacesized2; c.hp = t->S.hidenpoint;
+    // candidate grid over the cut box, one cell of margin each side; cell >= rc
+    const double acut = std::sqrt((double)t->aacut);
+    const double skin = 0.1 * acut;
+    const double rc = acut + skin;
+    c.rc2 = (float)(rc * rc);
+    c.disp2 = (float)((0.45 * skin) * (0.45 * skin));
+    const double hcell = rc * 1.0001;
+    c.cg_inv_h = (float)(1.0 / hcell);
+    c.cg_ox = (float)(t->S.center.x - t->S.spacesized2.x - hcell);
+    c.cg_oy = (float)(t->S.center.y - t->S.spacesized2.y - hcell);
+    c.cg_oz = (float)(t->S.center.z - t->S.spacesized2.z - hcell);
+    c.cg_nx = (uint32_t)std::ceil((2.0 * t->S.spacesized2.x + 2 * hcell) / hcell) + 1;
+    c.cg_ny = (uint32_t)std::ceil((2.0 * t->S.spacesized2.y + 2 * hcell) / hcell) + 1;
+    c.cg_nz = (uint32_t)std::ceil((2.0 * t->S.spacesized2.z + 2 * hcell) / hcell) + 1;
+    const uint64_t cells = (uint64_t)c.cg_nx * c.cg_ny * c.cg_nz;
+    if (cells >= 0x7FFFFFFFull) { set_error("rf_engine_create: candidate grid too large"); return fail(RF_ERR_INVALID); }
+    c.cg_cells = (uint32_t)cells;
+    e->cg_nb = (uint32_t)((cells + 1 + 4095) / 4096);
+    c.curve_cap = 1u << 20;
+    e->nblocks = (N + 127) / 128;
+
+    Dev& d = e->d;
+    d.n_particles = N;
+    const size_t NK = (size_t)N * K;
+    for (int b = 0; b < 2; ++b) {
+        if ((st = dalloc(e, &d.pos[b], N)) || (st = dalloc(e, &d.vel[b], N)) || (st = dalloc(e, &d.ang[b], N)))
+            return fail(st);
+    }
+    if ((st = dalloc(e, &d.ids, NK)) || (st = dalloc(e, &d.il, NK)) || (st = dalloc(e, &d.st, 12 * NK)) ||
+        (st = dalloc(e, &d.live, N)) || (st = dalloc(e, &d.bond, N)) || (st = dalloc(e, &d.cmask, N)) ||
+        (st = dalloc(e, &d.cand, (size_t)c.KC * N)) || (st = dalloc(e, &d.cand_n, N)) || (st = dalloc(e, &d.member, N)) ||
+        (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
+        (st = dalloc(e, &d.cg_start, cells + 1)) || (st = dalloc(e, &d.cg_fill, cells + 1)) ||
+        (st = dalloc(e, &d.cg_bsum, e->cg_nb)) || (st = dalloc(e, &d.cg_sorted, N)) ||
+        (st = dalloc(e, &d.partial, e->nblocks)) || (st = dalloc(e, &d.curve, 3 * (size_t)c.curve_cap)) ||
+        (st = dalloc(e, &d.sc, 1)) || (st = dalloc(e, &e->counters_dev, 4)))
+        return fail(st);
+    cudaStream_t s = e->stream;
+    for (int b = 0; b < 2; ++b) {
+        if (cudaMemsetAsync(d.vel[b], 0, N * sizeof(float4), s) || cudaMemsetAsync(d.ang[b], 0, N * sizeof(float4), s))
+            return fail(cuda_status(cudaGetLastError(), "memset"));
+    }
+    if (cudaMemsetAsync(d.st, 0, 12 * NK * sizeof(float), s) || cudaMemsetAsync(d.il, 0, NK * sizeof(float), s) ||
+        cudaMemsetAsync(d.member, 0, N * sizeof(unsigned long long), s) || cudaMemsetAsync(d.cand_n, 0, N * 4, s))
+        return fail(RF_ERR_CUDA);
+
+    // Initial rows exactly as the drivers build them (md_calculationbraziltest.cu:132-144),
+    // with the md_* kernels on temporary reference-layout buffers.
+    {
+        float *dR = nullptr, *dV = nullptr, *dIL_f = nullptr;
+        uint_fast32_t *dCI = nullptr, *dCIs = nullptr, *dpnC = nullptr, *dIL = nullptr;
+        uint8_t* dT = nullptr;
+        rf_float3* dS = nullptr;
+        void* scratch = nullptr;
+        const size_t sb = md_CellDistributionScratchBytes(N, t->C.N);
+        cudaError_t ce = cudaSuccess;
+        ce = cudaMalloc(&dR, 3 * (size_t)N * sizeof(float));
+        if (!ce) ce = cudaMalloc(&dV, 3 * (size_t)N * sizeof(float));
+        if (!ce) ce = cudaMalloc(&dCI, N * sizeof(uint_fast32_t));
+        if (!ce) ce = cudaMalloc(&dCIs, 2 * (size_t)N * sizeof(uint_fast32_t));
+        if (!ce) ce = cudaMalloc(&dpnC, 2 * t->C.N * sizeof(uint_fast32_t));
+        if (!ce) ce = cudaMalloc(&dIL, NK * sizeof(uint_fast32_t));
+        if (!ce) ce = cudaMalloc(&dT, NK);
+        if (!ce) ce = cudaMalloc(&dIL_f, NK * sizeof(float));
+        if (!ce) ce = cudaMalloc(&dS, 7 * NK * sizeof(rf_float3));
+        if (!ce) ce = cudaMalloc(&scratch, sb);
+        if (!ce) ce = cudaMemcpyAsync(dR, h_R, 3 * (size_t)N * sizeof(float), cudaMemcpyHostToDevice, s);
+        if (!ce) ce = cudaMemsetAsync(dV, 0, 3 * (size_t)N * sizeof(float), s);
+        if (!ce) ce = cudaMemsetAsync(dT, 0, NK, s);
+        if (!ce) ce = cudaMemsetAsync(dIL_f, 0, NK * sizeof(float), s);
+        if (!ce) ce = cudaMemsetAsync(dS, 0, 7 * NK * sizeof(rf_float3), s);
+        rf_status st2 = ce ? cuda_status(ce, "engine init buffers") : RF_OK;
+        rf_float3 *Rij = dS, *Oijt = dS + NK, *Fijn = dS + 2 * NK, *Fijt = dS + 3 * NK, *Mijn = dS + 4 * NK,
+                  *Mijt = dS + 5 * NK, *Mijadd = dS + 6 * NK;
+        rf_status init_dev = RF_OK;
+        if (!st2) {
+            rf_status a = md_CellDistribution(dR, N, dCI, dCIs, dpnC, t->C.N, t->C._1d_a, t->C.Nr, scratch, sb, s);
+            if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a) init_dev = a;
+        }
+        if (!st2) {
+            rf_status a = md_InteractionListConstruct(dR, N, dCIs, dpnC, dIL, K, t->C.a, t->C._1d_a, t->aacut,
+                                                      t->C.Nr, t->C.N, s);
+            if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a && !init_dev) init_dev = a;
+        }
+        if (!st2) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
+                                                      Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
+        if (!st2) st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
+                                          (float)P.aa_farcut, s);
+        if (!st2) {
+            k_planar_to_f4<<<(N + 255) / 256, 256, 0, s>>>(dR, N, d.pos[0]);
+            k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dIL_f, Rij, Oijt, Mijn, Mijt, d, c);
+            ce = cudaGetLastError();
+            if (ce) st2 = cuda_status(ce, "engine import");
+        }
+        if (!st2) { ce = cudaStreamSynchronize(s); if (ce) st2 = cuda_status(ce, "engine init"); }
+        cudaFree(dR); cudaFree(dV); cudaFree(dCI); cudaFree(dCIs); cudaFree(dpnC); cudaFree(dIL); cudaFree(dT);
+        cudaFree(dIL_f); cudaFree(dS); cudaFree(scratch);
+        if (st2) return fail(st2);
+        st = init_dev;
+    }
+
+    // scalar state
+    DevScalars h;
+    std::memset(&h, 0, sizeof(h));
+    const rf_compression& K_ = t->Compress;
+    h.V = K_.V; h.VLoad = K_.VLoad; h.Top = K_.Top; h.Bottom = K_.Bottom; h.TopR = K_.TopR; h.BottomR = K_.BottomR;
+    h.FractureStress = K_.FractureStress; h.FractureStrain = K_.FractureStrain; h.MinStress = K_.MinStress;
+    h.ZeroStress = K_.ZeroStress; h.Stress = K_.Stress; h.Strain = K_.Strain; h.MaxStrain = K_.MaxStrain;
+    h.Size0 = K_.Size0;
+    h.size_d[0] = K_.size_d.x; h.size_d[1] = K_.size_d.y; h.size_d[2] = K_.size_d.z;
+    h.center_d[0] = K_.center_d.x; h.center_d[1] = K_.center_d.y; h.center_d[2] = K_.center_d.z;
+    h.sz0 = t->sz0 != 0.0 ? t->sz0 : (double)K_.size.z;
+    h.center[0] = K_.center.x; h.center[1] = K_.center.y; h.center[2] = K_.center.z;
+    h.size[0] = K_.size.x; h.size[1] = K_.size.y; h.size[2] = K_.size.z;
+    h.sized2[0] = K_.sized2.x; h.sized2[1] = K_.sized2.y; h.sized2[2] = K_.sized2.z;
+    h.RR = K_.RR; h._1d_Area = K_._1d_Area; h.Hd2 = K_.Hd2;
+    h.Loading = K_.Loading; h.Fracture = K_.Fracture;
+    h.done = (K_.Strain < K_.MaxStrain && !K_.Fracture) ? 0u : 1u;
+    h.rebuild = 1;
+    h.err = (uint32_t)st;
+    if (cudaMemcpyAsync(d.sc, &h, sizeof(h), cudaMemcpyHostToDevice, s) || cudaStreamSynchronize(s))
+        return fail(RF_ERR_CUDA);
+
+    {
+        uint64_t cnt[5];
+        if (rf_engine_counters(e, cnt, 5) == RF_OK) e->bonds_initial = cnt[2];
+    }
+    // graph with device-driven loop; fall back to plain stream launches if unavailable
+    if (!getenv("RF_ENGINE_NO_GRAPH")) {
+        rf_status gs = build_graph(e);
+        if (gs == RF_OK) e->graph_ok = true;
+        else { cudaGetLastError(); e->c.use_graph = 0; }
+    }
+    *out = e;
+    return RF_OK;
+}
+
+rf_status rf_engine_destroy(rf_engine* e) {
+    if (!e) return RF_OK;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    if (e->graph) cudaGraphDestroy(e->graph);
+    for (void* p : e->allocs) cudaFree(p);
+    if (e->staging) cudaFree(e->staging);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    delete e;
+    return RF_OK;
+}
+
+rf_status rf_engine_step(rf_engine* e, uint64_t nsteps) {
+    if (!e) { set_error("rf_engine_step: null engine"); return RF_ERR_INVALID; }
+    if (nsteps == 0) return RF_OK;
+    k_set_target<<<1, 1, 0, e->stream>>>(e->d.sc, (unsigned long long)nsteps);
+    RF_CHECK_LAUNCH("k_set_target");
+    if (e->graph_ok) {
+        RF_CUDA(cudaGraphLaunch(e->exec, e->stream));
+        return RF_OK;
+    }
+    return launch_stream_steps(e, nsteps);
+}
+
+rf_status rf_engine_step_host(rf_engine* e, const float* h_R_in, uint64_t nsteps, float* h_R_out) {
+    if (!e) { set_error("rf_engine_step_host: null engine"); return RF_ERR_INVALID; }
+    const uint32_t N = e->c.N;
+    cudaStream_t s = e->stream;
+    if (!e->staging) RF_CUDA(cudaMalloc(&e->staging, 3 * (size_t)N * sizeof(float)));
+    if (h_R_in) {
+        RF_CUDA(cudaMemcpyAsync(e->staging, h_R_in, 3 * (size_t)N * sizeof(float), cudaMemcpyHostToDevice, s));
+        k_planar_to_cur<<<(N + 255) / 256, 256, 0, s>>>(e->staging, e->d);
+        RF_CHECK_LAUNCH("k_planar_to_cur");
+    }
+    rf_status st = rf_engine_step(e, nsteps);
+    if (st) return st;
+    if (h_R_out) {
+        k_cur_to_planar<<<(N + 255) / 256, 256, 0, s>>>(e->d, e->staging);
+        RF_CHECK_LAUNCH("k_cur_to_planar");
+        RF_CUDA(cudaMemcpyAsync(h_R_out, e->staging, 3 * (size_t)N * sizeof(float), cudaMemcpyDeviceToHost, s));
+        RF_CUDA(cudaStreamSynchronize(s));
+    }
+    return RF_OK;
+}
+
+rf_status rf_engine_sync(rf_engine* e, rf_task* t_out, rf_run_result* r_out) {
+    if (!e) { set_error("rf_engine_sync: null engine"); return RF_ERR_INVALID; }
+    DevScalars h;
+    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+    RF_CUDA(cudaStreamSynchronize(e->stream));
+    if (t_out) {
+        *t_out = e->task;
+        rf_compression& K = t_out->Compress;
+        K.V = h.V; K.Top = h.Top; K.Bottom = h.Bottom; K.TopR = h.TopR; K.BottomR = h.BottomR;
+        K.FractureStress = h.FractureStress; K.FractureStrain = h.FractureStrain; K.Stress = h.Stress;
+        K.Strain = h.Strain; K.Loading = h.Loading; K.Fracture = h.Fracture; K.Hd2 = h.Hd2;
+        K.size_d = rf_double3{h.size_d[0], h.size_d[1], h.size_d[2]};
+        K.center_d = rf_double3{h.center_d[0], h.center_d[1], h.center_d[2]};
+        K.size = rf_float3{h.size[0], h.size[1], h.size[2]};
+        K.sized2 = rf_float3{h.sized2[0], h.sized2[1], h.sized2[2]};
+        K.center = rf_float3{h.center[0], h.center[1], h.center[2]};
+    }
+    if (r_out) {
+        r_out->steps = h.steps;
+        r_out->FractureStress = h.FractureStress; r_out->FractureStrain = h.FractureStrain;
+        r_out->Stress = h.Stress; r_out->Strain = h.Strain; r_out->Fracture = h.Fracture;
+        r_out->broken_bonds = h.broken;
+        r_out->bonds_initial = e->bonds_initial;
+        r_out->error = (rf_status)h.err;
+    }
+    return RF_OK;
+}
+
+rf_status rf_engine_export(rf_engine* e, float* R, float* V, float* W, uint_fast32_t* IL, uint8_t* ILtype,
+                           float* _1d_iL, rf_float3* Rij, rf_float3* Oijt, rf_float3* Mijn, rf_float3* Mijt) {
+    if (!e) { set_error("rf_engine_export: null engine"); return RF_ERR_INVALID; }
+    const uint32_t N = e->c.N, K = e->c.K;
+    const size_t NK = (size_t)N * K;
+    cudaStream_t s = e->stream;
+    RF_CUDA(cudaStreamSynchronize(s));
+    DevScalars h;
+    RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
+    const int cur = (int)(h.steps & 1ull);
+    if (!e->staging) RF_CUDA(cudaMalloc(&e->staging, 3 * (size_t)N * sizeof(float)));
+    const float4* vecs[3] = {e->d.pos[cur], e->d.vel[cur], e->d.ang[cur]};
+    float* outs[3] = {R, V, W};
+    for (int q = 0; q < 3; ++q) {
+        if (!outs[q]) continue;
+        k_f4_to_planar<<<(N + 255) / 256, 256, 0, s>>>(vecs[q], N, e->staging);
+        RF_CHECK_LAUNCH("k_f4_to_planar");
+        RF_CUDA(cudaMemcpyAsync(outs[q], e->staging, 3 * (size_t)N * sizeof(float), cudaMemcpyDeviceToHost, s));
+        RF_CUDA(cudaStreamSynchronize(s));
+    }
+    if (IL || ILtype || _1d_iL || Rij || Oijt || Mijn || Mijt) {
+        uint_fast32_t* dIL = nullptr; uint8_t* dT = nullptr; float* dL = nullptr; rf_float3* dS = nullptr;
+        cudaError_t ce = cudaMalloc(&dIL, NK * sizeof(uint_fast32_t));
+        if (!ce) ce = cudaMalloc(&dT, NK);
+        if (!ce) ce = cudaMalloc(&dL, NK * sizeof(float));
+        if (!ce) ce = cudaMalloc(&dS, 4 * NK * sizeof(rf_float3));
+        if (!ce) {
+            k_rows_export<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dL, dS, dS + NK, dS + 2 * NK, dS + 3 * NK, e->d, e->c);
+            ce = cudaGetLastError();
+        }
+        if (!ce && IL) ce = cudaMemcpyAsync(IL, dIL, NK * sizeof(uint_fast32_t), cudaMemcpyDeviceToHost, s);
+        if (!ce && ILtype) ce = cudaMemcpyAsync(ILtype, dT, NK, cudaMemcpyDeviceToHost, s);
+        if (!ce && _1d_iL) ce = cudaMemcpyAsync(_1d_iL, dL, NK * sizeof(float), cudaMemcpyDeviceToHost, s);
+        rf_float3* outs3[4] = {Rij, Oijt, Mijn, Mijt};
+        for (int q = 0; q < 4 && !ce; ++q)
+            if (outs3[q]) ce = cudaMemcpyAsync(outs3[q], dS + q * NK, NK * sizeof(rf_float3), cudaMemcpyDeviceToHost, s);
+        if (!ce) ce = cudaStreamSynchronize(s);
+        cudaFree(dIL); cudaFree(dT); cudaFree(dL); cudaFree(dS);
+        if (ce) return cuda_status(ce, "rf_engine_export");
+    }
+    return RF_OK;
+}
+
+rf_status rf_engine_import(rf_engine* e, const float* R, const float* V, const float* W, const uint_fast32_t* IL,
+                           const uint8_t* ILtype, const float* _1d_iL, const rf_float3* Rij, const rf_float3* Oijt,
+                           const rf_float3* Mijn, const rf_float3* Mijt) {
+    if (!e || !R || !V || !W || !IL || !ILtype || !_1d_iL || !Rij || !Oijt || !Mijn || !Mijt) {
+        set_error("rf_engine_import: bad arguments");
+        return RF_ERR_INVALID;
+    }
+    const uint32_t N = e->c.N, K = e->c.K;
+    const size_t NK = (size_t)N * K;
+    cudaStream_t s = e->stream;
+    RF_CUDA(cudaStreamSynchronize(s));
+    DevScalars h;
+    RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
+    const int cur = (int)(h.steps & 1ull);
+    if (!e->staging) RF_CUDA(cudaMalloc(&e->staging, 3 * (size_t)N * sizeof(float)));
+    const float* ins[3] = {R, V, W};
+    float4* vecs[3] = {e->d.pos[cur], e->d.vel[cur], e->d.ang[cur]};
+    for (int q = 0; q < 3; ++q) {
+        RF_CUDA(cudaMemcpyAsync(e->staging, ins[q], 3 * (size_t)N * sizeof(float), cudaMemcpyHostToDevice, s));
+        k_planar_to_f4<<<(N + 255) / 256, 256, 0, s>>>(e->staging, N, vecs[q]);
+        RF_CHECK_LAUNCH("k_planar_to_f4");
+        RF_CUDA(cudaStreamSynchronize(s));
+    }
+    uint_fast32_t* dIL = nullptr; uint8_t* dT = nullptr; float* dL = nullptr; rf_float3* dS = nullptr;
+    cudaError_t ce = cudaMalloc(&dIL, NK * sizeof(uint_fast32_t));
+    if (!ce) ce = cudaMalloc(&dT, NK);
+    if (!ce) ce = cudaMalloc(&dL, NK * sizeof(float));
+    if (!ce) ce = cudaMalloc(&dS, 4 * NK * sizeof(rf_float3));
+    if (!ce) ce = cudaMemcpyAsync(dIL, IL, NK * sizeof(uint_fast32_t), cudaMemcpyHostToDevice, s);
+    if (!ce) ce = cudaMemcpyAsync(dT, ILtype, NK, cudaMemcpyHostToDevice, s);
+    if (!ce) ce = cudaMemcpyAsync(dL, _1d_iL, NK * sizeof(float), cudaMemcpyHostToDevice, s);
+    const rf_float3* ins3[4] = {Rij, Oijt, Mijn, Mijt};
+    for (int q = 0; q < 4 && !ce; ++q)
+        ce = cudaMemcpyAsync(dS + q * NK, ins3[q], NK * sizeof(rf_float3), cudaMemcpyHostToDevice, s);
+    if (!ce) {
+        k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dL, dS, dS + NK, dS + 2 * NK, dS + 3 * NK, e->d, e->c);
+        ce = cudaGetLastError();
+    }
+    if (!ce) {
+        k_force_rebuild<<<1, 1, 0, s>>>(e->d.sc);
+        ce = cudaGetLastError();
+    }
+    if (!ce) ce = cudaStreamSynchronize(s);
+    cudaFree(dIL); cudaFree(dT); cudaFree(dL); cudaFree(dS);
+    if (ce) return cuda_status(ce, "rf_engine_import");
+    return RF_OK;
+}
+
+rf_status rf_engine_curve(rf_engine* e, double* curve, uint64_t cap, uint64_t* n) {
+    if (!e) { set_error("rf_engine_curve: null engine"); return RF_ERR_INVALID; }
+    DevScalars h;
+    RF_CUDA(cudaStreamSynchronize(e->stream));
+    RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
+    uint64_t m = h.curve_n < e->c.curve_cap ? h.curve_n : e->c.curve_cap;
+    if (n) *n = h.curve_n;
+    if (curve && cap) {
+        if (m > cap) m = cap;
+        RF_CUDA(cudaMemcpy(curve, e->d.curve, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return RF_OK;
+}
+
+rf_status rf_engine_counters(rf_engine* e, uint64_t* out, int n) {
+    if (!e || !out || n <= 0) { set_error("rf_engine_counters: bad arguments"); return RF_ERR_INVALID; }
+    cudaStream_t s = e->stream;
+    RF_CUDA(cudaMemsetAsync(e->counters_dev, 0, 4 * sizeof(unsigned long long), s));
+    k_counters<<<148 * 4, 256, 0, s>>>(e->d, e->c, e->counters_dev);
+    RF_CHECK_LAUNCH("k_counters");
+    unsigned long long cnt[4];
+    DevScalars h;
+    RF_CUDA(cudaMemcpyAsync(cnt, e->counters_dev, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    const uint64_t v[5] = {h.steps, h.rebuilds, cnt[0], cnt[1], cnt[2]};
+    for (int q = 0; q < n && q < 5; ++q) out[q] = v[q];
+    return RF_OK;
+}
+
+int rf_engine_launches_per_step(void) { return 1; }
+rf_stream rf_engine_stream(rf_engine* e) { return e ? (rf_stream)e->stream : nullptr; }
+int rf_engine_uses_graph(rf_engine* e) { return (e && e->graph_ok) ? 1 : 0; }
+
+}  // extern "C"

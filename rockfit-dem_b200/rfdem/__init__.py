@@ -1,0 +1,315 @@
+"""Python host mirror of the rockfit-b200 C ABI (include/rockfit_b200.h).
+
+The engine is the CUDA library ``rockfit-dem_b200/lib/librfdem.so``; this module
+only binds it with ctypes. There is no CPU fallback: importing the module raises
+if the library is missing, and every call raises ``RFError`` on a non-zero status.
+
+Units are the reference's (md_phys_constants.h): mm, mg, us; stress in 1e9 Pa.
+"""
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "librfdem.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("rockfit-b200 engine library not built: %s (run rockfit-dem_b200/build.py)" % LIB_PATH)
+lib = C.CDLL(LIB_PATH)
+
+STATUS = {0: "RF_OK", 1: "RF_ERR_INVALID", 2: "RF_ERR_CUDA", 3: "RF_ERR_ROW_OVERFLOW", 4: "RF_ERR_CELL_RANGE",
+          5: "RF_ERR_NOT_CONVERGED", 6: "RF_ERR_CAPACITY", 7: "RF_ERR_NO_DEVICE", 8: "RF_ERR_STATE"}
+RF_OK, RF_ERR_INVALID, RF_ERR_CUDA, RF_ERR_ROW_OVERFLOW, RF_ERR_CELL_RANGE = 0, 1, 2, 3, 4
+RF_TEST_UNIAXIAL, RF_TEST_BRAZIL = 0, 1
+
+
+class RFError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        super().__init__("%s: %s (%s)" % (what, STATUS.get(code, code), lib.rf_last_error_string().decode()))
+
+
+def check(code, what=""):
+    if code != 0:
+        raise RFError(code, what)
+    return code
+
+
+# --- structs (field for field with include/rockfit_b200.h) ------------------
+class f3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class u3(C.Structure):
+    _fields_ = [("x", C.c_uint), ("y", C.c_uint), ("z", C.c_uint)]
+
+
+class d3(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+
+_POT_IN = ["m_E", "m_nu", "m_Ec", "m_Gc", "m_ro", "b_r", "b_d", "p_r", "p_e", "p_mu", "p_mur", "a_farcut"]
+_POT_OUT = ["m_G", "b_S", "p_V", "p_m", "b_dd", "p_1d_m", "p_I", "hm_E", "hm_G", "p_A", "aa_farcut", "Trayleigh",
+            "Tsim", "dt", "D", "a", "_1d_a", "aa", "dt_d_m", "dt_d_I"]
+
+
+class Potential(C.Structure):
+    _fields_ = [(n, C.c_double) for n in _POT_IN + _POT_OUT]
+
+
+class Sample(C.Structure):
+    _fields_ = [("A_real", d3), ("B_real", d3), ("size_real", d3), ("center_real", d3), ("Vext", C.c_double)] + \
+               [(n, f3) for n in ["L", "A", "B", "axis", "center", "size", "sized2", "hidenpoint", "spacesize",
+                                  "spacesized2"]] + \
+               [("R0", C.c_float), ("H0", C.c_float), ("Vgenmax", C.c_float)]
+
+
+class Cells(C.Structure):
+    _fields_ = [("Nr", u3), ("N", C.c_uint64), ("a", C.c_float), ("_1d_a", C.c_float), ("_1d_Nr", f3)]
+
+
+class Compression(C.Structure):
+    _fields_ = [("Loading", C.c_int32), ("Fracture", C.c_int32), ("center", f3), ("size", f3), ("sized2", f3),
+                ("size_d", d3), ("center_d", d3)] + \
+               [(n, C.c_float) for n in ["R", "RR", "Hd2", "C", "mu", "Area", "_1d_Area"]] + \
+               [(n, C.c_double) for n in ["V", "VLoad", "Top", "Bottom", "TopR", "BottomR", "FractureStress",
+                                          "FractureStrain", "MinStress", "ZeroStress", "Stress", "Strain",
+                                          "MaxStrain", "Size0"]]
+
+
+class Task(C.Structure):
+    _fields_ = [("kind", C.c_int), ("N", C.c_uint64), ("K", C.c_uint32), ("acut", C.c_float), ("aacut", C.c_float),
+                ("Po", Potential), ("S", Sample), ("C", Cells), ("Compress", Compression), ("bloks", C.c_uint64),
+                ("sz0", C.c_double)]
+
+
+class RunResult(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("FractureStress", C.c_double), ("FractureStrain", C.c_double),
+                ("Stress", C.c_double), ("Strain", C.c_double), ("Fracture", C.c_int32),
+                ("broken_bonds", C.c_uint64), ("bonds_initial", C.c_uint64), ("error", C.c_int)]
+
+
+# --- prototypes ---------------------------------------------------------------
+P = C.c_void_p
+ID = C.c_uint64 if lib.rf_id_bytes() == 8 else C.c_uint32     # uint_fast32_t
+ID_NP = np.uint64 if lib.rf_id_bytes() == 8 else np.uint32
+EMPTY = np.iinfo(ID_NP).max
+u64, f32, f64, i32 = C.c_uint64, C.c_float, C.c_double, C.c_int
+_proto = {
+    "rf_last_error_string": (C.c_char_p, []),
+    "rf_version": (i32, []), "rf_id_bytes": (i32, []),
+    "rf_task_prepare": (i32, [C.POINTER(Task), P, P, f64, f64, f64, f64]),
+    "md_CompressU": (i32, [C.POINTER(Task), f64]), "md_CompressB": (i32, [C.POINTER(Task), f64]),
+    "md_SumForcesULoading": (i32, [C.POINTER(Task), P, u64, u64, u64, f64, P, P]),
+    "md_CalculateCellIndex": (i32, [P, ID, P, f32, u3, P]),
+    "md_CellDistributionScratchBytes": (C.c_size_t, [ID, ID]),
+    "md_CellDistribution": (i32, [P, ID, P, P, P, ID, f32, u3, P, C.c_size_t, P]),
+    "md_InteractionListConstruct": (i32, [P, ID, P, P, P, ID, f32, f32, f32, u3, ID, P]),
+    "md_InteractionListReConstructBPM": (i32, [P, ID, P, P, P, P, ID, f32, f32, f32, u3, ID, P]),
+    "md_DeleteFarLinks": (i32, [P, ID, P, P, P, P, P, P, P, P, P, P, ID, f32, P]),
+    "md_ConstructBoundInteractions": (i32, [P, P, P, P, P, P, P, P, P, P, P, P, P, ID, ID, f32, f32, P]),
+    "md_CalculateForcesDEM_22": (i32, [P, P, P, P, P, P, P, P, P, P, P, P, ID, ID, f32, f32, f32, f32, f32, f32, P]),
+    "md_CalculateForcesDEM_21": (i32, [P, P, P, P, P, P, P, P, P, P, ID, ID, f32, f32, f32, f32, f32, f32, f32, f32, P]),
+    "md_CalculateIncrementsDEM": (i32, [P, P, P, P, P, ID, f32, f32, f32, P]),
+    "md_braziltest_simple2": (i32, [P, P, P, P, ID, f3, f32, f32, f32, f32, f32, f32, f32, u64, P]),
+    "md_UniaxialCompression3_simple": (i32, [P, P, P, P, ID, f3, f32, f32, f32, f32, f32, f32, f32, u64, P]),
+    "md_ParallelepipedCutRestriction": (i32, [P, P, P, ID, f3, f3, f3, P]),
+    "md_CalculateIncrementsFIRE": (i32, [P, P, P, ID, f32, f32, f32, P]),
+    "md_CalculateDecrementsHalfStepFIRE": (i32, [P, P, ID, f32, P]),
+    "md_FdotVEntire": (i32, [P, P, P, u64, ID, P]),
+    "md_CalculationBrazilTest": (i32, [C.POINTER(Task), P, u64, P, u64, P, C.POINTER(RunResult)]),
+    "md_CalculationUniaxialCompression": (i32, [C.POINTER(Task), P, u64, P, u64, P, C.POINTER(RunResult)]),
+    "rf_engine_create": (i32, [C.POINTER(Task), P, C.POINTER(P)]),
+    "rf_engine_destroy": (i32, [P]),
+    "rf_engine_step": (i32, [P, u64]),
+    "rf_engine_step_host": (i32, [P, P, u64, P]),
+    "rf_engine_sync": (i32, [P, C.POINTER(Task), C.POINTER(RunResult)]),
+    "rf_engine_export": (i32, [P] + [P] * 10),
+    "rf_engine_import": (i32, [P] + [P] * 10),
+    "rf_engine_curve": (i32, [P, P, u64, P]),
+    "rf_engine_counters": (i32, [P, P, i32]),
+    "rf_engine_launches_per_step": (i32, []),
+    "rf_engine_stream": (P, [P]),
+    "rf_engine_uses_graph": (i32, [P]),
+    "rf_specimen_lattice_cylinder": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
+    "rf_specimen_lattice_disc": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
+}
+for _n, (_r, _a) in _proto.items():
+    _f = getattr(lib, _n)
+    _f.restype = _r
+    _f.argtypes = _a
+
+ABI_SYMBOLS = sorted(_proto)
+
+
+def ptr(a):
+    """Address of a numpy array, a torch tensor, or None."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+# --- reference parameter presets ----------------------------------------------
+LENGTH = 1e-3          # md_phys_constants.h: length_const
+STRESS = 1e9           # force_const / length_const^2 with force_const = 1e3
+
+
+def granite_potential():
+    """The reference's granite start point (mp_determineconjgradient.cu:15-38, :123-127), mm-mg-us units."""
+    po = Potential()
+    po.m_nu = 0.247
+    po.m_E = 1.95255e+11 / STRESS
+    po.m_Ec = 5.1447e+08 / STRESS
+    po.m_Gc = 3.7131e+08 / STRESS
+    po.m_ro = 2610 / 1e3
+    po.b_r = 0.5 * 0.000330015 / LENGTH
+    po.p_r = 0.5 * 0.001 / LENGTH
+    po.b_d = 2.0 * po.p_r + 5.93169e-05 / LENGTH
+    po.p_e = 0.6
+    po.p_mu = 0.45
+    po.p_mur = 0.05
+    po.a_farcut = 2.9 * po.p_r
+    return po
+
+
+def specimen_positions(kind, seed, p_r, diameter, height, center, gap_frac=0.02, jitter=0.02):
+    """Seeded jittered-lattice specimen (cylinder, or Brazilian disc with axis z), planar float32[3N]."""
+    fn = lib.rf_specimen_lattice_disc if kind == RF_TEST_BRAZIL else lib.rf_specimen_lattice_cylinder
+    c = (C.c_double * 3)(*center)
+    n = C.c_uint64(0)
+    check(fn(seed, p_r, gap_frac, jitter, diameter, height, c, None, 0, C.byref(n)), "specimen")
+    R = np.zeros(3 * n.value, np.float32)
+    check(fn(seed, p_r, gap_frac, jitter, diameter, height, c, R.ctypes.data, n.value, C.byref(n)), "specimen")
+    return R
+
+
+def lattice_extent(p_r, gap_frac, size):
+    """Particle-centre half extent the lattice generator realises for a specimen dimension."""
+    sp = 2.0 * p_r * (1.0 + gap_frac)
+    return math.floor((0.5 * size - p_r) / sp) * sp
+
+
+def make_test(kind, diameter, height, seed=0xB2000000, potential=None, K=32, gap_frac=0.02, jitter=0.02,
+              margin=None, v_load=None, min_stress=None, max_strain=0.1):
+    """A prepared task plus its seeded specimen: returns (Task, R planar float32).
+
+    kind: RF_TEST_UNIAXIAL (cylinder along z, platens on z) or RF_TEST_BRAZIL (disc of
+    thickness `height` along z, platens on y). Sizes in mm. Defaults follow the
+    reference's CG driver (mp_determineconjgradient.cu:79-80, :97-98).
+    """
+    po = potential or granite_potential()
+    p_r = po.p_r
+    ext_r = lattice_extent(p_r, gap_frac, diameter)
+    ext_z = lattice_extent(p_r, gap_frac, height)
+    # SetLSi takes the specimen size + 2 p_r and stores particle-centre extents L
+    # the platens start at the outermost particle centre (lattice extent + jitter)
+    L = [2 * ext_r + 2 * jitter * p_r, 2 * ext_r + 2 * jitter * p_r, 2 * ext_z + 2 * jitter * p_r]
+    if margin is None:
+        margin = 4.0 * p_r + 0.25 * max(L)
+    space = [L[0] + 2 * p_r + 2 * margin, L[1] + 2 * p_r + 2 * margin, L[2] + 2 * p_r + 2 * margin]
+    t = Task()
+    t.kind = kind
+    t.K = K
+    t.Po = po
+    if v_load is None:
+        v_load = (-10.0 if kind == RF_TEST_UNIAXIAL else -100.0) * 0.02 / 1e3
+    if min_stress is None:
+        min_stress = (15e6 if kind == RF_TEST_UNIAXIAL else 2.1e6) / STRESS
+    ss = (C.c_double * 3)(*[s * LENGTH for s in space])
+    ls = (C.c_double * 3)(*[(x + 2 * p_r) * LENGTH for x in L])
+    t.N = 1
+    check(lib.rf_task_prepare(C.byref(t), ss, ls, 2.0 * po.a_farcut, v_load, min_stress, max_strain), "rf_task_prepare")
+    ctr = (t.S.center.x, t.S.center.y, t.S.center.z)
+    R = specimen_positions(kind, seed, p_r, diameter, height, ctr, gap_frac, jitter)
+    t.N = R.size // 3
+    t.bloks = t.N // 1024 + 1
+    return t, R
+
+
+class Engine:
+    """The fused engine on the current CUDA device."""
+
+    def __init__(self, task, R):
+        self.task = task
+        self.N = int(task.N)
+        self.K = int(task.K)
+        R = np.ascontiguousarray(R, np.float32)
+        assert R.size == 3 * self.N
+        h = P()
+        check(lib.rf_engine_create(C.byref(task), R.ctypes.data, C.byref(h)), "rf_engine_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.rf_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n):
+        check(lib.rf_engine_step(self.h, n), "rf_engine_step")
+
+    def step_host(self, R_in, n, R_out):
+        check(lib.rf_engine_step_host(self.h, ptr(R_in), n, ptr(R_out)), "rf_engine_step_host")
+
+    def sync(self):
+        t = Task()
+        r = RunResult()
+        check(lib.rf_engine_sync(self.h, C.byref(t), C.byref(r)), "rf_engine_sync")
+        return t, r
+
+    def export(self):
+        N, K = self.N, self.K
+        out = dict(R=np.zeros(3 * N, np.float32), V=np.zeros(3 * N, np.float32), W=np.zeros(3 * N, np.float32),
+                   IL=np.zeros(N * K, ID_NP), ILtype=np.zeros(N * K, np.uint8), iL=np.zeros(N * K, np.float32),
+                   Rij=np.zeros(3 * N * K, np.float32), Oijt=np.zeros(3 * N * K, np.float32),
+                   Mijn=np.zeros(3 * N * K, np.float32), Mijt=np.zeros(3 * N * K, np.float32))
+        check(lib.rf_engine_export(self.h, *[ptr(out[k]) for k in
+                                             ["R", "V", "W", "IL", "ILtype", "iL", "Rij", "Oijt", "Mijn", "Mijt"]]),
+              "rf_engine_export")
+        return out
+
+    def load(self, st):
+        check(lib.rf_engine_import(self.h, *[ptr(np.ascontiguousarray(st[k])) for k in
+                                             ["R", "V", "W", "IL", "ILtype", "iL", "Rij", "Oijt", "Mijn", "Mijt"]]),
+              "rf_engine_import")
+
+    def curve(self):
+        n = C.c_uint64(0)
+        check(lib.rf_engine_curve(self.h, None, 0, C.byref(n)), "rf_engine_curve")
+        m = min(n.value, 1 << 20)
+        buf = np.zeros(3 * max(m, 1), np.float64)
+        check(lib.rf_engine_curve(self.h, buf.ctypes.data, m, C.byref(n)), "rf_engine_curve")
+        return buf[:3 * m].reshape(m, 3)
+
+    def stream(self):
+        return lib.rf_engine_stream(self.h)
+
+    def uses_graph(self):
+        return bool(lib.rf_engine_uses_graph(self.h))
+
+    def counters(self):
+        out = np.zeros(5, np.uint64)
+        check(lib.rf_engine_counters(self.h, out.ctypes.data, 5), "rf_engine_counters")
+        return dict(steps=int(out[0]), rebuilds=int(out[1]), bonds=int(out[2]), contacts=int(out[3]),
+                    occupied=int(out[4]))
+
+
+def run_test(task, R, max_steps=0, curve_cap=0, want_positions=False):
+    """md_CalculationBrazilTest / md_CalculationUniaxialCompression from host buffers."""
+    R = np.ascontiguousarray(R, np.float32)
+    curve = np.zeros(3 * max(curve_cap, 1), np.float64)
+    Rout = np.zeros_like(R) if want_positions else None
+    res = RunResult()
+    fn = lib.md_CalculationBrazilTest if task.kind == RF_TEST_BRAZIL else lib.md_CalculationUniaxialCompression
+    check(fn(C.byref(task), R.ctypes.data, max_steps, curve.ctypes.data if curve_cap else None, curve_cap,
+             ptr(Rout), C.byref(res)), "md_Calculation")
+    return res, curve[:3 * curve_cap].reshape(-1, 3), Rout

@@ -1,0 +1,172 @@
+"""The oracle and the engine against the reference's OWN kernels (compiled unmodified
+from its sources for sm_100a into oracle/_ref), on identical seeded inputs.
+
+Integer outputs (cells, rows, bond flags) must match bit for bit. Float outputs are
+compared within tolerance: the reference build lets nvcc contract a*b+c into FMAs
+and uses the library norm3df, while the oracle and engine evaluate each operation
+separately and use sqrt(x*x+y*y+z*z)."""
+import numpy as np
+import pytest
+
+import mdcall as mc
+import oracle
+import rfdem
+
+pytestmark = pytest.mark.gpu
+
+REF = oracle.ref_gpu()
+needs_ref = pytest.mark.skipif(REF is None, reason="oracle/_ref/libmdref_gpu.so not built")
+
+
+def ref_cells(t, R):
+    N, CN = R.size // 3, int(t.C.N)
+    CI, CIs, pnC = np.zeros(N, np.uint32), np.zeros(2 * N, np.uint32), np.zeros(2 * CN, np.uint32)
+    assert REF.ref_cell_distribution(R.ctypes.data, N, CI.ctypes.data, CIs.ctypes.data, pnC.ctypes.data, CN, t.C.a,
+                                     t.C._1d_a, t.C.Nr) == 0
+    return CI, CIs, pnC
+
+
+def to64(a):
+    out = a.astype(np.uint64)
+    out[a == np.uint32(0xFFFFFFFF)] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    return out
+
+
+def to32(a):
+    out = a.astype(np.uint32)
+    out[a == np.uint64(0xFFFFFFFFFFFFFFFF)] = np.uint32(0xFFFFFFFF)
+    return out
+
+
+@pytest.fixture(scope="module", params=[(0, 9.0, 14.0), (1, 16.0, 6.0), (0, 24.0, 40.0)],
+                ids=["uniaxial-1k", "brazil-1k", "uniaxial-18k"])
+def case(request):
+    kind, d, h = request.param
+    return rfdem.make_test(kind, d, h, seed=0xB2000000 + 31)
+
+
+@needs_ref
+def test_cells_and_rows_bitexact_vs_reference(cuda, case):
+    t, R = case
+    N, K = R.size // 3, int(t.K)
+    CI, CIs, pnC = ref_cells(t, R)
+    _, CIo, CIso, pnCo = mc.oracle_cells(t, R)
+    assert np.array_equal(to64(CI), CIo)
+    assert np.array_equal(to64(CIs), CIso)
+    assert np.array_equal(to64(pnC), pnCo)
+    IL = np.zeros(N * K, np.uint32)
+    assert REF.ref_list_construct(R.ctypes.data, N, K, int(t.C.N), t.C.a, t.C._1d_a, t.aacut, t.C.Nr,
+                                  IL.ctypes.data) == 0
+    _, ILo = mc.oracle_list_construct(t, R, CIso, pnCo)
+    assert np.array_equal(to64(IL), ILo)
+    # engine md_* path too
+    _, ILg = mc.gpu_list_construct(cuda, t, R, CIso, pnCo)
+    assert np.array_equal(ILg, ILo)
+
+
+@needs_ref
+def test_reconstruct_bitexact_vs_reference(cuda, case):
+    t, R = case
+    N, K = R.size // 3, int(t.K)
+    _, CI, CIs, pnC = mc.oracle_cells(t, R)
+    _, IL = mc.oracle_list_construct(t, R, CIs, pnC)
+    rng = np.random.default_rng(17)
+    holes = IL.copy()
+    live = np.nonzero(holes != rfdem.EMPTY)[0]
+    holes[rng.choice(live, size=len(live) // 4, replace=False)] = rfdem.EMPTY
+    ty = rng.integers(0, 2, size=N * K).astype(np.uint8)
+    IL32, ty_r = to32(holes), ty.copy()
+    assert REF.ref_reconstruct_bpm(R.ctypes.data, N, K, int(t.C.N), t.C.a, t.C._1d_a, t.aacut, t.C.Nr,
+                                   IL32.ctypes.data, ty_r.ctypes.data) == 0
+    _, ILo, tyo = mc.oracle_reconstruct(t, R, CIs, pnC, holes, ty)
+    assert np.array_equal(to64(IL32), ILo)
+    assert np.array_equal(ty_r, tyo)
+
+
+@needs_ref
+def test_bond_construction_vs_reference(cuda, case):
+    """Bond flags and 1/L0 (the FMA-contracted |r|^2 and the correctly rounded rsqrt)."""
+    t, R = case
+    N, K = R.size // 3, int(t.K)
+    _, CI, CIs, pnC = mc.oracle_cells(t, R)
+    _, IL = mc.oracle_list_construct(t, R, CIs, pnC)
+    ty, iL = np.zeros(N * K, np.uint8), np.zeros(N * K, np.float32)
+    ty_r, iL_r = ty.copy(), iL.copy()
+    assert REF.ref_construct_bonds(R.ctypes.data, N, K, to32(IL).ctypes.data, ty_r.ctypes.data, iL_r.ctypes.data,
+                                   np.float32(t.Po.b_dd), np.float32(t.Po.b_r)) == 0
+    ILo, tyo, iLo, _ = mc.oracle_bonds_delete(t, R, IL, ty, iL, mc.zeros_state(N, K), np.float32(t.Po.b_dd),
+                                              np.float32(t.Po.aa_farcut), True, False)
+    assert np.array_equal(ty_r, tyo)
+    assert np.array_equal(iL_r.view(np.uint32), iLo.view(np.uint32))
+
+
+def _force_scale(F):
+    n = F.size // 3
+    return np.sqrt(F[:n] ** 2 + F[n:2 * n] ** 2 + F[2 * n:] ** 2).max()
+
+
+@needs_ref
+def test_forces_vs_reference_within_tolerance(cuda, case):
+    t, R = case
+    steps = 40 if R.size // 3 < 5000 else 10
+    t2, st = mc.oracle_state_after(t, R, steps)
+    N, K = R.size // 3, int(t.K)
+    S = {k: st[k].copy() for k in ["Rij", "Oijt", "Mijn", "Mijt"]}
+    rng = np.random.default_rng(4)
+    V = st["V"] + rng.normal(scale=2e-4, size=3 * N).astype(np.float32)
+    W = st["W"] + rng.normal(scale=2e-3, size=3 * N).astype(np.float32)
+    o = mc.oracle_forces(t, st["R"], V, W, st["IL"], st["ILtype"], st["iL"], S)
+    ref = {k: v.copy() for k, v in S.items()}
+    ty_r = st["ILtype"].copy()
+    F, M = np.zeros(3 * N, np.float32), np.zeros(3 * N, np.float32)
+    p22 = np.array(mc.bond_params(t), np.float32)
+    p21 = np.array(mc.contact_params(t), np.float32)
+    assert REF.ref_forces(st["R"].ctypes.data, V.ctypes.data, W.ctypes.data, N, K, to32(st["IL"]).ctypes.data,
+                          ty_r.ctypes.data, st["iL"].ctypes.data, ref["Rij"].ctypes.data, ref["Oijt"].ctypes.data,
+                          ref["Mijn"].ctypes.data, ref["Mijt"].ctypes.data, F.ctypes.data, M.ctypes.data,
+                          p22.ctypes.data, p21.ctypes.data, 3) == 0
+    # break decisions: identical except for bonds whose criterion sits within 4 ulp of the strength
+    flips = np.nonzero(ty_r != o["ty"])[0]
+    assert flips.size <= max(2, N * K // 100000), flips
+    fs, ms = _force_scale(o["F"]), _force_scale(o["M"])
+    np.testing.assert_allclose(F, o["F"], rtol=0, atol=1e-5 * fs)
+    np.testing.assert_allclose(M, o["M"], rtol=0, atol=1e-5 * ms)
+    for k in ["Rij", "Oijt", "Mijn", "Mijt"]:
+        sc = np.abs(o[k]).max() + 1e-30
+        np.testing.assert_allclose(ref[k], o[k], rtol=0, atol=1e-5 * sc, err_msg=k)
+
+
+@needs_ref
+@pytest.mark.parametrize("kind,d,h,steps", [(0, 9.0, 14.0, 300), (1, 16.0, 6.0, 300)], ids=["uniaxial", "brazil"])
+def test_whole_run_vs_reference(cuda, kind, d, h, steps):
+    """A short whole test through the reference's own driver sequence: rows and bond flags
+    equal, positions and load curve within tolerance, error against the FP64 oracle reported."""
+    t, R = rfdem.make_test(kind, d, h, seed=0xB2000000 + 41)
+    N, K = R.size // 3, int(t.K)
+    tr = mc.clone(t)
+    out = dict(R=np.zeros(3 * N, np.float32), V=np.zeros(3 * N, np.float32), W=np.zeros(3 * N, np.float32),
+               IL=np.zeros(N * K, np.uint32), ty=np.zeros(N * K, np.uint8), iL=np.zeros(N * K, np.float32),
+               Rij=np.zeros(3 * N * K, np.float32), Oijt=np.zeros(3 * N * K, np.float32),
+               Mijn=np.zeros(3 * N * K, np.float32), Mijt=np.zeros(3 * N * K, np.float32))
+    curve_r = np.zeros(3 * steps, np.float64)
+    import ctypes as C
+    ns = C.c_uint64(0)
+    n = REF.ref_run(C.byref(tr), R.ctypes.data, steps, *[out[k].ctypes.data for k in
+                                                        ["R", "V", "W", "IL", "ty", "iL", "Rij", "Oijt", "Mijn", "Mijt"]],
+                    curve_r.ctypes.data, steps, C.byref(ns))
+    assert n == steps
+    e = rfdem.Engine(mc.clone(t), R)
+    e.step(steps)
+    eg = e.export()
+    e.close()
+    assert np.array_equal(to64(out["IL"]), eg["IL"].astype(np.uint64))
+    flips = np.nonzero(out["ty"] != eg["ILtype"])[0]
+    assert flips.size <= 2, flips
+    ext = np.ptp(R)
+    np.testing.assert_allclose(out["R"], eg["R"], rtol=0, atol=2e-6 * ext)
+    to = mc.clone(t)
+    nd, Rd, curve_d, _, _ = oracle.run_d(to, R, steps)
+    err_engine = np.abs(eg["R"].astype(np.float64) - Rd).max()
+    err_ref = np.abs(out["R"].astype(np.float64) - Rd).max()
+    print("max |R - R_fp64|: engine %.3e  reference %.3e (mm)" % (err_engine, err_ref))
+    assert err_engine < 1e-4 and err_ref < 1e-4

@@ -252,13 +252,14 @@ def run_engine(args):
     launches = S * args.steps + 7 * rebuilds + 2 * args.steps
 
     # e2e through the reference-facing driver call with host buffers
+    graph_used = e.uses_graph()
     e.close()
     e2e_steps = S
     pinned = torch.from_numpy(R).pin_memory()
     Rout = torch.empty_like(pinned).pin_memory()
     curve = torch.empty(3 * e2e_steps, dtype=torch.float64).pin_memory()
     import ctypes as C
-    e2e_calls = 3
+    e2e_calls = 0 if args.no_e2e else 3
 
     def e2e_call():
         tt = rfdem.Task.from_buffer_copy(t)
@@ -267,16 +268,18 @@ def run_engine(args):
                                                                  curve.data_ptr(), e2e_steps, Rout.data_ptr(),
                                                                  C.byref(res)), "e2e")
         return res
-    e2e_call()
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_calls):
+    e2e_value = None
+    if e2e_calls:
         e2e_call()
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-    e2e_value = total_particles * e2e_steps * e2e_calls / e2e_s
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_calls):
+            e2e_call()
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+        e2e_value = total_particles * e2e_steps * e2e_calls / e2e_s
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -297,7 +300,7 @@ def run_engine(args):
            "config": {"workload": WORKLOAD, "particles": N, "explicit_steps_per_bench_step": S, "slots_K": K,
                       "bonds_per_particle": round(bbar, 3), "contacts_per_particle": round(cbar, 3),
                       "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 57 + N * 100) / 1e6),
-                      "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": e2e_value and True},
+                      "parallelism": "specimen-per-gpu" if ws > 1 else "single"},
            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 12 * N,
                    "d2h_bytes_per_step": 12 * N + 24 * e2e_steps,
                    "path": "md_CalculationUniaxialCompression, %d explicit steps per call incl. build" % e2e_steps},
@@ -309,7 +312,7 @@ def run_engine(args):
            "gpu_launches": launches,
            "rebuilds": rebuilds,
            "clocks": clk}
-    out["config"]["graph"] = True
+    out["config"]["graph"] = graph_used
     print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
@@ -322,6 +325,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the driver-call leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -259,9 +259,58 @@ __device__ __forceinline__ void zero_slot_state(const Dev& d, const Consts& c, u
     for (int p = 0; p < 12; ++p) plane(d, c, p, k)[i] = 0.f;
 }
 
+// DeleteFarLinks for particle i with the current positions. Every lane of the warp
+// calls it (the loop bound is warp-uniform); lanes without links have live == 0.
+__device__ __forceinline__ void delete_far(const Dev& d, const Consts& c, const float4* __restrict__ P, uint32_t i,
+                                           const f3 xi, uint32_t ncand, uint32_t& live, uint32_t& bond, uint32_t& cm,
+                                           unsigned long long& mem) {
+    const uint32_t N = c.N;
+    const uint32_t wl = __reduce_or_sync(0xffffffffu, live);
+    const uint32_t kend = 32u - __clz(wl);
+    for (uint32_t k = 0; k < kend; ++k) {
+        if (!((live >> k) & 1u)) continue;
+        const size_t s = (size_t)k * N + i;
+        const uint32_t j = d.ids[s];
+        const float rr = dist2_rn(xi, f4to3(P[j]));
+        if (rr > c.aa_farcut || (double)rr < 1e-10) {
+            d.ids[s] = EMPTY32;
+            zero_slot_state(d, c, k, i);
+            const uint32_t bit = 1u << k;
+            live &= ~bit; bond &= ~bit; cm &= ~bit;
+            for (uint32_t q = 0; q < ncand; ++q)
+                if (d.cand[(size_t)q * N + i] == j) { mem &= ~(1ull << q); break; }
+        }
+    }
+}
+
+// The delete pass of the last step, applied before the state is read out: the step
+// kernel defers each step's DeleteFarLinks to the start of the next step (same
+// positions), so a snapshot taken between steps applies it first. Idempotent.
+__global__ void k_delete_pending(Dev d, Consts c) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < c.N;
+    const float4* P = d.pos[d.sc->steps & 1ull];
+    f3 xi = mk3(0.f, 0.f, 0.f);
+    uint32_t live = 0, bond = 0, cm = 0, ncand = 0;
+    unsigned long long mem = 0ull;
+    if (valid) {
+        xi = f4to3(P[i]);
+        live = d.live[i]; bond = d.bond[i]; cm = d.cmask[i]; mem = d.member[i]; ncand = d.cand_n[i];
+    }
+    const uint32_t live0 = live;
+    delete_far(d, c, P, i, xi, ncand, live, bond, cm, mem);
+    if (valid && live != live0) {
+        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.member[i] = mem;
+    }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
     DevScalars* sc = d.sc;
+    // Loop safety: clear the WHILE condition first. Only the last block's finalize,
+    // which runs after every block has passed this point and advances the step
+    // counter towards the target, sets it again, so the device loop always ends.
+    if (c.use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c.h_loop, 0u);
     if (sc->done) return;
     const uint32_t cur = (uint32_t)(sc->steps & 1ull), nxt = cur ^ 1u;
     const float4* __restrict__ P = d.pos[cur];
@@ -291,24 +340,7 @@ __global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
     const unsigned long long mem0 = mem;
 
     // ---- delete: d_DeleteFarLinks (md_interaction_list_reconstructbpm.cu:141-186)
-    {
-        const uint32_t wl = __reduce_or_sync(FULL, live);
-        const uint32_t kend = 32u - __clz(wl);
-        for (uint32_t k = 0; k < kend; ++k) {
-            if (!((live >> k) & 1u)) continue;
-            const size_t s = (size_t)k * N + i;
-            const uint32_t j = d.ids[s];
-            const float rr = dist2_rn(xi, f4to3(P[j]));
-            if (rr > c.aa_farcut || (double)rr < 1e-10) {
-                d.ids[s] = EMPTY32;
-                zero_slot_state(d, c, k, i);
-                const uint32_t bit = 1u << k;
-                live &= ~bit; bond &= ~bit; cm &= ~bit;
-                for (uint32_t q = 0; q < ncand; ++q)
-                    if (d.cand[(size_t)q * N + i] == j) { mem &= ~(1ull << q); break; }
-            }
-        }
-    }
+    delete_far(d, c, P, i, xi, ncand, live, bond, cm, mem);
 
     // ---- add: InteractionListReConstructBPM (md_interaction_list_reconstructbpm.cu:13-46,80-139)
     if (valid) {
@@ -1005,6 +1037,8 @@ rf_status rf_engine_export(rf_engine* e, float* R, float* V, float* W, uint_fast
     RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
     const int cur = (int)(h.steps & 1ull);
     if (!e->staging) RF_CUDA(cudaMalloc(&e->staging, 3 * (size_t)N * sizeof(float)));
+    k_delete_pending<<<(N + 127) / 128, 128, 0, s>>>(e->d, e->c);
+    RF_CHECK_LAUNCH("k_delete_pending");
     const float4* vecs[3] = {e->d.pos[cur], e->d.vel[cur], e->d.ang[cur]};
     float* outs[3] = {R, V, W};
     for (int q = 0; q < 3; ++q) {

@@ -53,20 +53,25 @@ def gpu_list_construct(torch, task, R, CIs, pnC):
     N, K = R.size // 3, int(task.K)
     a, inv_a, Nr, CN = grid_args(task)
     dIL = torch.zeros(N * K, dtype=torch.int64, device="cuda")
-    st = rfdem.lib.md_InteractionListConstruct(dev(torch, R).data_ptr(), N, dev(torch, CIs).data_ptr(),
-                                               dev(torch, pnC).data_ptr(), dIL.data_ptr(), K, a, inv_a, task.aacut,
-                                               Nr, CN, None)
-    return st, host(dIL, ID_NP)
+    keep = [dev(torch, R), dev(torch, CIs), dev(torch, pnC)]       # alive until the kernel has run
+    st = rfdem.lib.md_InteractionListConstruct(keep[0].data_ptr(), N, keep[1].data_ptr(), keep[2].data_ptr(),
+                                               dIL.data_ptr(), K, a, inv_a, task.aacut, Nr, CN, None)
+    out = host(dIL, ID_NP)
+    del keep
+    return st, out
 
 
 def gpu_reconstruct(torch, task, R, CIs, pnC, IL, ty):
     N, K = R.size // 3, int(task.K)
     a, inv_a, Nr, CN = grid_args(task)
     dIL, dT = dev(torch, IL), dev(torch, ty)
-    st = rfdem.lib.md_InteractionListReConstructBPM(dev(torch, R).data_ptr(), N, dev(torch, CIs).data_ptr(),
-                                                    dev(torch, pnC).data_ptr(), dIL.data_ptr(), dT.data_ptr(), K, a,
-                                                    inv_a, task.aacut, Nr, CN, None)
-    return st, host(dIL, ID_NP), host(dT, np.uint8)
+    keep = [dev(torch, R), dev(torch, CIs), dev(torch, pnC)]       # alive until the kernel has run
+    st = rfdem.lib.md_InteractionListReConstructBPM(keep[0].data_ptr(), N, keep[1].data_ptr(), keep[2].data_ptr(),
+                                                    dIL.data_ptr(), dT.data_ptr(), K, a, inv_a, task.aacut, Nr, CN,
+                                                    None)
+    out = host(dIL, ID_NP), host(dT, np.uint8)
+    del keep
+    return (st,) + out
 
 
 def zeros_state(N, K):

@@ -35,6 +35,10 @@
 #include <algorithm>
 #include "rf_physics.cuh"
 
+#ifndef RF_STEP_MIN_BLOCKS
+#define RF_STEP_MIN_BLOCKS 6      // resident 128-thread CTAs per SM the step kernel is compiled for
+#endif
+
 namespace rf {
 
 // Scalar state of the run, device resident (compression_data + result bookkeeping).
@@ -75,12 +79,21 @@ struct Dev {
     float4* pos[2];
     float4* vel[2];
     float4* ang[2];
-    uint32_t* ids;      // [K][N]
-    float* il;          // [K][N]
-    float* st;          // [12][K][N]
-    uint32_t* live;     // [N]
-    uint32_t* bond;     // [N]
-    uint32_t* cmask;    // [N]
+    // rows: slot-major, K slots per particle
+    uint32_t* ids;      // [N][K] neighbour id of each occupied slot (row-major: a thread walks its own row)
+    float* il;          // [K][N] 1/L0 per slot, as the reference layout keeps it (read out only)
+    float* cO[2];       // [N][K][3] tangential overlap of type-0 slots, by step parity (read cur, write next)
+    uint32_t* live;     // [N] occupied slots
+    uint32_t* bond;     // [N] slots holding an intact bond
+    uint32_t* cmask;    // [N] type-0 slots whose overlap may be non-zero
+    // bond records: the bonds of particle i in slot order, ordinal-major [q][i]
+    uint32_t* bj;       // [QB][N] partner id
+    uint8_t* bk;        // [QB][N] slot of the record (0xFF: record retired)
+    float* bil;         // [QB][N] 1/L0
+    float4* bst;        // [3][QB][N] (Rij.xyz Oijt.x) (Oijt.yz Mijn.xy) (Mijn.z Mijt.xyz)
+    uint32_t* nbq;      // [N] records of the particle
+    uint32_t* bmask;    // [N] records holding an intact bond
+    // Verlet candidates
     uint32_t* cand;     // [KC][N]
     uint32_t* cand_n;   // [N]
     unsigned long long* member;   // [N]
@@ -93,13 +106,15 @@ struct Dev {
     uint32_t* cg_sorted;   // [N]
     double2* partial;   // [blocks]
     unsigned long long n_particles;
+    uint32_t QB;
     double* curve;      // [cap][3]
     DevScalars* sc;
 };
 
 __device__ __forceinline__ f3 f4to3(const float4 v) { return mk3(v.x, v.y, v.z); }
-__device__ __forceinline__ float* plane(const Dev& d, const Consts& c, int p, uint32_t k) {
-    return d.st + ((size_t)p * c.K + k) * c.N;
+__device__ __forceinline__ void zero_record(const Dev& d, size_t QN, size_t s) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    d.bst[s] = z; d.bst[s + QN] = z; d.bst[s + 2 * QN] = z;
 }
 
 // ---------------------------------------------------------------------------
@@ -242,7 +257,7 @@ __global__ void k_rb_cand(Dev d, Consts c) {
         while (live) {
             const uint32_t k = __ffs(live) - 1;
             live &= live - 1;
-            const uint32_t j = d.ids[(size_t)k * c.N + i];
+            const uint32_t j = d.ids[(size_t)i * c.K + k];
             for (uint32_t q = 0; q < n; ++q)
                 if (d.cand[(size_t)q * c.N + i] == j) { mem |= 1ull << q; break; }
         }
@@ -254,32 +269,49 @@ __global__ void k_rb_cand(Dev d, Consts c) {
 // ---------------------------------------------------------------------------
 // The step kernel
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void zero_slot_state(const Dev& d, const Consts& c, uint32_t k, uint32_t i) {
-#pragma unroll
-    for (int p = 0; p < 12; ++p) plane(d, c, p, k)[i] = 0.f;
+// Retire the bond record of slot k of particle i, if it has one: its state is
+// zeroed (DeleteFarLinks zeroes Rij, Oijt, Mijn, Mijt of the slot) and it stops
+// belonging to the slot.
+__device__ __forceinline__ void retire_record(const Dev& d, const Consts& c, uint32_t i, uint32_t k, uint32_t nbq,
+                                              uint32_t& bmask) {
+    const uint32_t N = c.N;
+    for (uint32_t q = 0; q < nbq; ++q) {
+        const size_t s = (size_t)q * N + i;
+        if (d.bk[s] == (uint8_t)k) {
+            d.bk[s] = 0xFF;
+            zero_record(d, (size_t)d.QB * N, s);
+            bmask &= ~(1u << q);
+            return;
+        }
+    }
 }
 
-// DeleteFarLinks for particle i with the current positions. Every lane of the warp
-// calls it (the loop bound is warp-uniform); lanes without links have live == 0.
-__device__ __forceinline__ void delete_far(const Dev& d, const Consts& c, const float4* __restrict__ P, uint32_t i,
-                                           const f3 xi, uint32_t ncand, uint32_t& live, uint32_t& bond, uint32_t& cm,
-                                           unsigned long long& mem) {
+// DeleteFarLinks (md_interaction_list_reconstructbpm.cu:141-186) of one slot.
+__device__ __forceinline__ void delete_slot(const Dev& d, const Consts& c, uint32_t i, uint32_t k, uint32_t j,
+                                            uint32_t ncand, uint32_t nbq, uint32_t& live, uint32_t& bond, uint32_t& cm,
+                                            uint32_t& bmask, unsigned long long& mem) {
     const uint32_t N = c.N;
-    const uint32_t wl = __reduce_or_sync(0xffffffffu, live);
-    const uint32_t kend = 32u - __clz(wl);
-    for (uint32_t k = 0; k < kend; ++k) {
-        if (!((live >> k) & 1u)) continue;
-        const size_t s = (size_t)k * N + i;
-        const uint32_t j = d.ids[s];
-        const float rr = dist2_rn(xi, f4to3(P[j]));
-        if (rr > c.aa_farcut || (double)rr < 1e-10) {
-            d.ids[s] = EMPTY32;
-            zero_slot_state(d, c, k, i);
-            const uint32_t bit = 1u << k;
-            live &= ~bit; bond &= ~bit; cm &= ~bit;
-            for (uint32_t q = 0; q < ncand; ++q)
-                if (d.cand[(size_t)q * N + i] == j) { mem &= ~(1ull << q); break; }
-        }
+    const size_t s = (size_t)i * c.K + k;
+    d.ids[s] = EMPTY32;                       // its overlap reads as zero once the cmask bit is clear
+    retire_record(d, c, i, k, nbq, bmask);
+    const uint32_t bit = 1u << k;
+    live &= ~bit; bond &= ~bit; cm &= ~bit;
+    for (uint32_t q = 0; q < ncand; ++q)
+        if (d.cand[(size_t)q * N + i] == j) { mem &= ~(1ull << q); break; }
+}
+
+// DeleteFarLinks for every occupied slot of particle i with the current positions.
+__device__ __forceinline__ void delete_far(const Dev& d, const Consts& c, const float4* __restrict__ P, uint32_t i,
+                                           const f3 xi, uint32_t ncand, uint32_t nbq, uint32_t& live, uint32_t& bond,
+                                           uint32_t& cm, uint32_t& bmask, unsigned long long& mem) {
+    const uint32_t* row = d.ids + (size_t)i * c.K;
+    uint32_t m = live;
+    while (m) {
+        const uint32_t k = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t j = row[k];
+        const float rr = dist2_rn(xi, f4to3(__ldg(&P[j])));
+        if (rr > c.aa_farcut || (double)rr < 1e-10) delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
     }
 }
 
@@ -291,21 +323,22 @@ __global__ void k_delete_pending(Dev d, Consts c) {
     const bool valid = i < c.N;
     const float4* P = d.pos[d.sc->steps & 1ull];
     f3 xi = mk3(0.f, 0.f, 0.f);
-    uint32_t live = 0, bond = 0, cm = 0, ncand = 0;
+    uint32_t live = 0, bond = 0, cm = 0, ncand = 0, nbq = 0, bmask = 0;
     unsigned long long mem = 0ull;
     if (valid) {
         xi = f4to3(P[i]);
         live = d.live[i]; bond = d.bond[i]; cm = d.cmask[i]; mem = d.member[i]; ncand = d.cand_n[i];
+        nbq = d.nbq[i]; bmask = d.bmask[i];
     }
     const uint32_t live0 = live;
-    delete_far(d, c, P, i, xi, ncand, live, bond, cm, mem);
+    delete_far(d, c, P, i, xi, ncand, nbq, live, bond, cm, bmask, mem);
     if (valid && live != live0) {
-        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.member[i] = mem;
+        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.member[i] = mem; d.bmask[i] = bmask;
     }
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
+__global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts c) {
     DevScalars* sc = d.sc;
     // Loop safety: clear the WHILE condition first. Only the last block's finalize,
     // which runs after every block has passed this point and advances the step
@@ -328,36 +361,118 @@ __global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
     cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
 
     f3 xi = mk3(0.f, 0.f, 0.f), vi = xi, wi = xi;
-    uint32_t live = 0, bond = 0, cm = 0;
+    uint32_t live = 0, bond = 0, cm = 0, nbq = 0, bmask = 0;
     unsigned long long mem = 0ull;
     uint32_t ncand = 0;
     if (valid) {
         xi = f4to3(P[i]); vi = f4to3(Vv[i]); wi = f4to3(Wv[i]);
         live = d.live[i]; bond = d.bond[i]; cm = d.cmask[i];
         mem = d.member[i]; ncand = d.cand_n[i];
+        nbq = d.nbq[i]; bmask = d.bmask[i];
     }
-    const uint32_t live0 = live, bond0 = bond, cm0 = cm;
+    const uint32_t live0 = live, bond0 = bond, cm0 = cm, bmask0 = bmask;
     const unsigned long long mem0 = mem;
+    const size_t QN = (size_t)d.QB * N;
 
-    // ---- delete: d_DeleteFarLinks (md_interaction_list_reconstructbpm.cu:141-186)
-    delete_far(d, c, P, i, xi, ncand, live, bond, cm, mem);
+    // ---- bonds: d_CalculateForcesDEM_22 (md_calculateforcesdem3.cu:424-483) over the bond
+    // records in slot order, with the DeleteFarLinks test of each bond slot on the same
+    // gathered position (md_interaction_list_reconstructbpm.cu:141-186). The next record
+    // is fetched while the current one is computed.
+    f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
+    uint32_t nbroken = 0;
+    {
+        const uint32_t wb = __reduce_or_sync(FULL, bmask);
+        const uint32_t qend = 32u - __clz(wb);
+        uint32_t nj = i;
+        float nil = 0.f;
+        float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0, n2 = n0;
+        if (qend > 0 && (bmask & 1u)) {
+            const size_t s = (size_t)i;
+            nj = __ldg(&d.bj[s]); nil = __ldg(&d.bil[s]);
+            n0 = d.bst[s]; n1 = d.bst[s + QN]; n2 = d.bst[s + 2 * QN];
+        }
+        for (uint32_t q = 0; q < qend; ++q) {
+            const uint32_t j = nj;
+            const float il = nil;
+            const float4 s0 = n0, s1 = n1, s2 = n2;
+            const bool act = (bmask >> q) & 1u;
+            if (q + 1 < qend && ((bmask >> (q + 1)) & 1u)) {
+                const size_t s = (size_t)(q + 1) * N + i;
+                nj = __ldg(&d.bj[s]); nil = __ldg(&d.bil[s]);
+                n0 = d.bst[s]; n1 = d.bst[s + QN]; n2 = d.bst[s + 2 * QN];
+            }
+            if (!act) continue;
+            const size_t s = (size_t)q * N + i;
+            const float4 pj = __ldg(&P[j]), vj = __ldg(&Vv[j]), wj = __ldg(&Wv[j]);
+            const f3 xj = f4to3(pj);
+            const float rr = dist2_rn(xi, xj);
+            if (rr > c.aa_farcut || (double)rr < 1e-10) {
+                delete_slot(d, c, i, d.bk[s], j, ncand, nbq, live, bond, cm, bmask, mem);
+                continue;
+            }
+            const f3 r = mk3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
+            f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
+            f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
+            const bool broke = bond_slot(c.bp, r, vi, f4to3(vj), wi, f4to3(wj), il, rij, oijt, mijn, mijt, fsb, msb);
+            d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
+            d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
+            d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
+            if (broke) { bmask &= ~(1u << q); bond &= ~(1u << d.bk[s]); ++nbroken; }
+        }
+    }
+
+    // ---- type-0 slots, one gather each: the rest of the previous step's DeleteFarLinks,
+    // then d_CalculateForcesDEM_21 (md_calculateforcesdem3.cu:338-422) in slot order
+    // (bonds broken above included). Overlaps are read from this step's buffer and
+    // written to the next one, so the pass can be replayed below if a link added by
+    // this step's list update turns out to be in contact.
+    const uint32_t* row = d.ids + (size_t)i * c.K;
+    const float* oin = d.cO[cur] + (size_t)i * c.K * 3;
+    float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
+    const uint32_t cm_in = cm;
+    const float twoR = 2.0f * c.cp.rP;
+    f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
+    uint32_t cm_out = 0;
+    {
+        uint32_t m = live & ~bond;
+        while (m) {
+            const uint32_t k = __ffs(m) - 1;
+            m &= m - 1;
+            const uint32_t j = row[k];
+            const f3 xj = f4to3(__ldg(&P[j]));
+            const float rr = dist2_rn(xi, xj);
+            if (rr > c.aa_farcut || (double)rr < 1e-10) {
+                delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
+                continue;
+            }
+            const f3 r = mk3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
+            const float rijm = norm3(r.x, r.y, r.z);
+            if (!(rijm < twoR)) continue;
+            const uint32_t bit = 1u << k;
+            f3 o = (cm_in & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
+            contact_pair(c.cp, r, rijm, vi, f4to3(__ldg(&Vv[j])), wi, f4to3(__ldg(&Wv[j])), o, fsc, msc);
+            oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
+            cm_out |= bit;
+        }
+    }
 
     // ---- add: InteractionListReConstructBPM (md_interaction_list_reconstructbpm.cu:13-46,80-139)
+    bool replay = false;
     if (valid) {
         unsigned long long tried = mem;
         bool have_cells = false;
-        int64_t cells[8];
+        Octant oc;
         for (;;) {
             unsigned long long best = ~0ull;
             uint32_t best_q = 0;
             for (uint32_t q = 0; q < ncand; ++q) {
                 if ((tried >> q) & 1ull) continue;
-                const uint32_t j = d.cand[(size_t)q * N + i];
-                const f3 xj = f4to3(P[j]);
+                const uint32_t j = __ldg(&d.cand[(size_t)q * N + i]);
+                const f3 xj = f4to3(__ldg(&P[j]));
                 const float rr = dist2_rn(xi, xj);
                 if (!(rr < c.aacut && (double)rr > 1e-10)) continue;
-                if (!have_cells) { octant_cells(xi, c.g, cells); have_cells = true; }
-                const int rank = octant_rank(cells, ref_cell(xj, c.g));
+                if (!have_cells) { oc = octant_of(xi, c.g); have_cells = true; }
+                const int rank = octant_rank(oc, ref_cell(xj, c.g));
                 if (rank < 0) continue;
                 const unsigned long long key = ((unsigned long long)rank << 32) | j;
                 if (key < best) { best = key; best_q = q; }
@@ -369,65 +484,36 @@ __global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
             uint32_t k;
             if (i == 0 && (free & 1u) && (free & ~1u)) k = __ffs(free & ~1u) - 1;   // kdxfree==0 quirk
             else k = __ffs(free) - 1;
-            d.ids[(size_t)k * N + i] = (uint32_t)(best & 0xffffffffull);
+            const uint32_t j = (uint32_t)(best & 0xffffffffull);
+            d.ids[(size_t)i * c.K + k] = j;
             live |= 1u << k;
             mem |= 1ull << best_q;
+            const f3 xj = f4to3(__ldg(&P[j]));
+            if (norm3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z) < twoR) replay = true;
         }
     }
-
-    // ---- bonds: d_CalculateForcesDEM_22 (md_calculateforcesdem3.cu:424-483)
-    f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
-    uint32_t nbroken = 0;
-    {
-        const uint32_t wb = __reduce_or_sync(FULL, bond);
-        const uint32_t kend = 32u - __clz(wb);
-        for (uint32_t k = 0; k < kend; ++k) {
-            if (!((bond >> k) & 1u)) continue;
-            const size_t s = (size_t)k * N + i;
-            const uint32_t j = d.ids[s];
-            const f3 xj = f4to3(P[j]);
+    // A new link already in contact: _21 would have visited it in slot order among the
+    // others, so the contact pass is replayed over the final row from the unchanged
+    // overlaps of this step.
+    if (replay) {
+        fsc = mk3(0.f, 0.f, 0.f); msc = fsc; cm_out = 0;
+        uint32_t m = live & ~bond;
+        while (m) {
+            const uint32_t k = __ffs(m) - 1;
+            m &= m - 1;
+            const uint32_t j = row[k];
+            const f3 xj = f4to3(__ldg(&P[j]));
             const f3 r = mk3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
-            float* p0 = d.st + (size_t)k * N + i;
-            const size_t ps = (size_t)c.K * N;
-            f3 rij = mk3(p0[0], p0[ps], p0[2 * ps]);
-            f3 oijt = mk3(p0[3 * ps], p0[4 * ps], p0[5 * ps]);
-            f3 mijn = mk3(p0[6 * ps], p0[7 * ps], p0[8 * ps]);
-            f3 mijt = mk3(p0[9 * ps], p0[10 * ps], p0[11 * ps]);
-            const bool broke = bond_slot(c.bp, r, vi, f4to3(Vv[j]), wi, f4to3(Wv[j]), d.il[s], rij, oijt, mijn, mijt,
-                                         fsb, msb);
-            p0[0] = rij.x; p0[ps] = rij.y; p0[2 * ps] = rij.z;
-            p0[3 * ps] = oijt.x; p0[4 * ps] = oijt.y; p0[5 * ps] = oijt.z;
-            p0[6 * ps] = mijn.x; p0[7 * ps] = mijn.y; p0[8 * ps] = mijn.z;
-            p0[9 * ps] = mijt.x; p0[10 * ps] = mijt.y; p0[11 * ps] = mijt.z;
-            if (broke) { bond &= ~(1u << k); ++nbroken; }
-        }
-    }
-
-    // ---- contacts: d_CalculateForcesDEM_21 (md_calculateforcesdem3.cu:338-422)
-    f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
-    {
-        const uint32_t ct = live & ~bond;
-        const uint32_t wc = __reduce_or_sync(FULL, ct);
-        const uint32_t kend = 32u - __clz(wc);
-        const size_t ps = (size_t)c.K * N;
-        for (uint32_t k = 0; k < kend; ++k) {
-            if (!((ct >> k) & 1u)) continue;
-            const size_t s = (size_t)k * N + i;
-            const uint32_t j = d.ids[s];
-            const f3 xj = f4to3(P[j]);
-            const f3 r = mk3(xj.x - xi.x, xj.y - xi.y, xj.z - xi.z);
-            float* o0 = d.st + 3 * ps + (size_t)k * N + i;
+            const float rijm = norm3(r.x, r.y, r.z);
+            if (!(rijm < twoR)) continue;
             const uint32_t bit = 1u << k;
-            f3 o = (cm & bit) ? mk3(o0[0], o0[ps], o0[2 * ps]) : mk3(0.f, 0.f, 0.f);
-            if (contact_slot(c.cp, r, vi, f4to3(Vv[j]), wi, f4to3(Wv[j]), o, fsc, msc)) {
-                o0[0] = o.x; o0[ps] = o.y; o0[2 * ps] = o.z;
-                cm |= bit;
-            } else if (cm & bit) {
-                o0[0] = 0.f; o0[ps] = 0.f; o0[2 * ps] = 0.f;
-                cm &= ~bit;
-            }
+            f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
+            contact_pair(c.cp, r, rijm, vi, f4to3(__ldg(&Vv[j])), wi, f4to3(__ldg(&Wv[j])), o, fsc, msc);
+            oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
+            cm_out |= bit;
         }
     }
+    cm = cm_out;
 
     double sfb = 0.0, sft = 0.0;
     uint32_t moved = 0;
@@ -436,6 +522,7 @@ __global__ void __launch_bounds__(128) k_step(Dev d, Consts c) {
         if (bond != bond0) d.bond[i] = bond;
         if (cm != cm0) d.cmask[i] = cm;
         if (mem != mem0) d.member[i] = mem;
+        if (bmask != bmask0) d.bmask[i] = bmask;
         // F = 0 after the memset, then += _22 sums, then += _21 sums
         float Fx = 0.0f + fsb.x, Fy = 0.0f + fsb.y, Fz = 0.0f + fsb.z;
         Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
@@ -584,32 +671,67 @@ __global__ void k_f4_to_planar(const float4* __restrict__ in, uint32_t N, float*
     }
 }
 
-// Reference-layout rows (uint_fast32_t ids, AoS float3 state) -> engine rows.
+// Bond records a reference-layout row needs: its intact bonds, and broken bonds that
+// still carry a bond direction (Rij is kept until the slot is deleted).
+__device__ __forceinline__ bool needs_record(uint8_t type, const rf_float3 r) {
+    return type == 1 || r.x != 0.f || r.y != 0.f || r.z != 0.f;
+}
+
+__global__ void k_count_records(const uint_fast32_t* __restrict__ IL, const uint8_t* __restrict__ type,
+                                const rf_float3* __restrict__ Rij, uint32_t N, uint32_t K, uint32_t* maxq) {
+    const uint_fast32_t E = empty_id<uint_fast32_t>();
+    uint32_t m = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        uint32_t n = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+            const size_t r = (size_t)i * K + k;
+            if (IL[r] != E && IL[r] < N && needs_record(type[r], Rij[r])) ++n;
+        }
+        m = max(m, n);
+    }
+    atomicMax(maxq, m);
+}
+
+// Reference-layout rows (uint_fast32_t ids, AoS float3 state) -> engine rows and records.
 __global__ void k_rows_import(const uint_fast32_t* __restrict__ IL, const uint8_t* __restrict__ type,
                               const float* __restrict__ iL, const rf_float3* __restrict__ Rij,
                               const rf_float3* __restrict__ Oijt, const rf_float3* __restrict__ Mijn,
                               const rf_float3* __restrict__ Mijt, Dev d, Consts c) {
     const uint_fast32_t E = empty_id<uint_fast32_t>();
-    const size_t ps = (size_t)c.K * c.N;
+    const size_t QN = (size_t)d.QB * c.N;
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
-        uint32_t live = 0, bond = 0, cm = 0;
+        uint32_t live = 0, bond = 0, cm = 0, nq = 0, bmask = 0;
         for (uint32_t k = 0; k < c.K; ++k) {
             const size_t r = (size_t)i * c.K + k, s = (size_t)k * c.N + i;
             const uint_fast32_t j = IL[r];
-            d.ids[s] = (j == E || j >= c.N) ? EMPTY32 : (uint32_t)j;
+            const bool ok = (j != E && j < c.N);
+            d.ids[r] = ok ? (uint32_t)j : EMPTY32;
             d.il[s] = iL[r];
-            float* p0 = d.st + s;
-            p0[0] = Rij[r].x; p0[ps] = Rij[r].y; p0[2 * ps] = Rij[r].z;
-            p0[3 * ps] = Oijt[r].x; p0[4 * ps] = Oijt[r].y; p0[5 * ps] = Oijt[r].z;
-            p0[6 * ps] = Mijn[r].x; p0[7 * ps] = Mijn[r].y; p0[8 * ps] = Mijn[r].z;
-            p0[9 * ps] = Mijt[r].x; p0[10 * ps] = Mijt[r].y; p0[11 * ps] = Mijt[r].z;
-            if (j != E && j < c.N) {
-                live |= 1u << k;
-                if (type[r] == 1) bond |= 1u << k;
-                else if (Oijt[r].x != 0.f || Oijt[r].y != 0.f || Oijt[r].z != 0.f) cm |= 1u << k;
+            const bool t1 = ok && type[r] == 1;
+            float* co = d.cO[cur] + 3 * r;
+            co[0] = t1 ? 0.f : Oijt[r].x; co[1] = t1 ? 0.f : Oijt[r].y; co[2] = t1 ? 0.f : Oijt[r].z;
+            if (!ok) continue;
+            live |= 1u << k;
+            if (t1) bond |= 1u << k;
+            else if (Oijt[r].x != 0.f || Oijt[r].y != 0.f || Oijt[r].z != 0.f) cm |= 1u << k;
+            if (needs_record(type[r], Rij[r]) && nq < d.QB) {
+                const size_t b = (size_t)nq * c.N + i;
+                d.bj[b] = (uint32_t)j; d.bk[b] = (uint8_t)k; d.bil[b] = iL[r];
+                const float ox = t1 ? Oijt[r].x : 0.f, oy = t1 ? Oijt[r].y : 0.f, oz = t1 ? Oijt[r].z : 0.f;
+                d.bst[b] = make_float4(Rij[r].x, Rij[r].y, Rij[r].z, ox);
+                d.bst[b + QN] = make_float4(oy, oz, Mijn[r].x, Mijn[r].y);
+                d.bst[b + 2 * QN] = make_float4(Mijn[r].z, Mijt[r].x, Mijt[r].y, Mijt[r].z);
+                if (t1) bmask |= 1u << nq;
+                ++nq;
             }
         }
-        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm;
+        for (uint32_t q = nq; q < d.QB; ++q) {          // unused records: retired, zero
+            const size_t b = (size_t)q * c.N + i;
+            d.bj[b] = 0; d.bk[b] = 0xFF; d.bil[b] = 0.f;
+            zero_record(d, QN, b);
+        }
+        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.nbq[i] = nq; d.bmask[i] = bmask;
     }
 }
 
@@ -617,19 +739,31 @@ __global__ void k_rows_export(uint_fast32_t* __restrict__ IL, uint8_t* __restric
                               rf_float3* __restrict__ Rij, rf_float3* __restrict__ Oijt, rf_float3* __restrict__ Mijn,
                               rf_float3* __restrict__ Mijt, Dev d, Consts c) {
     const uint_fast32_t E = empty_id<uint_fast32_t>();
-    const size_t ps = (size_t)c.K * c.N;
+    const size_t QN = (size_t)d.QB * c.N;
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
-        const uint32_t live = d.live[i], bond = d.bond[i];
+        const uint32_t live = d.live[i], bond = d.bond[i], nq = d.nbq[i];
         for (uint32_t k = 0; k < c.K; ++k) {
             const size_t r = (size_t)i * c.K + k, s = (size_t)k * c.N + i;
-            IL[r] = ((live >> k) & 1u) ? (uint_fast32_t)d.ids[s] : E;
+            IL[r] = ((live >> k) & 1u) ? (uint_fast32_t)d.ids[r] : E;
             type[r] = (uint8_t)((bond >> k) & 1u);
             iL[r] = d.il[s];
-            const float* p0 = d.st + s;
-            Rij[r].x = p0[0]; Rij[r].y = p0[ps]; Rij[r].z = p0[2 * ps];
-            Oijt[r].x = p0[3 * ps]; Oijt[r].y = p0[4 * ps]; Oijt[r].z = p0[5 * ps];
-            Mijn[r].x = p0[6 * ps]; Mijn[r].y = p0[7 * ps]; Mijn[r].z = p0[8 * ps];
-            Mijt[r].x = p0[9 * ps]; Mijt[r].y = p0[10 * ps]; Mijt[r].z = p0[11 * ps];
+            Rij[r].x = 0.f; Rij[r].y = 0.f; Rij[r].z = 0.f;
+            Mijn[r] = Rij[r]; Mijt[r] = Rij[r];
+            const bool has = ((d.cmask[i] >> k) & 1u) != 0;
+            const float* co = d.cO[cur] + 3 * r;
+            Oijt[r].x = has ? co[0] : 0.f; Oijt[r].y = has ? co[1] : 0.f; Oijt[r].z = has ? co[2] : 0.f;
+        }
+        for (uint32_t q = 0; q < nq; ++q) {
+            const size_t b = (size_t)q * c.N + i;
+            const uint32_t k = d.bk[b];
+            if (k == 0xFF) continue;
+            const size_t r = (size_t)i * c.K + k;
+            const float4 s0 = d.bst[b], s1 = d.bst[b + QN], s2 = d.bst[b + 2 * QN];
+            Rij[r].x = s0.x; Rij[r].y = s0.y; Rij[r].z = s0.z;
+            Mijn[r].x = s1.z; Mijn[r].y = s1.w; Mijn[r].z = s2.x;
+            Mijt[r].x = s2.y; Mijt[r].y = s2.z; Mijt[r].z = s2.w;
+            if ((bond >> k) & 1u) { Oijt[r].x = s0.w; Oijt[r].y = s1.x; Oijt[r].z = s1.y; }
         }
     }
 }
@@ -681,6 +815,7 @@ struct rf_engine {
     unsigned long long* counters_dev;
     float* staging;
     uint64_t bonds_initial;
+    uint32_t* maxq_dev;
 };
 
 namespace {
@@ -796,7 +931,7 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
     std::memset(&e->c, 0, sizeof(e->c));
     e->task = *t;
     e->graph = nullptr; e->exec = nullptr; e->graph_ok = false; e->staging = nullptr; e->bonds_initial = 0;
-    e->stream = nullptr; e->counters_dev = nullptr;
+    e->stream = nullptr; e->counters_dev = nullptr; e->maxq_dev = nullptr;
     cudaGetDevice(&e->device);
     rf_status st = RF_OK;
     auto fail = [&](rf_status s) { rf_engine_destroy(e); return s; };
@@ -844,8 +979,9 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
         if ((st = dalloc(e, &d.pos[b], N)) || (st = dalloc(e, &d.vel[b], N)) || (st = dalloc(e, &d.ang[b], N)))
             return fail(st);
     }
-    if ((st = dalloc(e, &d.ids, NK)) || (st = dalloc(e, &d.il, NK)) || (st = dalloc(e, &d.st, 12 * NK)) ||
+    if ((st = dalloc(e, &d.ids, NK)) || (st = dalloc(e, &d.il, NK)) || (st = dalloc(e, &d.cO[0], 3 * NK)) || (st = dalloc(e, &d.cO[1], 3 * NK)) ||
         (st = dalloc(e, &d.live, N)) || (st = dalloc(e, &d.bond, N)) || (st = dalloc(e, &d.cmask, N)) ||
+        (st = dalloc(e, &d.nbq, N)) || (st = dalloc(e, &d.bmask, N)) || (st = dalloc(e, &e->maxq_dev, 1)) ||
         (st = dalloc(e, &d.cand, (size_t)c.KC * N)) || (st = dalloc(e, &d.cand_n, N)) || (st = dalloc(e, &d.member, N)) ||
         (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
         (st = dalloc(e, &d.cg_start, cells + 1)) || (st = dalloc(e, &d.cg_fill, cells + 1)) ||
@@ -858,8 +994,9 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
         if (cudaMemsetAsync(d.vel[b], 0, N * sizeof(float4), s) || cudaMemsetAsync(d.ang[b], 0, N * sizeof(float4), s))
             return fail(cuda_status(cudaGetLastError(), "memset"));
     }
-    if (cudaMemsetAsync(d.st, 0, 12 * NK * sizeof(float), s) || cudaMemsetAsync(d.il, 0, NK * sizeof(float), s) ||
-        cudaMemsetAsync(d.member, 0, N * sizeof(unsigned long long), s) || cudaMemsetAsync(d.cand_n, 0, N * 4, s))
+    // the scalar block is read (step parity) by the row import below: start it at zero
+    if (cudaMemsetAsync(d.member, 0, N * sizeof(unsigned long long), s) || cudaMemsetAsync(d.cand_n, 0, N * 4, s) ||
+        cudaMemsetAsync(d.sc, 0, sizeof(DevScalars), s))
         return fail(RF_ERR_CUDA);
 
     // Initial rows exactly as the drivers build them (md_calculationbraziltest.cu:132-144),
@@ -904,6 +1041,20 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
                                                       Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
         if (!st2) st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
                                           (float)P.aa_farcut, s);
+        if (!st2) {
+            // bond records: as many per particle as its row holds bonds (bonds are never created later)
+            uint32_t qb = 0;
+            ce = cudaMemsetAsync(e->maxq_dev, 0, sizeof(uint32_t), s);
+            if (!ce) { k_count_records<<<148 * 4, 256, 0, s>>>(dIL, dT, Rij, N, K, e->maxq_dev); ce = cudaGetLastError(); }
+            if (!ce) ce = cudaMemcpyAsync(&qb, e->maxq_dev, sizeof(qb), cudaMemcpyDeviceToHost, s);
+            if (!ce) ce = cudaStreamSynchronize(s);
+            if (ce) st2 = cuda_status(ce, "engine bond count");
+            if (qb == 0) qb = 1;
+            d.QB = qb;
+            const size_t QN = (size_t)qb * N;
+            if (!st2 && ((st2 = dalloc(e, &d.bj, QN)) || (st2 = dalloc(e, &d.bk, QN)) || (st2 = dalloc(e, &d.bil, QN)) ||
+                         (st2 = dalloc(e, &d.bst, 3 * QN)))) {}
+        }
         if (!st2) {
             k_planar_to_f4<<<(N + 255) / 256, 256, 0, s>>>(dR, N, d.pos[0]);
             k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dIL_f, Rij, Oijt, Mijn, Mijt, d, c);
@@ -1105,6 +1256,16 @@ rf_status rf_engine_import(rf_engine* e, const float* R, const float* V, const f
     const rf_float3* ins3[4] = {Rij, Oijt, Mijn, Mijt};
     for (int q = 0; q < 4 && !ce; ++q)
         ce = cudaMemcpyAsync(dS + q * NK, ins3[q], NK * sizeof(rf_float3), cudaMemcpyHostToDevice, s);
+    uint32_t qb = 0;
+    if (!ce) ce = cudaMemsetAsync(e->maxq_dev, 0, sizeof(uint32_t), s);
+    if (!ce) { k_count_records<<<148 * 4, 256, 0, s>>>(dIL, dT, dS, N, K, e->maxq_dev); ce = cudaGetLastError(); }
+    if (!ce) ce = cudaMemcpyAsync(&qb, e->maxq_dev, sizeof(qb), cudaMemcpyDeviceToHost, s);
+    if (!ce) ce = cudaStreamSynchronize(s);
+    if (!ce && qb > e->d.QB) {
+        cudaFree(dIL); cudaFree(dT); cudaFree(dL); cudaFree(dS);
+        set_error("rf_engine_import: a row holds %u bond records, the engine was sized for %u", qb, e->d.QB);
+        return RF_ERR_CAPACITY;
+    }
     if (!ce) {
         k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dL, dS, dS + NK, dS + 2 * NK, dS + 3 * NK, e->d, e->c);
         ce = cudaGetLastError();

@@ -119,12 +119,22 @@ __device__ __forceinline__ bool bond_slot(const BondParams& p, const f3 r, const
 // One contact slot of type 0 (d_CalculateForcesDEM_21 loop body, :356-402).
 // r = Rj - Ri. Returns true when the pair overlaps (rijm < 2 rP); otherwise the
 // caller sets Oijt to zero, as the reference does.
+// The overlapping pair (rijm < 2 rP) part of the contact slot; rijm = norm3(r).
+__device__ __forceinline__ void contact_pair(const ContactParams& p, const f3 r, const float rijm, const f3 vi,
+                                             const f3 vj, const f3 wi, const f3 wj, f3& Oijt, f3& fs, f3& ms);
+
 __device__ __forceinline__ bool contact_slot(const ContactParams& p, const f3 r, const f3 vi, const f3 vj,
                                              const f3 wi, const f3 wj, f3& Oijt, f3& fs, f3& ms) {
     const float rijm = norm3(r.x, r.y, r.z);
+    if (!(rijm < 2.0f * p.rP)) return false;
+    contact_pair(p, r, rijm, vi, vj, wi, wj, Oijt, fs, ms);
+    return true;
+}
+
+__device__ __forceinline__ void contact_pair(const ContactParams& p, const f3 r, const float rijm, const f3 vi,
+                                             const f3 vj, const f3 wi, const f3 wj, f3& Oijt, f3& fs, f3& ms) {
     const float inv_rm = __frcp_rn(rijm);
     const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
-    if (!(rijm < 2.0f * p.rP)) return false;
     // dd_Calculate_fijn_ppHM_2 (:199-253)
     float c1 = __fsqrt_rn(p.rP * fabsf(p.rP - 0.5f * rijm));
     const float Kn = 2.0f * p.m_E * c1;
@@ -174,7 +184,6 @@ __device__ __forceinline__ bool contact_slot(const ContactParams& p, const f3 r,
     } else {
         ms = mk3(0.f, 0.f, 0.f);
     }
-    return true;
 }
 
 // rr as the list kernels compute it: __fmul_rn products, summed left to right.
@@ -215,6 +224,35 @@ __device__ __forceinline__ void octant_cells(const f3 x, const RefGrid& g, int64
     const int64_t b = (int64_t)c;
     cells[0] = b;           cells[1] = b + ox;           cells[2] = b + oy;      cells[3] = b + oz;
     cells[4] = b + ox + oy; cells[5] = b + ox + oz;      cells[6] = b + oy + oz; cells[7] = b + ox + oy + oz;
+}
+
+// The same 8 cells as base + offsets (compact form for register-tight kernels).
+struct Octant {
+    int64_t b, ox, oy, oz;
+};
+__device__ __forceinline__ Octant octant_of(const f3 x, const RefGrid& g) {
+    uint32_t ix, iy, iz;
+    const uint32_t c = ref_cell(x, g, &ix, &iy, &iz);
+    const float hx = __fadd_rn((float)ix, 0.5f), hy = __fadd_rn((float)iy, 0.5f), hz = __fadd_rn((float)iz, 0.5f);
+    Octant o;
+    o.b = (int64_t)c;
+    o.ox = signbit(x.x - __fmul_rn(hx, g.a)) ? -1 : 1;
+    o.oy = (signbit(x.y - __fmul_rn(hy, g.a)) ? -1 : 1) * (int64_t)g.nx;
+    o.oz = (signbit(x.z - __fmul_rn(hz, g.a)) ? -1 : 1) * (int64_t)g.ny * g.nx;
+    return o;
+}
+// Rank of cell cj in the visiting order own, +x, +y, +z, +xy, +xz, +yz, +xyz, or -1.
+__device__ __forceinline__ int octant_rank(const Octant& o, uint32_t cj) {
+    const int64_t dlt = (int64_t)cj - o.b;
+    if (dlt == 0) return 0;
+    if (dlt == o.ox) return 1;
+    if (dlt == o.oy) return 2;
+    if (dlt == o.oz) return 3;
+    if (dlt == o.ox + o.oy) return 4;
+    if (dlt == o.ox + o.oz) return 5;
+    if (dlt == o.oy + o.oz) return 6;
+    if (dlt == o.ox + o.oy + o.oz) return 7;
+    return -1;
 }
 
 // Rank (0..7) of cell cj among the octant cells of a particle at x, or -1.

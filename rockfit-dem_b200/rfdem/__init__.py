@@ -13,7 +13,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "librfdem.so")
+LIB_PATH = os.environ.get("RFDEM_LIBRARY") or os.path.join(os.path.dirname(_HERE), "lib", "librfdem.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError("rockfit-b200 engine library not built: %s (run rockfit-dem_b200/build.py)" % LIB_PATH)

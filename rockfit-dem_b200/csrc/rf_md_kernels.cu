@@ -7,6 +7,7 @@
 // counting sort (histogram, scan, scatter, per-cell id order), whose output is
 // the same stable (cell, id) order.
 #include <cstdio>
+#include <mutex>
 #include "rf_physics.cuh"
 
 namespace rf {
@@ -648,3 +649,94 @@ rf_status md_FdotVEntire(const float* V, const float* F, double* FdotV, uint64_t
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Cell binning without any allocation.
+//
+// Some callers cannot allocate device memory at the point where they bin: a host
+// framework that owns every device byte through its own allocator and forbids other
+// allocations, or a latency-critical step loop where cudaMalloc's implicit device
+// synchronisation is not acceptable. md_CellDistribution needs caller-provided
+// scratch; md_CellDistributionNoAlloc instead uses the file-scope device array below
+// as its scratch, so it allocates nothing. The array is fixed in size (cell grids of
+// up to RF_NOALLOC_MAX_CELLS - 1 cells, about 6.3 MB) and every GPU that loads this
+// library holds it until the process exits.
+// ---------------------------------------------------------------------------
+#define RF_NOALLOC_MAX_CELLS (1u << 19)   /* cells + the out-of-grid tail bin */
+#define RF_NOALLOC_WORDS (3u * RF_NOALLOC_MAX_CELLS + 256u)
+static __device__ __align__(256) uint32_t g_noalloc_scratch[RF_NOALLOC_WORDS];
+
+namespace rf {
+namespace {
+// Device address of g_noalloc_scratch per device. In host code the symbol name is
+// only a host-side stand-in, so the address comes from cudaGetSymbolAddress, once
+// per device, with that device current.
+const int kMaxDevices = 64;
+uint32_t* g_noalloc_ptr[kMaxDevices] = {nullptr};
+std::mutex g_noalloc_mu;
+
+rf_status noalloc_scratch(uint32_t** out) {
+    int dev = 0;
+    RF_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) { set_error("md_CellDistributionNoAlloc: device %d out of range", dev); return RF_ERR_INVALID; }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "md_CellDistributionNoAlloc: cudaGetSymbolAddress");
+        g_noalloc_ptr[dev] = (uint32_t*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return RF_OK;
+}
+}  // namespace
+}  // namespace rf
+
+extern "C" rf_status md_CellDistributionNoAlloc(const float* R, uint_fast32_t N, uint_fast32_t* CI,
+                                                uint_fast32_t* CIs, uint_fast32_t* pnC, uint_fast32_t CN,
+                                                float _1d_a, rf_uint3 cN, rf_stream stream) {
+    if (!R || !CI || !CIs || !pnC || N == 0 || CN == 0) {
+        set_error("md_CellDistributionNoAlloc: bad arguments");
+        return RF_ERR_INVALID;
+    }
+    if ((uint64_t)cN.x * cN.y * cN.z != (uint64_t)CN) {
+        set_error("md_CellDistributionNoAlloc: CN != Nr.x*Nr.y*Nr.z");
+        return RF_ERR_INVALID;
+    }
+    if ((uint64_t)CN + 1 > RF_NOALLOC_MAX_CELLS) {
+        set_error("md_CellDistributionNoAlloc: %llu cells exceed the fixed scratch limit of %u cells; "
+                  "use md_CellDistribution with caller scratch", (unsigned long long)CN, RF_NOALLOC_MAX_CELLS - 1);
+        return RF_ERR_INVALID;
+    }
+    uint32_t* base = nullptr;
+    rf_status st = noalloc_scratch(&base);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t cells = (size_t)CN + 1, nb = (cells + 4095) / 4096;
+    uint32_t* counts = base;
+    uint32_t* start = counts + cells;
+    uint32_t* fill = start + cells;
+    uint32_t* bsum = fill + cells;
+    uint32_t* status = base + RF_NOALLOC_WORDS - 1;
+    RefGrid g = make_grid(0.f, _1d_a, cN, CN);
+    // The array keeps the previous call's contents: counters and status start at zero.
+    RF_CUDA(cudaMemsetAsync(counts, 0, cells * sizeof(uint32_t), s));
+    RF_CUDA(cudaMemsetAsync(fill, 0, cells * sizeof(uint32_t), s));
+    RF_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), s));
+    k_cell_index<<<grid_for(N, 256), 256, 0, s>>>(R, N, CI, g, counts, status);
+    k_scan_block_sums<<<(unsigned)nb, 1024, 0, s>>>(counts, cells, bsum);
+    k_scan_totals<<<1, 32, 0, s>>>(bsum, nb);
+    k_scan_apply<<<(unsigned)nb, 1024, 0, s>>>(counts, cells, bsum, start);
+    k_cell_scatter<<<grid_for(N, 256), 256, 0, s>>>(CI, N, CN, start, fill, CIs);
+    k_cell_finish<<<grid_for(cells, 128), 128, 0, s>>>(CI, N, CN, counts, start, CIs, pnC);
+    k_cell_last_run<<<1, 32, 0, s>>>(N, CN, CIs, pnC);
+    RF_CHECK_LAUNCH("md_CellDistributionNoAlloc");
+    uint32_t h = 0;
+    RF_CUDA(cudaMemcpyAsync(&h, status, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    if (h) {
+        set_error("md_CellDistributionNoAlloc: device status %u", h);
+        return (rf_status)h;
+    }
+    return RF_OK;
+}

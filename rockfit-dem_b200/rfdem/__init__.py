@@ -106,6 +106,7 @@ _proto = {
     "md_CalculateCellIndex": (i32, [P, ID, P, f32, u3, P]),
     "md_CellDistributionScratchBytes": (C.c_size_t, [ID, ID]),
     "md_CellDistribution": (i32, [P, ID, P, P, P, ID, f32, u3, P, C.c_size_t, P]),
+    "md_CellDistributionNoAlloc": (i32, [P, ID, P, P, P, ID, f32, u3, P]),
     "md_InteractionListConstruct": (i32, [P, ID, P, P, P, ID, f32, f32, f32, u3, ID, P]),
     "md_InteractionListReConstructBPM": (i32, [P, ID, P, P, P, P, ID, f32, f32, f32, u3, ID, P]),
     "md_DeleteFarLinks": (i32, [P, ID, P, P, P, P, P, P, P, P, P, P, ID, f32, P]),

@@ -313,6 +313,33 @@ typedef struct rf_engine rf_engine;
  * (md_calculationbraziltest.cu:132-144). V, W start at zero.
  */
 rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out);
+
+/*
+ * Extended model (no reference counterpart: the reference is mono-sized FP32 with
+ * global bond constants). Polydisperse particles with FP64 positions; per-particle
+ * mass density*4/3*pi*r^3 (density from t->Po: p_m / p_r^3) and inertia 0.4 m r^2;
+ * bonds between pairs whose gap |r_ij| - r_i - r_j is below gap_frac * min(r_i, r_j),
+ * bond radius bond_lambda * min(r_i, r_j), FP64 rest length, stiffness per area kn
+ * (normal) and ks (shear) in place of E/L0 and G/L0, and tensile / shear strengths
+ * drawn per unordered pair from Weibull(weibull_m) with scales sigma_c and tau_c.
+ * Contacts are the reference's Hertz-Mindlin with equivalent radius and mass. Units
+ * are the reference's (mm, mg, microseconds; stress unit 1e9 Pa).
+ */
+typedef struct rf_ext_params {
+    double kn, ks;            /* bond stiffness per area (stress / length) */
+    double bond_lambda;       /* bond radius / min(r_i, r_j) */
+    double gap_frac;          /* bonding rule */
+    double weibull_m;         /* Weibull modulus of both strengths */
+    double sigma_c, tau_c;    /* Weibull scales of the tensile and shear strength */
+    uint64_t seed;            /* strength stream; a pair draws from (seed, min(i,j), max(i,j)) */
+} rf_ext_params;
+
+/* Create an extended-model engine: h_R double[3N] planar (mm), h_radius double[N].
+   t is prepared as for rf_engine_create; t->Po.a_farcut must exceed 2 * max radius. */
+rf_status rf_engine_create_ext(const rf_task* t, const rf_ext_params* x, const double* h_R,
+                               const double* h_radius, rf_engine** out);
+/* FP64 positions of an extended-model engine, double[3N] planar (host). */
+rf_status rf_engine_positions_f64(rf_engine* e, double* R);
 rf_status rf_engine_destroy(rf_engine* e);
 
 /* Advance nsteps explicit steps (stops early, on device, at fracture / max strain). */
@@ -370,6 +397,21 @@ rf_status rf_specimen_lattice_cylinder(uint64_t seed, double p_r, double gap_fra
 rf_status rf_specimen_lattice_disc(uint64_t seed, double p_r, double gap_frac, double jitter,
                                    double d, double h, const double center[3],
                                    float* R, uint64_t cap, uint64_t* n);
+
+/*
+ * Seeded polydisperse packing on the GPU (the reference generates positions with
+ * cuRAND and relaxes a 1/r repulsion, md_createcylindersample.cu:136-343; this
+ * generator is its own design). N radii r0 * U[rmin, rmax] (r0 in mm, rmin and rmax
+ * relative to it), centres uniform in a cylinder (axis z, height/diameter = aspect)
+ * sized for packing fraction phi, then FIRE with a repulsive Hertz contact (spheres and
+ * container wall) while the radii grow in stages to their targets, until the largest
+ * overlap is below 2e-4 of the smaller radius. Outputs: R double[3N] planar (centred at
+ * center, mm), radius double[N] (mm), the container's diameter and height (mm), and the
+ * final largest relative overlap. aspect 0.5 gives a Brazilian disc (axis z).
+ */
+rf_status rf_pack_cylinder(uint64_t seed, uint64_t N, double r0, double rmin, double rmax, double aspect,
+                           double phi, const double center[3], double* R, double* radius,
+                           double* diameter, double* height, double* max_overlap);
 
 #ifdef __cplusplus
 }

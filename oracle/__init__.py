@@ -57,6 +57,8 @@ def _declare(L):
         "rfo_sum_forces": (None, [T, f64, f64, f64]),
         "rfo_run_f": (u64, [T, P, u64, P, P, P, P, P, P, P, P, P, P, P, u64, P, P]),
         "rfo_run_d": (u64, [T, P, u64, P, P, u64, P, P, P]),
+        "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
+        "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
     }
     for n, (r, a) in proto.items():
         f = getattr(L, n)
@@ -100,6 +102,27 @@ def run_d(task, R0, max_steps):
     steps = L.rfo_run_d(C.byref(task), p(np.ascontiguousarray(R0, np.float32)), max_steps, p(R), p(curve), cap,
                         C.byref(ns), p(ty), C.byref(status))
     return int(steps), R, curve[:3 * min(ns.value, cap)].reshape(-1, 3), ty, status.value
+
+
+def run_ext(task, x, R0, radius, max_steps, fp64=False):
+    """Extended model run (float forces as the engine computes them, or the FP64 oracle).
+    Returns dict(steps, R (double planar, after the pending delete pass), V, IL, ILtype,
+    curve, status, broken)."""
+    L = load()
+    N, K = int(task.N), int(task.K)
+    R = np.array(R0, np.float64, copy=True)
+    rad = np.ascontiguousarray(radius, np.float64)
+    V = np.zeros(3 * N, np.float64 if fp64 else np.float32)
+    IL = np.zeros(N * K, np.uint64)
+    ty = np.zeros(N * K, np.uint8)
+    cap = max(int(max_steps), 1) + 1
+    curve = np.zeros(3 * cap, np.float64)
+    ns, status, broken = C.c_uint64(0), C.c_int(0), C.c_uint64(0)
+    fn = L.rfo_run_ext_d if fp64 else L.rfo_run_ext_f
+    steps = fn(C.byref(task), C.byref(x), p(R), p(rad), max_steps, p(V), p(IL), p(ty), p(curve), cap, C.byref(ns),
+               C.byref(status), C.byref(broken))
+    return dict(steps=int(steps), R=R, V=V, IL=IL, ILtype=ty, curve=curve[:3 * min(ns.value, cap)].reshape(-1, 3),
+                status=status.value, broken=int(broken.value))
 
 
 def ref_gpu():

@@ -830,6 +830,452 @@ struct Run {
 };
 }  // namespace rfo
 
+// ===========================================================================
+// Extended model (polydisperse, FP64 positions, per-bond strengths). This model has
+// no counterpart in the reference: it is the engine's own, and each formula is the
+// reference's with the mono-sized constants replaced (E/L0 -> kn, G/L0 -> ks,
+// b_r -> lambda*min(r_i, r_j), 2 r_P -> r_i + r_j, r_P(r_P - r/2) -> R* delta,
+// m_P/2 -> m*, lever arm r_P -> r_i). The loop is the reference's
+// (md_calculationbraziltest.cu:170-190) with DeleteFarLinks moved to the start of
+// the next step (same positions) and all distance tests on the FP64 positions.
+// TF = float restates the engine's arithmetic operation for operation (bit-exact
+// target); TF = double is the FP64 oracle of the same model.
+// ===========================================================================
+namespace rfo {
+
+template <class T> static inline T rcp(T x) { return (T)1 / x; }
+
+struct ExtPar {
+    double kn, ks, lambda, gap, wm, sig, tau;
+    uint64_t seed;
+};
+
+static inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// Uniform in (0, 1) keyed on the unordered pair (a, b) and a stream number.
+static inline double pair_uniform(uint64_t seed, uint64_t a, uint64_t b, uint32_t stream) {
+    const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+    const uint64_t h = mix64(mix64(seed ^ (0x51ED270B27F3A4C1ull * (stream + 1))) + (hi << 32 | lo));
+    return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+template <class TF>
+struct RunExt {
+    rf_task* t;
+    ExtPar x;
+    uint64_t N, K, CN;
+    std::vector<double> R, rad, L0, sig, tau;
+    std::vector<float> Rf;
+    std::vector<TF> V, W;
+    std::vector<id_t> IL, CI, CIs, pnC;
+    std::vector<uint8_t> type;
+    std::vector<V3<TF>> Rij, Oijt, Mijn, Mijt;
+    double sz0, aa_farcut, aacut;
+    int status;
+    uint64_t steps, broken;
+    TF dt, hm_E, hm_G, p_A, mu, mur, kn, ks, lambda, cmass;
+
+    void to_float() {
+        for (uint64_t q = 0; q < 3 * N; ++q) Rf[q] = (float)R[q];
+    }
+    double rr(uint64_t i, uint64_t j) const {
+        const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
+        return dx * dx + dy * dy + dz * dz;
+    }
+    void zero_slot(uint64_t k) {
+        Rij[k] = {0, 0, 0}; Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
+    }
+
+    void init(const double* R0, const double* r0) {
+        N = t->N; K = t->K; CN = t->C.N;
+        R.assign(R0, R0 + 3 * N); rad.assign(r0, r0 + N); Rf.assign(3 * N, 0.f);
+        V.assign(3 * N, 0); W.assign(3 * N, 0);
+        IL.assign(N * K, EMPTY); type.assign(N * K, 0); L0.assign(N * K, 1.0); sig.assign(N * K, 0.0);
+        tau.assign(N * K, 0.0);
+        Rij.assign(N * K, {0, 0, 0}); Oijt = Rij; Mijn = Rij; Mijt = Rij;
+        CI.assign(N, 0); CIs.assign(2 * N, 0); pnC.assign(2 * CN, 0);
+        sz0 = t->sz0 != 0.0 ? t->sz0 : (double)t->Compress.size.z;
+        status = 0; steps = 0; broken = 0;
+        const rf_potential& P = t->Po;
+        dt = (TF)P.dt; hm_E = (TF)P.hm_E; hm_G = (TF)P.hm_G; p_A = (TF)P.p_A; mu = (TF)P.p_mu; mur = (TF)P.p_mur;
+        kn = (TF)x.kn; ks = (TF)x.ks; lambda = (TF)x.lambda; cmass = (TF)(P.p_m / (P.p_r * P.p_r * P.p_r));
+        aa_farcut = P.aa_farcut; aacut = (double)t->aacut;
+        to_float();
+        const float inv_a = t->C._1d_a, a = t->C.a;
+        int s = cell_distribution<float>(Rf.data(), N, CI.data(), CIs.data(), pnC.data(), CN, inv_a, t->C.Nr);
+        if (s) status = s;
+        s = construct_list<float>(Rf.data(), N, CIs.data(), pnC.data(), IL.data(), K, a, inv_a, t->aacut, t->C.Nr, CN);
+        if (s) status = s;
+        // bonds: gap below gap_frac * min radius; FP64 rest length; Weibull strengths per pair
+        for (uint64_t i = 0; i < N; ++i)
+            for (uint64_t q = 0; q < K; ++q) {
+                const uint64_t k = i * K + q;
+                const id_t j = IL[k];
+                if (j == EMPTY || j >= N) continue;
+                const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
+                const double L = std::sqrt(dx * dx + dy * dy + dz * dz);
+                if (!(L - rad[i] - rad[j] < x.gap * std::fmin(rad[i], rad[j])) || !(L > 0)) continue;
+                type[k] = 1;
+                L0[k] = L;
+                const double us = pair_uniform(x.seed, i, j, 0), ut = pair_uniform(x.seed, i, j, 1);
+                sig[k] = x.sig * std::pow(-std::log(us), 1.0 / x.wm);
+                tau[k] = x.tau * std::pow(-std::log(ut), 1.0 / x.wm);
+                if (sizeof(TF) == 4) { sig[k] = (float)sig[k]; tau[k] = (float)tau[k]; }
+            }
+        // DeleteFarLinks on the float positions, as the initial build does
+        std::vector<V3<float>> z(N * K, {0, 0, 0});
+        delete_far_links<float>(Rf.data(), N, IL.data(), type.data(), z.data(), z.data(), z.data(), z.data(), K,
+                                (float)P.aa_farcut);
+    }
+
+    void delete_far() {
+        for (uint64_t i = 0; i < N; ++i)
+            for (uint64_t q = 0; q < K; ++q) {
+                const uint64_t k = i * K + q;
+                const id_t j = IL[k];
+                if (j == EMPTY || j >= N) continue;
+                const double d2 = rr(i, j);
+                if (d2 > aa_farcut || d2 < 1e-10) { IL[k] = EMPTY; type[k] = 0; zero_slot(k); }
+            }
+    }
+
+    void add_links() {
+        to_float();
+        const float inv_a = t->C._1d_a, a = t->C.a;
+        int s = cell_distribution<float>(Rf.data(), N, CI.data(), CIs.data(), pnC.data(), CN, inv_a, t->C.Nr);
+        if (s && !status) status = s;
+        for (uint64_t i = 0; i < N; ++i) {
+            int64_t cells[8];
+            octant_cells<float>(Rf.data(), N, i, a, inv_a, t->C.Nr, cells);
+            for (int c = 0; c < 8; ++c) {
+                if (cells[c] < 0 || (uint64_t)cells[c] >= CN) continue;
+                const uint64_t start = pnC[cells[c]], cnt = pnC[cells[c] + CN];
+                for (uint64_t m = 0; m < cnt && start + m < N; ++m) {
+                    const id_t j = CIs[start + m + N];
+                    if (j >= N) continue;
+                    const double d2 = rr(i, j);
+                    if (!(d2 < aacut && d2 > 1e-10)) continue;
+                    bool have = false;
+                    for (uint64_t q = 0; q < K; ++q) if (IL[i * K + q] == j) have = true;
+                    if (have) continue;
+                    int64_t kf = -1;
+                    for (uint64_t q = 0; q < K; ++q)
+                        if (IL[i * K + q] == EMPTY) {
+                            // QUIRK (md_interaction_list_reconstructbpm.cu:30-36): particle 0 skips a
+                            // free slot 0 while a later free slot exists
+                            if (i == 0 && q == 0) {
+                                bool later = false;
+                                for (uint64_t u = 1; u < K; ++u) if (IL[u] == EMPTY) later = true;
+                                if (later) continue;
+                            }
+                            kf = (int64_t)q;
+                            break;
+                        }
+                    if (kf < 0) { if (!status) status = ST_ROW_OVERFLOW; continue; }
+                    IL[i * K + kf] = j;
+                    type[i * K + kf] = 0;
+                }
+            }
+        }
+    }
+
+    // One bond slot (engine bond_slot_ext).
+    bool bond(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& vi, const V3<TF>& vj, const V3<TF>& wi,
+              const V3<TF>& wj, TF br, V3<TF>& fs, V3<TF>& ms) {
+        const TF PI = pi_t<TF>();
+        const TF rijm = (TF)rlen;
+        const TF inv_rm = rcp(rijm);
+        const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
+        const TF stretch = (TF)(rlen - L0[k]);
+        const TF A = br * br * PI;
+        const TF J = PI * br * br * br * br;
+        TF cef = kn * stretch;
+        TF Sc = cef;
+        cef *= A;
+        fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
+        V3<TF>& Rk = Rij[k];
+        const TF tx = Rk.y * nz - Rk.z * ny, ty = Rk.z * nx - Rk.x * nz, tz = Rk.x * ny - Rk.y * nx;
+        const TF wsx = wj.x + wi.x, wsy = wj.y + wi.y, wsz = wj.z + wi.z;
+        const TF cphi = (wsx * nx + wsy * ny + wsz * nz) * dt * (TF)0.5f;
+        const TF phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
+        Rk = {nx, ny, nz};
+        const TF M1x = (TF)1.0f + tz * phz + ty * phy, M1y = phz - tz - ty * phx, M1z = -phy - tz * phx + ty;
+        const TF M2x = tz - phz - tx * phy, M2y = tz * phz + (TF)1.0f + tx * phx, M2z = -tz * phy + phx - tx;
+        const TF M3x = -ty - tx * phz + phy, M3y = -ty * phz + tx - phx, M3z = ty * phy + tx * phx + (TF)1.0f;
+        const TF dwx = wj.x - wi.x, dwy = wj.y - wi.y, dwz = wj.z - wi.z;
+        {
+            TF c1 = nx * dwx + ny * dwy + nz * dwz;
+            c1 *= dt * (TF)0.5f * ks;
+            const V3<TF> o = Mijn[k];
+            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
+            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
+            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
+            Mijn[k] = {mx, my, mz};
+            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+        }
+        {
+            const TF c1 = nx * dwx + ny * dwy + nz * dwz;
+            TF c2 = dt * (TF)0.25f * kn;
+            const V3<TF> o = Mijt[k];
+            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
+            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
+            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
+            Mijt[k] = {mx, my, mz};
+            c2 *= J;
+            ms.x += mx * c2; ms.y += my * c2; ms.z += mz * c2;
+        }
+        TF Mc;
+        {
+            const TF hx = (TF)0.5f * wsx, hy = (TF)0.5f * wsy, hz = (TF)0.5f * wsz;
+            const TF vx = vj.x - vi.x - hy * r.z + hz * r.y;
+            const TF vy = vj.y - vi.y - hz * r.x + hx * r.z;
+            const TF vz = vj.z - vi.z - hx * r.y + hy * r.x;
+            TF c = nx * vx + ny * vy + nz * vz;
+            const V3<TF> o = Oijt[k];
+            const TF ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c) * dt;
+            const TF oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (vy - ny * c) * dt;
+            const TF oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (vz - nz * c) * dt;
+            c = ks;
+            Mc = c;
+            c *= A;
+            fs.x += ox * c; fs.y += oy * c; fs.z += oz * c;
+            Oijt[k] = {ox, oy, oz};
+            ms.x += (TF)0.5f * (r.y * oz - r.z * oy) * c;
+            ms.y += (TF)0.5f * (r.z * ox - r.x * oz) * c;
+            ms.z += (TF)0.5f * (r.x * oy - r.y * ox) * c;
+        }
+        const V3<TF>& O = Oijt[k];
+        const V3<TF>& Mt = Mijt[k];
+        const V3<TF>& Mn = Mijn[k];
+        Mc *= norm3(O.x, O.y, O.z);
+        Sc += norm3(Mt.x, Mt.y, Mt.z) * (TF)4.0f * br;
+        Mc += norm3(Mn.x, Mn.y, Mn.z) * (TF)2.0f * br;
+        if ((Sc > (TF)sig[k]) || (Mc > (TF)tau[k])) {
+            Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
+            return true;
+        }
+        return false;
+    }
+
+    // One overlapping pair (engine contact_pair_ext).
+    void contact(uint64_t k, const V3<TF>& r, TF rijm, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
+                 const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms) {
+        const TF inv_rm = rcp(rijm);
+        const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
+        const TF Rs = ri * rj / (ri + rj);
+        const TF ms_ = mi * mj / (mi + mj);
+        const TF delta = ri + rj - rijm;
+        TF c1 = std::sqrt(Rs * std::fabs(delta));
+        const TF Kn = (TF)2.0f * hm_E * c1;
+        const TF Kt = (TF)8.0f * hm_G * c1;
+        const TF ax = ri * wi.x + rj * wj.x, ay = ri * wi.y + rj * wj.y, az = ri * wi.z + rj * wj.z;
+        const TF vx = vj.x - vi.x + (ny * az - nz * ay);
+        const TF vy = vj.y - vi.y + (nz * ax - nx * az);
+        const TF vz = vj.z - vi.z + (nx * ay - ny * ax);
+        const TF vn = nx * vx + ny * vy + nz * vz;
+        const TF fn = -delta * Kn * two_thirds_t<TF>();
+        c1 = (TF)-1.8257f * p_A * vn * std::sqrt(Kn * ms_);
+        fs.x += nx * (fn + c1); fs.y += ny * (fn + c1); fs.z += nz * (fn + c1);
+        const TF vtx = vx - nx * vn, vty = vy - ny * vn, vtz = vz - nz * vn;
+        const V3<TF> o = Oijt[k];
+        TF c = nx * o.x + ny * o.y + nz * o.z;
+        TF ox = o.x - nx * c, oy = o.y - ny * c, oz = o.z - nz * c;
+        c = ox * ox + oy * oy + oz * oz;
+        if ((double)c > 1e-18) {
+            c = rcp(c);
+            c *= o.x * o.x + o.y * o.y + o.z * o.z;
+            c = std::sqrt(c);
+            ox *= c; oy *= c; oz *= c;
+        }
+        ox += vtx * dt; oy += vty * dt; oz += vtz * dt;
+        TF ftx = ox * Kt, fty = oy * Kt, ftz = oz * Kt;
+        const TF ftm = ftx * ftx + fty * fty + ftz * ftz;
+        if (ftm > mu * mu * fn * fn) {
+            c = mu * std::fabs(fn) * rsqrt_rn<TF>(ftm);
+            ftx *= c; fty *= c; ftz *= c;
+            c = rcp(Kt);
+            ox = ftx * c; oy = fty * c; oz = ftz * c;
+        } else {
+            c = (TF)-1.8257f * p_A * std::sqrt(Kt * ms_);
+            ftx += vtx * c; fty += vty * c; ftz += vtz * c;
+        }
+        Oijt[k] = {ox, oy, oz};
+        fs.x += ftx; fs.y += fty; fs.z += ftz;
+        ms.x += (ny * ftz - nz * fty) * ri;
+        ms.y += (nz * ftx - nx * ftz) * ri;
+        ms.z += (nx * fty - ny * ftx) * ri;
+        const TF wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
+        if ((double)wim > 1e-18) {
+            const TF cr = -mur * std::fabs(fn) * rsqrt_rn<TF>(wim);
+            ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
+        } else {
+            ms = {0, 0, 0};    // QUIRK (md_calculateforcesdem3.cu:316-336): clears the contact sum
+        }
+    }
+
+    bool running() const { return t->Compress.Strain < t->Compress.MaxStrain && !t->Compress.Fracture; }
+
+    void step(double* curve, uint64_t cap, uint64_t* nsaved) {
+        rf_compression& Kc = t->Compress;
+        delete_far();                       // the previous step's DeleteFarLinks
+        add_links();
+        std::vector<V3<TF>> Fn(N), Mn(N);
+        for (uint64_t i = 0; i < N; ++i) {
+            const V3<TF> vi = {V[i], V[i + N], V[i + 2 * N]}, wi = {W[i], W[i + N], W[i + 2 * N]};
+            const TF ri = (TF)rad[i];
+            const TF mi = cmass * ri * ri * ri;
+            V3<TF> fsb = {0, 0, 0}, msb = {0, 0, 0}, fsc = {0, 0, 0}, msc = {0, 0, 0};
+            for (uint64_t q = 0; q < K; ++q) {                   // _22 order: bonds by slot
+                const uint64_t k = i * K + q;
+                const id_t j = IL[k];
+                if (j == EMPTY || type[k] != 1) continue;
+                const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
+                const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
+                const TF br = lambda * std::min(ri, (TF)rad[j]);
+                if (bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb)) { type[k] = 0; ++broken; }
+            }
+            for (uint64_t q = 0; q < K; ++q) {                   // _21 order: type-0 slots by slot
+                const uint64_t k = i * K + q;
+                const id_t j = IL[k];
+                if (j == EMPTY || type[k] != 0) continue;
+                const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                const TF rj = (TF)rad[j];
+                const TF rijm = (TF)std::sqrt(d2);
+                if (!(rijm < ri + rj)) { Oijt[k] = {0, 0, 0}; continue; }
+                const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
+                const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
+                contact(k, r, rijm, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsc, msc);
+            }
+            TF Fx = (TF)0 + fsb.x, Fy = (TF)0 + fsb.y, Fz = (TF)0 + fsb.z;
+            Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
+            TF Mx = (TF)0 + msb.x, My = (TF)0 + msb.y, Mz = (TF)0 + msb.z;
+            Mx += msc.x; My += msc.y; Mz += msc.z;
+            Fn[i] = {Fx, Fy, Fz}; Mn[i] = {Mx, My, Mz};
+        }
+        // platen, increments, cut (per particle, in particle order)
+        double sfb = 0, sft = 0;
+        const float cx = Kc.center.x, cy = Kc.center.y, cz = Kc.center.z, RR = Kc.RR;
+        const double Top = Kc.Top, Bottom = Kc.Bottom, TopR = Kc.TopR, BottomR = Kc.BottomR;
+        const TF vt = (TF)(float)Kc.V;
+        const bool brz = t->kind == RF_TEST_BRAZIL;
+        const double Zcut = brz ? (double)(float)((double)t->S.center.y + (double)t->S.spacesized2.y)
+                                : (double)(float)((double)t->S.center.z + (double)t->S.spacesized2.z);
+        const rf_sample& S = t->S;
+        for (uint64_t i = 0; i < N; ++i) {
+            TF Fx = Fn[i].x, Fy = Fn[i].y, Fz = Fn[i].z;
+            double Rx = R[i], Ry = R[i + N], Rz = R[i + 2 * N];
+            TF Vx = V[i], Vy = V[i + N], Vz = V[i + 2 * N];
+            if (brz) {
+                const TF rx = (TF)(float)(Rx - cx), rz = (TF)(float)(Rz - cz);
+                if (rx * rx + rz * rz < (TF)RR && (double)rz < Zcut) {
+                    if (Ry - TopR > -1e-9) {
+                        const TF fy = Fy;
+                        if (fy > 0) {
+                            sft += (double)fy;
+                            TF iv = Vx * Vx + Vz * Vz;
+                            if ((double)iv > 1e-9) {
+                                iv = rsqrt_rn<TF>(iv);
+                                Fx -= (TF)0.45f * fy * Vx * iv;
+                                Fz -= (TF)0.45f * fy * Vz * iv;
+                            }
+                        }
+                        if (Ry - Top > -1e-9) { Ry = Top; Vy = vt; Fy = 0; }
+                    }
+                    if (Ry - BottomR < 1e-9) {
+                        const TF fy = Fy;
+                        if (fy < 0) {
+                            sfb += (double)fy;
+                            TF iv = Vx * Vx + Vz * Vz;
+                            if ((double)iv > 1e-9) {
+                                iv = rsqrt_rn<TF>(iv);
+                                Fx += (TF)0.45f * fy * Vx * iv;
+                                Fz += (TF)0.45f * fy * Vz * iv;
+                            }
+                        }
+                        if (Ry - Bottom < 1e-9) { Ry = Bottom; Vy = 0; Fy = 0; }
+                    }
+                }
+            } else {
+                const TF rx = (TF)(float)(Rx - cx), ry = (TF)(float)(Ry - cy);
+                if (rx * rx + ry * ry < (TF)RR && Rz < Zcut) {
+                    if (Rz - TopR > -1e-9) {
+                        if (Fz > 0) sft += (double)Fz;
+                        if (Rz - Top > -1e-9) { Rz = Top; Vz = vt; Fz = 0; }
+                    }
+                    if (Rz - BottomR < 1e-9) {
+                        if (Fz < 0) sfb += (double)Fz;
+                        if (Rz - Bottom < 1e-9) { Rz = Bottom; Vz = 0; Fz = 0; }
+                    }
+                }
+            }
+            const TF ri = (TF)rad[i];
+            const TF mi = cmass * ri * ri * ri;
+            const TF dtm = dt / mi, dtI = dt / ((TF)0.4f * mi * ri * ri);
+            Vx += Fx * dtm; Vy += Fy * dtm; Vz += Fz * dtm;
+            Rx += (double)(Vx * dt); Ry += (double)(Vy * dt); Rz += (double)(Vz * dt);
+            W[i] += Mn[i].x * dtI; W[i + N] += Mn[i].y * dtI; W[i + 2 * N] += Mn[i].z * dtI;
+            const double dx = Rx - S.center.x, dy = Ry - S.center.y, dz = Rz - S.center.z;
+            if ((dx - S.spacesized2.x > 0) || (dx + S.spacesized2.x < 0) || (dy - S.spacesized2.y > 0) ||
+                (dy + S.spacesized2.y < 0) || (dz - S.spacesized2.z > 0) || (dz + S.spacesized2.z < 0)) {
+                Rx = S.hidenpoint.x; Ry = S.hidenpoint.y; Rz = S.hidenpoint.z;
+                Vx = 0; Vy = 0; Vz = 0;
+            }
+            R[i] = Rx; R[i + N] = Ry; R[i + 2 * N] = Rz;
+            V[i] = Vx; V[i + N] = Vy; V[i + 2 * N] = Vz;
+        }
+        sum_forces(t, sfb, sft, sz0, curve, cap, nsaved);
+        compress(t, Kc.Stress);
+        ++steps;
+    }
+};
+
+template <class TF>
+static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const double* rad, uint64_t max_steps,
+                        TF* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,
+                        uint64_t* nsaved, int* status, uint64_t* broken) {
+    RunExt<TF> r;
+    r.t = t;
+    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed};
+    r.init(R_io, rad);
+    uint64_t ns = 0;
+    while (r.running() && r.steps < max_steps) r.step(curve, cap, &ns);   // max_steps 0: bonds only
+    r.delete_far();                         // the pending DeleteFarLinks of the last step
+    if (nsaved) *nsaved = ns;
+    std::memcpy(R_io, r.R.data(), sizeof(double) * 3 * r.N);
+    if (V_out) std::memcpy(V_out, r.V.data(), sizeof(TF) * 3 * r.N);
+    if (IL_out) std::memcpy(IL_out, r.IL.data(), sizeof(uint64_t) * r.N * r.K);
+    if (type_out) std::memcpy(type_out, r.type.data(), r.N * r.K);
+    if (status) *status = r.status;
+    if (broken) *broken = r.broken;
+    return r.steps;
+}
+
+}  // namespace rfo
+
+extern "C" {
+// Extended model, float forces (the engine's arithmetic) and FP64 (the FP64 oracle).
+// R_io: double[3N] planar in, final positions out (after the pending delete pass).
+uint64_t rfo_run_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,
+                       float* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,
+                       uint64_t* nsaved, int* status, uint64_t* broken) {
+    return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
+                               broken);
+}
+uint64_t rfo_run_ext_d(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,
+                       double* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,
+                       uint64_t* nsaved, int* status, uint64_t* broken) {
+    return rfo::run_ext<double>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
+                                broken);
+}
+}  // extern "C"
+
 extern "C" {
 int rfo_task_prepare(rf_task* t, const double ss[3], const double ls[3], double cell_a, double vload,
                      double minstress, double maxstrain) {

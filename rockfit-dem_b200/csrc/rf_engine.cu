@@ -73,9 +73,18 @@ struct Consts {
     unsigned long long curve_cap;
     cudaGraphConditionalHandle h_loop, h_rebuild;
     int use_graph;
+    // extended model (ext != 0): FP64 positions with radii, per-bond strengths
+    int ext;
+    ExtParams ep;
+    float kn, ks, br_lambda, cmass;     // bond stiffness per area, bond radius / min(r_i, r_j), mass = cmass r^3
+    double aa_farcut_d, aacut_d;
+    double Top_shift;                   // unused (reserved)
 };
 
 struct Dev {
+    double4* posd[2];   // extended model: x, y, z (FP64) and radius
+    double* bL0;        // extended model: [QB][N] rest length of each bond record
+    float2* bstr;       // extended model: [QB][N] tensile and shear strength of each bond record
     float4* pos[2];
     float4* vel[2];
     float4* ang[2];
@@ -112,6 +121,14 @@ struct Dev {
 };
 
 __device__ __forceinline__ f3 f4to3(const float4 v) { return mk3(v.x, v.y, v.z); }
+// Position of particle j as float4 (x, y, z, radius) in either model.
+__device__ __forceinline__ float4 posf(const Dev& d, const Consts& c, uint32_t buf, uint32_t j) {
+    if (c.ext) {
+        const double4 p = d.posd[buf][j];
+        return make_float4((float)p.x, (float)p.y, (float)p.z, (float)p.w);
+    }
+    return d.pos[buf][j];
+}
 __device__ __forceinline__ void zero_record(const Dev& d, size_t QN, size_t s) {
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     d.bst[s] = z; d.bst[s + QN] = z; d.bst[s + 2 * QN] = z;
@@ -145,9 +162,9 @@ __global__ void k_rb_zero(Dev d, Consts c) {
 
 __global__ void k_rb_bin(Dev d, Consts c) {
     if (gate_closed(d, c)) return;
-    const float4* P = d.pos[d.sc->steps & 1];
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
-        uint32_t key = cg_cell_of(P[i], c);
+        uint32_t key = cg_cell_of(posf(d, c, cur, i), c);
         if (key == 0xFFFFFFFFu) key = c.cg_cells;          // parked or outside: tail bin, no candidates
         d.cg_key[i] = key;
         atomicAdd(&d.cg_count[key], 1u);
@@ -215,9 +232,9 @@ __global__ void k_rb_scatter(Dev d, Consts c) {
 // Candidates: every j != i within rc of i (27 cells), and which of them sit in i's row.
 __global__ void k_rb_cand(Dev d, Consts c) {
     if (gate_closed(d, c)) return;
-    const float4* P = d.pos[d.sc->steps & 1];
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
-        const float4 xi = P[i];
+        const float4 xi = posf(d, c, cur, i);
         d.pos_ref[i] = xi;
         const uint32_t key = d.cg_key[i];
         uint32_t n = 0;
@@ -237,7 +254,7 @@ __global__ void k_rb_cand(Dev d, Consts c) {
                         for (uint32_t q = s; q < e; ++q) {
                             const uint32_t j = d.cg_sorted[q];
                             if (j == i) continue;
-                            const float4 xj = P[j];
+                            const float4 xj = posf(d, c, cur, j);
                             const float ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
                             if (ddx * ddx + ddy * ddy + ddz * ddz < c.rc2) {
                                 if (n < c.KC) d.cand[(size_t)n * c.N + i] = j;
@@ -334,6 +351,98 @@ __global__ void k_delete_pending(Dev d, Consts c) {
     delete_far(d, c, P, i, xi, ncand, nbq, live, bond, cm, bmask, mem);
     if (valid && live != live0) {
         d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.member[i] = mem; d.bmask[i] = bmask;
+    }
+}
+
+// End of a step: block partial sums of the platen loads (fixed tree, deterministic);
+// the last block to finish does SumForcesULoading (md_results.cu:34-74) and
+// CompressB/U (md_data_types.h:223-293) and sets the graph conditions.
+template <int KIND>
+__device__ __forceinline__ void step_finish(const Dev& d, const Consts& c, double sfb, double sft,
+                                            uint32_t nbroken, uint32_t moved) {
+    DevScalars* sc = d.sc;
+    const uint32_t FULL = 0xffffffffu;
+    // ---- block reductions (fixed tree: deterministic)
+    __shared__ double s_b[4], s_t[4];
+    __shared__ uint32_t s_n[4], s_m[4];
+    __shared__ bool s_last;
+    for (int o = 16; o; o >>= 1) {
+        sfb += __shfl_xor_sync(FULL, sfb, o);
+        sft += __shfl_xor_sync(FULL, sft, o);
+    }
+    const uint32_t wn = __reduce_add_sync(FULL, nbroken), wm = __reduce_or_sync(FULL, moved);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { s_b[w] = sfb; s_t[w] = sft; s_n[w] = wn; s_m[w] = wm; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double b = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
+        const double t = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
+        d.partial[blockIdx.x] = make_double2(b, t);
+        const uint32_t nb = s_n[0] + s_n[1] + s_n[2] + s_n[3];
+        if (nb) atomicAdd(&sc->broken, (unsigned long long)nb);
+        if (s_m[0] | s_m[1] | s_m[2] | s_m[3]) atomicOr(&sc->moved, 1u);
+        __threadfence();
+        const uint32_t ticket = atomicAdd(&sc->block_counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+
+    // ---- last block: SumForcesULoading (md_results.cu:34-74) and CompressB/U
+    __threadfence();
+    double pb = 0.0, pt = 0.0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        const double2 v = __ldcg(&d.partial[b]);
+        pb += v.x; pt += v.y;
+    }
+    for (int o = 16; o; o >>= 1) {
+        pb += __shfl_xor_sync(FULL, pb, o);
+        pt += __shfl_xor_sync(FULL, pt, o);
+    }
+    __syncthreads();
+    if (l == 0) { s_b[w] = pb; s_t[w] = pt; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const double sfb_all = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
+    const double sft_all = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
+    sc->block_counter = 0;
+    // curve record and stress
+    const double a1 = (double)sc->_1d_Area;
+    if (sc->curve_n < c.curve_cap) {
+        double* rec = d.curve + 3 * sc->curve_n;
+        rec[0] = (sc->size_d[2] - sc->sz0) / sc->sz0;
+        rec[1] = sfb_all * a1;
+        rec[2] = sft_all * a1;
+    }
+    sc->curve_n += 1;
+    sc->Stress = 0.5 * (fabs(sfb_all) + fabs(sft_all)) * a1;
+    if (!sc->Loading && sc->Stress > sc->MinStress) sc->Loading = 1;
+    if (sc->FractureStress < sc->Stress) {
+        sc->FractureStress = sc->Stress;
+        sc->FractureStrain = (sc->sz0 - sc->size_d[2]) / sc->sz0;
+    }
+    if (sc->Loading && sc->Stress < sc->ZeroStress) sc->Fracture = 1;
+    // CompressU / CompressB (md_data_types.h:223-293)
+    const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+    sc->V = (sc->Stress < 1e-9) ? 10.0 * sc->VLoad : sc->VLoad;
+    sc->size_d[ax] += sc->V * c.dt_d;
+    sc->Top += sc->V * c.dt_d;
+    sc->TopR = sc->Top - 2.0 * c.p_r_d;
+    sc->size[ax] = (float)sc->size_d[ax];
+    sc->sized2[ax] = (float)(0.5 * sc->size_d[ax]);
+    sc->center_d[ax] += sc->V * c.dt_d;
+    sc->center[ax] = (float)sc->center_d[ax];
+    sc->Hd2 = sc->sized2[ax];
+    sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
+    sc->steps += 1;
+    const bool running = (sc->Strain < sc->MaxStrain) && !sc->Fracture;
+    sc->done = running ? 0u : 1u;
+    const uint32_t mv = sc->moved;
+    sc->moved = 0;
+    sc->rebuild = mv;
+    if (c.use_graph) {
+        cudaGraphSetConditional(c.h_rebuild, mv ? 1u : 0u);
+        cudaGraphSetConditional(c.h_loop, (running && sc->steps < sc->target) ? 1u : 0u);
     }
 }
 
@@ -550,88 +659,289 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
         moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
     }
 
-    // ---- block reductions (fixed tree: deterministic)
-    __shared__ double s_b[4], s_t[4];
-    __shared__ uint32_t s_n[4], s_m[4];
-    __shared__ bool s_last;
-    for (int o = 16; o; o >>= 1) {
-        sfb += __shfl_xor_sync(FULL, sfb, o);
-        sft += __shfl_xor_sync(FULL, sft, o);
-    }
-    const uint32_t wn = __reduce_add_sync(FULL, nbroken), wm = __reduce_or_sync(FULL, moved);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0) { s_b[w] = sfb; s_t[w] = sft; s_n[w] = wn; s_m[w] = wm; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const double b = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
-        const double t = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
-        d.partial[blockIdx.x] = make_double2(b, t);
-        const uint32_t nb = s_n[0] + s_n[1] + s_n[2] + s_n[3];
-        if (nb) atomicAdd(&sc->broken, (unsigned long long)nb);
-        if (s_m[0] | s_m[1] | s_m[2] | s_m[3]) atomicOr(&sc->moved, 1u);
-        __threadfence();
-        const uint32_t ticket = atomicAdd(&sc->block_counter, 1u);
-        s_last = (ticket == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!s_last) return;
+    step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
+}
 
-    // ---- last block: SumForcesULoading (md_results.cu:34-74) and CompressB/U
-    __threadfence();
-    double pb = 0.0, pt = 0.0;
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-        const double2 v = __ldcg(&d.partial[b]);
-        pb += v.x; pt += v.y;
+// ===========================================================================
+// Extended model step: FP64 positions (x, y, z, radius), per-particle mass and
+// inertia from the radius, bond records with an FP64 rest length and their own
+// strengths, contacts with equivalent radius and mass. Same structure and order as
+// k_step; list maintenance compares FP64 squared distances.
+// ===========================================================================
+// Read-only load of a 32-byte particle record (two 16-byte loads of one sector pair).
+__device__ __forceinline__ double4 ldg_d4(const double4* p) {
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ double3 dsub(const double4 a, const double4 b) {
+    return make_double3(a.x - b.x, a.y - b.y, a.z - b.z);
+}
+__device__ __forceinline__ double dlen2(const double3 r) { return r.x * r.x + r.y * r.y + r.z * r.z; }
+
+__device__ __forceinline__ void delete_far_ext(const Dev& d, const Consts& c, const double4* __restrict__ P,
+                                               uint32_t i, const double4 xi, uint32_t ncand, uint32_t nbq,
+                                               uint32_t& live, uint32_t& bond, uint32_t& cm, uint32_t& bmask,
+                                               unsigned long long& mem) {
+    const uint32_t* row = d.ids + (size_t)i * c.K;
+    uint32_t m = live;
+    while (m) {
+        const uint32_t k = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t j = row[k];
+        const double rr = dlen2(dsub(ldg_d4(&P[j]), xi));
+        if (rr > c.aa_farcut_d || rr < 1e-10) delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
     }
-    for (int o = 16; o; o >>= 1) {
-        pb += __shfl_xor_sync(FULL, pb, o);
-        pt += __shfl_xor_sync(FULL, pt, o);
+}
+
+__global__ void k_delete_pending_ext(Dev d, Consts c) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const double4* P = d.posd[d.sc->steps & 1ull];
+    uint32_t live = d.live[i], bond = d.bond[i], cm = d.cmask[i], ncand = d.cand_n[i], nbq = d.nbq[i],
+             bmask = d.bmask[i];
+    unsigned long long mem = d.member[i];
+    const uint32_t live0 = live;
+    delete_far_ext(d, c, P, i, P[i], ncand, nbq, live, bond, cm, bmask, mem);
+    if (live != live0) {
+        d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.member[i] = mem; d.bmask[i] = bmask;
     }
-    __syncthreads();
-    if (l == 0) { s_b[w] = pb; s_t[w] = pt; }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    const double sfb_all = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
-    const double sft_all = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
-    sc->block_counter = 0;
-    // curve record and stress
-    const double a1 = (double)sc->_1d_Area;
-    if (sc->curve_n < c.curve_cap) {
-        double* rec = d.curve + 3 * sc->curve_n;
-        rec[0] = (sc->size_d[2] - sc->sz0) / sc->sz0;
-        rec[1] = sfb_all * a1;
-        rec[2] = sft_all * a1;
+}
+
+// Platen contact and clamp with FP64 positions (d_UniaxialCompression3_simple /
+// d_braziltest_simple2 with the coordinates kept in double).
+__device__ __forceinline__ void uniaxial_particle_ext(double& Rx, double& Ry, double& Rz, float& Vz, float& Fz,
+                                                      const rf_float3 c, float RR, double Zt, double Zb, double Ztr,
+                                                      double Zbr, float vt, double Zcut, double& sfb, double& sft) {
+    const float rx = (float)(Rx - c.x), ry = (float)(Ry - c.y);
+    const double rz = Rz;
+    if (rx * rx + ry * ry < RR && rz < Zcut) {
+        if (rz - Ztr > -1e-9) {
+            if (Fz > 0) sft += (double)Fz;
+            if (rz - Zt > -1e-9) { Rz = Zt; Vz = vt; Fz = 0.f; }
+        }
+        if (rz - Zbr < 1e-9) {
+            if (Fz < 0) sfb += (double)Fz;
+            if (rz - Zb < 1e-9) { Rz = Zb; Vz = 0.f; Fz = 0.f; }
+        }
     }
-    sc->curve_n += 1;
-    sc->Stress = 0.5 * (fabs(sfb_all) + fabs(sft_all)) * a1;
-    if (!sc->Loading && sc->Stress > sc->MinStress) sc->Loading = 1;
-    if (sc->FractureStress < sc->Stress) {
-        sc->FractureStress = sc->Stress;
-        sc->FractureStrain = (sc->sz0 - sc->size_d[2]) / sc->sz0;
+}
+__device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, double& Rz, float& Vx, float& Vy,
+                                                    float& Vz, float& Fx, float& Fy, float& Fz, const rf_float3 c,
+                                                    float RR, double Yt, double Yb, double Ytr, double Ybr, float vt,
+                                                    double Zcut, double& sfb, double& sft) {
+    const float rx = (float)(Rx - c.x), rz = (float)(Rz - c.z);
+    const double ry = Ry;
+    if (rx * rx + rz * rz < RR && (double)rz < Zcut) {
+        if (ry - Ytr > -1e-9) {
+            const float fy = Fy;
+            if (fy > 0) {
+                sft += (double)fy;
+                float iv = Vx * Vx + Vz * Vz;
+                if ((double)iv > 1e-9) {
+                    iv = __frsqrt_rn(iv);
+                    Fx -= 0.45f * fy * Vx * iv;
+                    Fz -= 0.45f * fy * Vz * iv;
+                }
+            }
+            if (ry - Yt > -1e-9) { Ry = Yt; Vy = vt; Fy = 0.f; }
+        }
+        if (ry - Ybr < 1e-9) {
+            const float fy = Fy;
+            if (fy < 0) {
+                sfb += (double)fy;
+                float iv = Vx * Vx + Vz * Vz;
+                if ((double)iv > 1e-9) {
+                    iv = __frsqrt_rn(iv);
+                    Fx += 0.45f * fy * Vx * iv;
+                    Fz += 0.45f * fy * Vz * iv;
+                }
+            }
+            if (ry - Yb < 1e-9) { Ry = Yb; Vy = 0.f; Fy = 0.f; }
+        }
     }
-    if (sc->Loading && sc->Stress < sc->ZeroStress) sc->Fracture = 1;
-    // CompressU / CompressB (md_data_types.h:223-293)
-    const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
-    sc->V = (sc->Stress < 1e-9) ? 10.0 * sc->VLoad : sc->VLoad;
-    sc->size_d[ax] += sc->V * c.dt_d;
-    sc->Top += sc->V * c.dt_d;
-    sc->TopR = sc->Top - 2.0 * c.p_r_d;
-    sc->size[ax] = (float)sc->size_d[ax];
-    sc->sized2[ax] = (float)(0.5 * sc->size_d[ax]);
-    sc->center_d[ax] += sc->V * c.dt_d;
-    sc->center[ax] = (float)sc->center_d[ax];
-    sc->Hd2 = sc->sized2[ax];
-    sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
-    sc->steps += 1;
-    const bool running = (sc->Strain < sc->MaxStrain) && !sc->Fracture;
-    sc->done = running ? 0u : 1u;
-    const uint32_t mv = sc->moved;
-    sc->moved = 0;
-    sc->rebuild = mv;
-    if (c.use_graph) {
-        cudaGraphSetConditional(c.h_rebuild, mv ? 1u : 0u);
-        cudaGraphSetConditional(c.h_loop, (running && sc->steps < sc->target) ? 1u : 0u);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Consts c) {
+    DevScalars* sc = d.sc;
+    if (c.use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c.h_loop, 0u);
+    if (sc->done) return;
+    const uint32_t cur = (uint32_t)(sc->steps & 1ull), nxt = cur ^ 1u;
+    const double4* __restrict__ P = d.posd[cur];
+    const float4* __restrict__ Vv = d.vel[cur];
+    const float4* __restrict__ Wv = d.ang[cur];
+    const uint32_t N = c.N;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < N;
+    const uint32_t FULL = 0xffffffffu;
+    const double Top = sc->Top, Bottom = sc->Bottom, TopR = sc->TopR, BottomR = sc->BottomR;
+    const float vt = (float)sc->V, RR = sc->RR;
+    rf_float3 cc;
+    cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
+
+    double4 xi = make_double4(0, 0, 0, 1);
+    f3 vi = mk3(0.f, 0.f, 0.f), wi = vi;
+    uint32_t live = 0, bond = 0, cm = 0, nbq = 0, bmask = 0, ncand = 0;
+    unsigned long long mem = 0ull;
+    if (valid) {
+        xi = P[i]; vi = f4to3(Vv[i]); wi = f4to3(Wv[i]);
+        live = d.live[i]; bond = d.bond[i]; cm = d.cmask[i];
+        mem = d.member[i]; ncand = d.cand_n[i];
+        nbq = d.nbq[i]; bmask = d.bmask[i];
     }
+    const float ri = (float)xi.w;
+    const float mi = c.cmass * ri * ri * ri;
+    const uint32_t live0 = live, bond0 = bond, cm0 = cm, bmask0 = bmask;
+    const unsigned long long mem0 = mem;
+    const size_t QN = (size_t)d.QB * N;
+    const ExtParams& ep = c.ep;
+
+    f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
+    uint32_t nbroken = 0;
+    {
+        const uint32_t wb = __reduce_or_sync(FULL, bmask);
+        const uint32_t qend = 32u - __clz(wb);
+        for (uint32_t q = 0; q < qend; ++q) {
+            if (!((bmask >> q) & 1u)) continue;
+            const size_t s = (size_t)q * N + i;
+            const uint32_t j = __ldg(&d.bj[s]);
+            const double4 xj = ldg_d4(&P[j]);
+            const double3 rd = dsub(xj, xi);
+            const double rr = dlen2(rd);
+            if (rr > c.aa_farcut_d || rr < 1e-10) {
+                delete_slot(d, c, i, d.bk[s], j, ncand, nbq, live, bond, cm, bmask, mem);
+                continue;
+            }
+            const float4 s0 = d.bst[s], s1 = d.bst[s + QN], s2 = d.bst[s + 2 * QN];
+            const float2 str = __ldg(&d.bstr[s]);
+            BondExt b;
+            b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ri, (float)xj.w);
+            b.sc = str.x; b.tc = str.y; b.L0 = __ldg(&d.bL0[s]);
+            const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
+            f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
+            f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
+            const bool broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(__ldg(&Vv[j])), wi, f4to3(__ldg(&Wv[j])),
+                                             rij, oijt, mijn, mijt, fsb, msb);
+            d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
+            d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
+            d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
+            if (broke) { bmask &= ~(1u << q); bond &= ~(1u << d.bk[s]); ++nbroken; }
+        }
+    }
+
+    const uint32_t* row = d.ids + (size_t)i * c.K;
+    const float* oin = d.cO[cur] + (size_t)i * c.K * 3;
+    float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
+    f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
+    uint32_t cm_out = 0;
+    auto contact_pass = [&](bool with_delete) {
+        uint32_t m = live & ~bond;
+        while (m) {
+            const uint32_t k = __ffs(m) - 1;
+            m &= m - 1;
+            const uint32_t j = row[k];
+            const double4 xj = ldg_d4(&P[j]);
+            const double3 rd = dsub(xj, xi);
+            const double rr = dlen2(rd);
+            if (with_delete && (rr > c.aa_farcut_d || rr < 1e-10)) {
+                delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
+                continue;
+            }
+            const float rj = (float)xj.w;
+            const float rijm = (float)sqrt(rr);
+            if (!(rijm < ri + rj)) continue;
+            const uint32_t bit = 1u << k;
+            // cm: step-start contacts minus slots deleted this step (a refilled slot starts at zero)
+            f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
+            const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
+            contact_pair_ext(ep, r, rijm, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(__ldg(&Vv[j])), wi,
+                             f4to3(__ldg(&Wv[j])), o, fsc, msc);
+            oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
+            cm_out |= bit;
+        }
+    };
+    contact_pass(true);
+
+    bool replay = false;
+    if (valid) {
+        unsigned long long tried = mem;
+        bool have_cells = false;
+        Octant oc;
+        const f3 xif = mk3((float)xi.x, (float)xi.y, (float)xi.z);
+        for (;;) {
+            unsigned long long best = ~0ull;
+            uint32_t best_q = 0;
+            for (uint32_t q = 0; q < ncand; ++q) {
+                if ((tried >> q) & 1ull) continue;
+                const uint32_t j = __ldg(&d.cand[(size_t)q * N + i]);
+                const double4 xj = ldg_d4(&P[j]);
+                const double rr = dlen2(dsub(xj, xi));
+                if (!(rr < c.aacut_d && rr > 1e-10)) continue;
+                if (!have_cells) { oc = octant_of(xif, c.g); have_cells = true; }
+                const int rank = octant_rank(oc, ref_cell(mk3((float)xj.x, (float)xj.y, (float)xj.z), c.g));
+                if (rank < 0) continue;
+                const unsigned long long key = ((unsigned long long)rank << 32) | j;
+                if (key < best) { best = key; best_q = q; }
+            }
+            if (best == ~0ull) break;
+            tried |= 1ull << best_q;
+            const uint32_t free = ~live & (c.K >= 32 ? 0xffffffffu : ((1u << c.K) - 1u));
+            if (!free) { raise_status(&sc->err, RF_ERR_ROW_OVERFLOW); continue; }
+            uint32_t k;
+            if (i == 0 && (free & 1u) && (free & ~1u)) k = __ffs(free & ~1u) - 1;
+            else k = __ffs(free) - 1;
+            const uint32_t j = (uint32_t)(best & 0xffffffffull);
+            d.ids[(size_t)i * c.K + k] = j;
+            live |= 1u << k;
+            mem |= 1ull << best_q;
+            const double4 xj = ldg_d4(&P[j]);
+            if ((float)sqrt(dlen2(dsub(xj, xi))) < ri + (float)xj.w) replay = true;
+        }
+    }
+    if (replay) {
+        fsc = mk3(0.f, 0.f, 0.f); msc = fsc; cm_out = 0;
+        contact_pass(false);
+    }
+    cm = cm_out;
+
+    double sfb = 0.0, sft = 0.0;
+    uint32_t moved = 0;
+    if (valid) {
+        if (live != live0) d.live[i] = live;
+        if (bond != bond0) d.bond[i] = bond;
+        if (cm != cm0) d.cmask[i] = cm;
+        if (mem != mem0) d.member[i] = mem;
+        if (bmask != bmask0) d.bmask[i] = bmask;
+        float Fx = 0.0f + fsb.x, Fy = 0.0f + fsb.y, Fz = 0.0f + fsb.z;
+        Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
+        float Mx = 0.0f + msb.x, My = 0.0f + msb.y, Mz = 0.0f + msb.z;
+        Mx += msc.x; My += msc.y; Mz += msc.z;
+        double Rx = xi.x, Ry = xi.y, Rz = xi.z;
+        float Vx = vi.x, Vy = vi.y, Vz = vi.z;
+        if (KIND == RF_TEST_BRAZIL)
+            brazil_particle_ext(Rx, Ry, Rz, Vx, Vy, Vz, Fx, Fy, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt,
+                                (double)c.zcut, sfb, sft);
+        else
+            uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)c.zcut, sfb,
+                                  sft);
+        const float dtm = ep.dt / mi, dtI = ep.dt / (0.4f * mi * ri * ri);
+        Vx += Fx * dtm; Vy += Fy * dtm; Vz += Fz * dtm;
+        Rx += (double)(Vx * ep.dt); Ry += (double)(Vy * ep.dt); Rz += (double)(Vz * ep.dt);
+        const float Wx = wi.x + Mx * dtI, Wy = wi.y + My * dtI, Wz = wi.z + Mz * dtI;
+        const double dx = Rx - c.box_c.x, dy = Ry - c.box_c.y, dz = Rz - c.box_c.z;
+        if ((dx - c.box_h.x > 0) || (dx + c.box_h.x < 0) || (dy - c.box_h.y > 0) || (dy + c.box_h.y < 0) ||
+            (dz - c.box_h.z > 0) || (dz + c.box_h.z < 0)) {
+            Rx = c.hp.x; Ry = c.hp.y; Rz = c.hp.z;
+            Vx = 0.f; Vy = 0.f; Vz = 0.f;
+        }
+        d.posd[nxt][i] = make_double4(Rx, Ry, Rz, xi.w);
+        d.vel[nxt][i] = make_float4(Vx, Vy, Vz, 0.f);
+        d.ang[nxt][i] = make_float4(Wx, Wy, Wz, 0.f);
+        const float4 pr = d.pos_ref[i];
+        const float ex = (float)Rx - pr.x, ey = (float)Ry - pr.y, ez = (float)Rz - pr.z;
+        moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+    }
+    step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
 }
 
 // Sets both graph conditions at the start of a launch.
@@ -696,7 +1006,8 @@ __global__ void k_count_records(const uint_fast32_t* __restrict__ IL, const uint
 __global__ void k_rows_import(const uint_fast32_t* __restrict__ IL, const uint8_t* __restrict__ type,
                               const float* __restrict__ iL, const rf_float3* __restrict__ Rij,
                               const rf_float3* __restrict__ Oijt, const rf_float3* __restrict__ Mijn,
-                              const rf_float3* __restrict__ Mijt, Dev d, Consts c) {
+                              const rf_float3* __restrict__ Mijt, const double* __restrict__ L0x,
+                              const float2* __restrict__ strx, Dev d, Consts c) {
     const uint_fast32_t E = empty_id<uint_fast32_t>();
     const size_t QN = (size_t)d.QB * c.N;
     const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
@@ -722,6 +1033,7 @@ __global__ void k_rows_import(const uint_fast32_t* __restrict__ IL, const uint8_
                 d.bst[b] = make_float4(Rij[r].x, Rij[r].y, Rij[r].z, ox);
                 d.bst[b + QN] = make_float4(oy, oz, Mijn[r].x, Mijn[r].y);
                 d.bst[b + 2 * QN] = make_float4(Mijn[r].z, Mijt[r].x, Mijt[r].y, Mijt[r].z);
+                if (L0x) { d.bL0[b] = L0x[r]; d.bstr[b] = strx[r]; }
                 if (t1) bmask |= 1u << nq;
                 ++nq;
             }
@@ -729,6 +1041,7 @@ __global__ void k_rows_import(const uint_fast32_t* __restrict__ IL, const uint8_
         for (uint32_t q = nq; q < d.QB; ++q) {          // unused records: retired, zero
             const size_t b = (size_t)q * c.N + i;
             d.bj[b] = 0; d.bk[b] = 0xFF; d.bil[b] = 0.f;
+            if (L0x) { d.bL0[b] = 1.0; d.bstr[b] = make_float2(0.f, 0.f); }
             zero_record(d, QN, b);
         }
         d.live[i] = live; d.bond[i] = bond; d.cmask[i] = cm; d.nbq[i] = nq; d.bmask[i] = bmask;
@@ -768,6 +1081,68 @@ __global__ void k_rows_export(uint_fast32_t* __restrict__ IL, uint8_t* __restric
     }
 }
 
+// Bond construction of the extended model: slot (i, k) -> j becomes a bond when the
+// gap |r_ij| - r_i - r_j is below gap_frac * min(r_i, r_j) (distances in double). The
+// rest length is |r_ij| in double; tensile and shear strengths are Weibull draws
+// scale * (-ln U)^(1/m) keyed on the unordered pair, so both directed slots of a pair
+// share them. The slot state starts at zero, as d_ConstructBoundInteractions leaves it.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double pair_uniform(uint64_t seed, uint32_t a, uint32_t b, uint32_t stream) {
+    const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+    const uint64_t h = mix64(mix64(seed ^ (0x51ED270B27F3A4C1ull * (stream + 1))) + (hi << 32 | lo));
+    return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);       // in (0, 1)
+}
+__global__ void k_bond_ext(const double4* __restrict__ P, const uint_fast32_t* __restrict__ IL,
+                           uint8_t* __restrict__ type, float* __restrict__ iL, double* __restrict__ L0x,
+                           float2* __restrict__ strx, uint32_t N, uint32_t K, double gap_frac, double wm,
+                           double sig, double tau, uint64_t seed) {
+    const uint_fast32_t E = empty_id<uint_fast32_t>();
+    const double inv_m = 1.0 / wm;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double4 xi = P[i];
+        for (uint32_t k = 0; k < K; ++k) {
+            const size_t r = (size_t)i * K + k;
+            const uint_fast32_t j = IL[r];
+            type[r] = 0; iL[r] = 0.f; L0x[r] = 1.0; strx[r] = make_float2(0.f, 0.f);
+            if (j == E || j >= N) continue;
+            const double4 xj = P[j];
+            const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+            const double L = sqrt(dx * dx + dy * dy + dz * dz);
+            if (!(L - xi.w - xj.w < gap_frac * fmin(xi.w, xj.w)) || !(L > 0)) continue;
+            type[r] = 1;
+            iL[r] = (float)(1.0 / L);
+            L0x[r] = L;
+            const double us = pair_uniform(seed, i, (uint32_t)j, 0), ut = pair_uniform(seed, i, (uint32_t)j, 1);
+            strx[r] = make_float2((float)(sig * pow(-log(us), inv_m)), (float)(tau * pow(-log(ut), inv_m)));
+        }
+    }
+}
+__global__ void k_posd_from_planar(const double* __restrict__ R, const double* __restrict__ rad, uint32_t N,
+                                   double4* __restrict__ out, float* __restrict__ Rf) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double x = R[i], y = R[i + N], z = R[i + 2 * (size_t)N];
+        out[i] = make_double4(x, y, z, rad[i]);
+        if (Rf) { Rf[i] = (float)x; Rf[i + N] = (float)y; Rf[i + 2 * (size_t)N] = (float)z; }
+    }
+}
+__global__ void k_posd_to_planar(const double4* __restrict__ in, uint32_t N, double* __restrict__ R) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double4 v = in[i];
+        R[i] = v.x; R[i + N] = v.y; R[i + 2 * (size_t)N] = v.z;
+    }
+}
+__global__ void k_posd_to_planar_f(const double4* __restrict__ in, uint32_t N, float* __restrict__ R) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const double4 v = in[i];
+        R[i] = (float)v.x; R[i + N] = (float)v.y; R[i + 2 * (size_t)N] = (float)v.z;
+    }
+}
+
 __global__ void k_counters(Dev d, Consts c, unsigned long long* out) {
     unsigned long long nb = 0, nc = 0, nl = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
@@ -781,15 +1156,29 @@ __global__ void k_counters(Dev d, Consts c, unsigned long long* out) {
 __global__ void k_set_target(DevScalars* sc, unsigned long long n) { sc->target = sc->steps + n; }
 __global__ void k_force_rebuild(DevScalars* sc) { sc->rebuild = 1u; }
 __global__ void k_planar_to_cur(const float* __restrict__ R, Dev d) {
-    float4* out = d.pos[d.sc->steps & 1ull];
     const uint32_t N = (uint32_t)(d.n_particles);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
-        out[i] = make_float4(R[i], R[i + N], R[i + 2 * (size_t)N], 0.f);
+    if (d.posd[0]) {                      // extended model: keep the radius
+        double4* out = d.posd[d.sc->steps & 1ull];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+            out[i] = make_double4(R[i], R[i + N], R[i + 2 * (size_t)N], out[i].w);
+    } else {
+        float4* out = d.pos[d.sc->steps & 1ull];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+            out[i] = make_float4(R[i], R[i + N], R[i + 2 * (size_t)N], 0.f);
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) d.sc->rebuild = 1u;
 }
 __global__ void k_cur_to_planar(Dev d, float* __restrict__ R) {
-    const float4* in = d.pos[d.sc->steps & 1ull];
     const uint32_t N = (uint32_t)(d.n_particles);
+    if (d.posd[0]) {
+        const double4* in = d.posd[d.sc->steps & 1ull];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+            const double4 v = in[i];
+            R[i] = (float)v.x; R[i + N] = (float)v.y; R[i + 2 * (size_t)N] = (float)v.z;
+        }
+        return;
+    }
+    const float4* in = d.pos[d.sc->steps & 1ull];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const float4 v = in[i];
         R[i] = v.x; R[i + N] = v.y; R[i + 2 * (size_t)N] = v.z;
@@ -829,6 +1218,12 @@ template <class T> rf_status dalloc(rf_engine* e, T** p, size_t n) {
 }
 
 #define TRY(x) do { rf_status s__ = (x); if (s__ != RF_OK) return s__; } while (0)
+
+void* step_kernel(const rf_engine* e) {
+    const bool br = e->task.kind == RF_TEST_BRAZIL;
+    if (e->c.ext) return br ? (void*)k_step_ext<RF_TEST_BRAZIL> : (void*)k_step_ext<RF_TEST_UNIAXIAL>;
+    return br ? (void*)k_step<RF_TEST_BRAZIL> : (void*)k_step<RF_TEST_UNIAXIAL>;
+}
 
 rf_status build_graph(rf_engine* e) {
     cudaGraph_t g;
@@ -883,7 +1278,7 @@ rf_status build_graph(rf_engine* e) {
         prev = n;
     }
     cudaGraphNode_t step;
-    void* fn = (e->task.kind == RF_TEST_BRAZIL) ? (void*)k_step<RF_TEST_BRAZIL> : (void*)k_step<RF_TEST_UNIAXIAL>;
+    void* fn = step_kernel(e);
     kp = kparams(fn, e->nblocks, 128);
     RF_CUDA(cudaGraphAddKernelNode(&step, body, &inode, 1, &kp));
     RF_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
@@ -905,8 +1300,8 @@ rf_status launch_stream_steps(rf_engine* e, uint64_t nsteps) {
         k_rb_scan_apply<<<e->cg_nb, 1024, 0, s>>>(d, c);
         k_rb_scatter<<<gN, 256, 0, s>>>(d, c);
         k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
-        if (e->task.kind == RF_TEST_BRAZIL) k_step<RF_TEST_BRAZIL><<<e->nblocks, 128, 0, s>>>(d, c);
-        else k_step<RF_TEST_UNIAXIAL><<<e->nblocks, 128, 0, s>>>(d, c);
+        void* sargs[] = {&d, &c};
+        if (cudaLaunchKernel(step_kernel(e), dim3(e->nblocks), dim3(128), sargs, 0, s) != cudaSuccess) break;
         k_stream_ungate<<<1, 32, 0, s>>>(d);
     }
     RF_CHECK_LAUNCH("engine stream steps");
@@ -918,10 +1313,29 @@ rf_status launch_stream_steps(rf_engine* e, uint64_t nsteps) {
 // Host-side helpers from the md_* layer.
 extern "C" size_t md_CellDistributionScratchBytes(uint_fast32_t N, uint_fast32_t CN);
 
-extern "C" {
+namespace {
 
-rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) {
-    if (!t || !h_R || !out || t->N == 0 || t->K == 0) { set_error("rf_engine_create: bad arguments"); return RF_ERR_INVALID; }
+rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h_Rd, const double* h_rad,
+                             const rf_ext_params* x, rf_engine** out) {
+    const bool ext = x != nullptr;
+    if (!t || !out || t->N == 0 || t->K == 0 || (ext ? (!h_Rd || !h_rad) : !h_R)) {
+        set_error("rf_engine_create: bad arguments");
+        return RF_ERR_INVALID;
+    }
+    double rmax = 0.0, rmin = 1e300;
+    if (ext) {
+        for (uint64_t i = 0; i < t->N; ++i) { rmax = std::max(rmax, h_rad[i]); rmin = std::min(rmin, h_rad[i]); }
+        if (!(rmin > 0.0) || !(x->kn > 0.0) || !(x->ks >= 0.0) || !(x->bond_lambda > 0.0) || !(x->weibull_m > 0.0) ||
+            !(x->sigma_c > 0.0) || !(x->tau_c > 0.0)) {
+            set_error("rf_engine_create_ext: radii and bond parameters must be positive");
+            return RF_ERR_INVALID;
+        }
+        if (!(2.0 * rmax < std::sqrt(t->Po.aa_farcut))) {
+            set_error("rf_engine_create_ext: a_farcut (%g) must exceed the largest contact distance 2*r_max (%g)",
+                      std::sqrt(t->Po.aa_farcut), 2.0 * rmax);
+            return RF_ERR_INVALID;
+        }
+    }
     if (t->K > 32) { set_error("rf_engine_create: the engine keeps slot masks in 32 bits (K <= 32), got K=%u", t->K); return RF_ERR_INVALID; }
     if (t->N >= 0xFFFFFFFFull) { set_error("rf_engine_create: N too large"); return RF_ERR_INVALID; }
     int ndev = 0;
@@ -946,6 +1360,13 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
     c.cp = ContactParams{(float)P.dt, (float)P.hm_E, (float)P.hm_G, (float)P.p_A, (float)P.p_mu, (float)P.p_mur,
                          (float)P.p_m, (float)P.p_r};
     c.dtm = (float)P.dt_d_m; c.dt = (float)P.dt; c.dtI = (float)P.dt_d_I;
+    if (ext) {
+        c.ext = 1;
+        c.ep = ExtParams{(float)P.dt, (float)P.hm_E, (float)P.hm_G, (float)P.p_A, (float)P.p_mu, (float)P.p_mur};
+        c.kn = (float)x->kn; c.ks = (float)x->ks; c.br_lambda = (float)x->bond_lambda;
+        c.cmass = (float)(P.p_m / (P.p_r * P.p_r * P.p_r));     // mass = density * 4/3 pi r^3
+        c.aa_farcut_d = P.aa_farcut; c.aacut_d = (double)t->aacut;
+    }
     c.aacut = t->aacut; c.aa_farcut = (float)P.aa_farcut;
     c.g.a = t->C.a; c.g.inv_a = t->C._1d_a; c.g.nx = t->C.Nr.x; c.g.ny = t->C.Nr.y; c.g.nz = t->C.Nr.z; c.g.CN = t->C.N;
     c.zcut = (t->kind == RF_TEST_BRAZIL) ? (float)((double)t->S.center.y + (double)t->S.spacesized2.y)
@@ -976,7 +1397,8 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
     d.n_particles = N;
     const size_t NK = (size_t)N * K;
     for (int b = 0; b < 2; ++b) {
-        if ((st = dalloc(e, &d.pos[b], N)) || (st = dalloc(e, &d.vel[b], N)) || (st = dalloc(e, &d.ang[b], N)))
+        if ((ext ? (st = dalloc(e, &d.posd[b], N)) : (st = dalloc(e, &d.pos[b], N))) ||
+            (st = dalloc(e, &d.vel[b], N)) || (st = dalloc(e, &d.ang[b], N)))
             return fail(st);
     }
     if ((st = dalloc(e, &d.ids, NK)) || (st = dalloc(e, &d.il, NK)) || (st = dalloc(e, &d.cO[0], 3 * NK)) || (st = dalloc(e, &d.cO[1], 3 * NK)) ||
@@ -1006,6 +1428,8 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
         uint_fast32_t *dCI = nullptr, *dCIs = nullptr, *dpnC = nullptr, *dIL = nullptr;
         uint8_t* dT = nullptr;
         rf_float3* dS = nullptr;
+        double *dRd = nullptr, *dRad = nullptr, *dL0 = nullptr;
+        float2* dStr = nullptr;
         void* scratch = nullptr;
         const size_t sb = md_CellDistributionScratchBytes(N, t->C.N);
         cudaError_t ce = cudaSuccess;
@@ -1019,7 +1443,17 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
         if (!ce) ce = cudaMalloc(&dIL_f, NK * sizeof(float));
         if (!ce) ce = cudaMalloc(&dS, 7 * NK * sizeof(rf_float3));
         if (!ce) ce = cudaMalloc(&scratch, sb);
-        if (!ce) ce = cudaMemcpyAsync(dR, h_R, 3 * (size_t)N * sizeof(float), cudaMemcpyHostToDevice, s);
+        if (ext) {
+            if (!ce) ce = cudaMalloc(&dRd, 3 * (size_t)N * sizeof(double));
+            if (!ce) ce = cudaMalloc(&dRad, (size_t)N * sizeof(double));
+            if (!ce) ce = cudaMalloc(&dL0, NK * sizeof(double));
+            if (!ce) ce = cudaMalloc(&dStr, NK * sizeof(float2));
+            if (!ce) ce = cudaMemcpyAsync(dRd, h_Rd, 3 * (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+            if (!ce) ce = cudaMemcpyAsync(dRad, h_rad, (size_t)N * sizeof(double), cudaMemcpyHostToDevice, s);
+            if (!ce) { k_posd_from_planar<<<(N + 255) / 256, 256, 0, s>>>(dRd, dRad, N, d.posd[0], dR); ce = cudaGetLastError(); }
+        } else if (!ce) {
+            ce = cudaMemcpyAsync(dR, h_R, 3 * (size_t)N * sizeof(float), cudaMemcpyHostToDevice, s);
+        }
         if (!ce) ce = cudaMemsetAsync(dV, 0, 3 * (size_t)N * sizeof(float), s);
         if (!ce) ce = cudaMemsetAsync(dT, 0, NK, s);
         if (!ce) ce = cudaMemsetAsync(dIL_f, 0, NK * sizeof(float), s);
@@ -1037,8 +1471,14 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
                                                       t->C.Nr, t->C.N, s);
             if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a && !init_dev) init_dev = a;
         }
-        if (!st2) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
-                                                      Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
+        if (!st2 && !ext) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
+                                                              Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
+        if (!st2 && ext) {
+            k_bond_ext<<<(N + 127) / 128, 128, 0, s>>>(d.posd[0], dIL, dT, dIL_f, dL0, dStr, N, K, x->gap_frac,
+                                                       x->weibull_m, x->sigma_c, x->tau_c, x->seed);
+            ce = cudaGetLastError();
+            if (ce) st2 = cuda_status(ce, "k_bond_ext");
+        }
         if (!st2) st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
                                           (float)P.aa_farcut, s);
         if (!st2) {
@@ -1054,16 +1494,17 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
             const size_t QN = (size_t)qb * N;
             if (!st2 && ((st2 = dalloc(e, &d.bj, QN)) || (st2 = dalloc(e, &d.bk, QN)) || (st2 = dalloc(e, &d.bil, QN)) ||
                          (st2 = dalloc(e, &d.bst, 3 * QN)))) {}
+            if (!st2 && ext && ((st2 = dalloc(e, &d.bL0, QN)) || (st2 = dalloc(e, &d.bstr, QN)))) {}
         }
         if (!st2) {
-            k_planar_to_f4<<<(N + 255) / 256, 256, 0, s>>>(dR, N, d.pos[0]);
-            k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dIL_f, Rij, Oijt, Mijn, Mijt, d, c);
+            if (!ext) k_planar_to_f4<<<(N + 255) / 256, 256, 0, s>>>(dR, N, d.pos[0]);
+            k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dIL_f, Rij, Oijt, Mijn, Mijt, dL0, dStr, d, c);
             ce = cudaGetLastError();
             if (ce) st2 = cuda_status(ce, "engine import");
         }
         if (!st2) { ce = cudaStreamSynchronize(s); if (ce) st2 = cuda_status(ce, "engine init"); }
         cudaFree(dR); cudaFree(dV); cudaFree(dCI); cudaFree(dCIs); cudaFree(dpnC); cudaFree(dIL); cudaFree(dT);
-        cudaFree(dIL_f); cudaFree(dS); cudaFree(scratch);
+        cudaFree(dIL_f); cudaFree(dS); cudaFree(scratch); cudaFree(dRd); cudaFree(dRad); cudaFree(dL0); cudaFree(dStr);
         if (st2) return fail(st2);
         st = init_dev;
     }
@@ -1101,6 +1542,39 @@ rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) 
         else { cudaGetLastError(); e->c.use_graph = 0; }
     }
     *out = e;
+    return RF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rf_status rf_engine_create(const rf_task* t, const float* h_R, rf_engine** out) {
+    return engine_create_impl(t, h_R, nullptr, nullptr, nullptr, out);
+}
+
+rf_status rf_engine_create_ext(const rf_task* t, const rf_ext_params* x, const double* h_R, const double* h_radius,
+                               rf_engine** out) {
+    if (!x) { set_error("rf_engine_create_ext: null parameters"); return RF_ERR_INVALID; }
+    return engine_create_impl(t, nullptr, h_R, h_radius, x, out);
+}
+
+rf_status rf_engine_positions_f64(rf_engine* e, double* R) {
+    if (!e || !R) { set_error("rf_engine_positions_f64: bad arguments"); return RF_ERR_INVALID; }
+    if (!e->c.ext) { set_error("rf_engine_positions_f64: engine keeps float positions"); return RF_ERR_STATE; }
+    const uint32_t N = e->c.N;
+    cudaStream_t s = e->stream;
+    DevScalars h;
+    RF_CUDA(cudaStreamSynchronize(s));
+    RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
+    double* tmp = nullptr;
+    RF_CUDA(cudaMalloc(&tmp, 3 * (size_t)N * sizeof(double)));
+    k_posd_to_planar<<<(N + 255) / 256, 256, 0, s>>>(e->d.posd[h.steps & 1ull], N, tmp);
+    cudaError_t ce = cudaGetLastError();
+    if (!ce) ce = cudaMemcpyAsync(R, tmp, 3 * (size_t)N * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (!ce) ce = cudaStreamSynchronize(s);
+    cudaFree(tmp);
+    if (ce) return cuda_status(ce, "rf_engine_positions_f64");
     return RF_OK;
 }
 
@@ -1188,13 +1662,15 @@ rf_status rf_engine_export(rf_engine* e, float* R, float* V, float* W, uint_fast
     RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
     const int cur = (int)(h.steps & 1ull);
     if (!e->staging) RF_CUDA(cudaMalloc(&e->staging, 3 * (size_t)N * sizeof(float)));
-    k_delete_pending<<<(N + 127) / 128, 128, 0, s>>>(e->d, e->c);
+    if (e->c.ext) k_delete_pending_ext<<<(N + 127) / 128, 128, 0, s>>>(e->d, e->c);
+    else k_delete_pending<<<(N + 127) / 128, 128, 0, s>>>(e->d, e->c);
     RF_CHECK_LAUNCH("k_delete_pending");
     const float4* vecs[3] = {e->d.pos[cur], e->d.vel[cur], e->d.ang[cur]};
     float* outs[3] = {R, V, W};
     for (int q = 0; q < 3; ++q) {
         if (!outs[q]) continue;
-        k_f4_to_planar<<<(N + 255) / 256, 256, 0, s>>>(vecs[q], N, e->staging);
+        if (q == 0 && e->c.ext) k_posd_to_planar_f<<<(N + 255) / 256, 256, 0, s>>>(e->d.posd[cur], N, e->staging);
+        else k_f4_to_planar<<<(N + 255) / 256, 256, 0, s>>>(vecs[q], N, e->staging);
         RF_CHECK_LAUNCH("k_f4_to_planar");
         RF_CUDA(cudaMemcpyAsync(outs[q], e->staging, 3 * (size_t)N * sizeof(float), cudaMemcpyDeviceToHost, s));
         RF_CUDA(cudaStreamSynchronize(s));
@@ -1228,6 +1704,10 @@ rf_status rf_engine_import(rf_engine* e, const float* R, const float* V, const f
     if (!e || !R || !V || !W || !IL || !ILtype || !_1d_iL || !Rij || !Oijt || !Mijn || !Mijt) {
         set_error("rf_engine_import: bad arguments");
         return RF_ERR_INVALID;
+    }
+    if (e->c.ext) {
+        set_error("rf_engine_import: the extended model resumes from its own state only (no reference layout)");
+        return RF_ERR_STATE;
     }
     const uint32_t N = e->c.N, K = e->c.K;
     const size_t NK = (size_t)N * K;
@@ -1267,7 +1747,8 @@ rf_status rf_engine_import(rf_engine* e, const float* R, const float* V, const f
         return RF_ERR_CAPACITY;
     }
     if (!ce) {
-        k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dL, dS, dS + NK, dS + 2 * NK, dS + 3 * NK, e->d, e->c);
+        k_rows_import<<<(N + 127) / 128, 128, 0, s>>>(dIL, dT, dL, dS, dS + NK, dS + 2 * NK, dS + 3 * NK, nullptr,
+                                                      nullptr, e->d, e->c);
         ce = cudaGetLastError();
     }
     if (!ce) {

@@ -325,3 +325,170 @@ __device__ __forceinline__ bool outside_box(float Rx, float Ry, float Rz, const 
 }
 
 }  // namespace rf
+
+// ===========================================================================
+// Extended model: polydisperse particles, per-bond stiffness and strength, FP64
+// positions. Each formula is the reference's with its mono-sized constants replaced:
+//   E/L0 -> kn, G/L0 -> ks (normal / shear stiffness per area, kn = E/L0 as the
+//   reference's moduli imply), b_r -> the bond's radius (lambda * min(r_i, r_j)),
+//   2 rP -> r_i + r_j, rP*(rP - r/2) -> R* delta/2... (equivalent radius),
+//   0.5 mP -> m* (equivalent mass), rP lever arms -> r_i.
+// Positions are double; r = Rj - Ri and the bond stretch |r| - L0 are formed in
+// double and rounded once to float, so small increments and small strains survive.
+// ===========================================================================
+namespace rf {
+
+struct BondExt {            // per-bond constants of the extended model
+    float kn, ks, br, sc, tc;   // stiffness (normal, shear), bond radius, tensile and shear strength
+    double L0;                  // initial length
+};
+struct ExtParams {
+    float dt, hm_E, hm_G, p_A, mu, mur;
+};
+
+// One bond slot of the extended model (same structure and order as bond_slot).
+// rlen = |r| in double; r is the float rounding of the double separation.
+__device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt& b, const f3 r, const double rlen,
+                                              const f3 vi, const f3 vj, const f3 wi, const f3 wj, f3& Rij, f3& Oijt,
+                                              f3& Mijn, f3& Mijt, f3& fs, f3& ms) {
+    const float rijm = (float)rlen;
+    const float inv_rm = __frcp_rn(rijm);
+    const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
+    const float il = (float)(1.0 / b.L0);
+    const float stretch = (float)(rlen - b.L0);
+    const float A = b.br * b.br * RF_PI_F;
+    const float J = RF_PI_F * b.br * b.br * b.br * b.br;
+    float cef = b.kn * stretch;
+    float Sc = cef;
+    cef *= A;
+    fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
+    const float tx = Rij.y * nz - Rij.z * ny;
+    const float ty = Rij.z * nx - Rij.x * nz;
+    const float tz = Rij.x * ny - Rij.y * nx;
+    const float wsx = wj.x + wi.x, wsy = wj.y + wi.y, wsz = wj.z + wi.z;
+    const float cphi = (wsx * nx + wsy * ny + wsz * nz) * p.dt * 0.5f;
+    const float phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
+    Rij = mk3(nx, ny, nz);
+    const float M1x = 1.0f + tz * phz + ty * phy;
+    const float M1y = phz - tz - ty * phx;
+    const float M1z = -phy - tz * phx + ty;
+    const float M2x = tz - phz - tx * phy;
+    const float M2y = tz * phz + 1.0f + tx * phx;
+    const float M2z = -tz * phy + phx - tx;
+    const float M3x = -ty - tx * phz + phy;
+    const float M3y = -ty * phz + tx - phx;
+    const float M3z = ty * phy + tx * phx + 1.0f;
+    const float dwx = wj.x - wi.x, dwy = wj.y - wi.y, dwz = wj.z - wi.z;
+    {
+        float c1 = nx * dwx + ny * dwy + nz * dwz;
+        c1 *= p.dt * 0.5f * b.ks;
+        const f3 o = Mijn;
+        const float mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
+        const float my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
+        const float mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
+        Mijn = mk3(mx, my, mz);
+        ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+    }
+    {
+        const float c1 = nx * dwx + ny * dwy + nz * dwz;
+        float c2 = p.dt * 0.25f * b.kn;
+        const f3 o = Mijt;
+        const float mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
+        const float my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
+        const float mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
+        Mijt = mk3(mx, my, mz);
+        c2 *= J;
+        ms.x += mx * c2; ms.y += my * c2; ms.z += mz * c2;
+    }
+    float Mc;
+    {
+        const float hx = 0.5f * wsx, hy = 0.5f * wsy, hz = 0.5f * wsz;
+        const float vx = vj.x - vi.x - hy * r.z + hz * r.y;
+        const float vy = vj.y - vi.y - hz * r.x + hx * r.z;
+        const float vz = vj.z - vi.z - hx * r.y + hy * r.x;
+        float c = nx * vx + ny * vy + nz * vz;
+        const f3 o = Oijt;
+        const float ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c) * p.dt;
+        const float oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (vy - ny * c) * p.dt;
+        const float oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (vz - nz * c) * p.dt;
+        c = b.ks;
+        Mc = c;
+        c *= A;
+        fs.x += ox * c; fs.y += oy * c; fs.z += oz * c;
+        Oijt = mk3(ox, oy, oz);
+        ms.x += 0.5f * (r.y * oz - r.z * oy) * c;
+        ms.y += 0.5f * (r.z * ox - r.x * oz) * c;
+        ms.z += 0.5f * (r.x * oy - r.y * ox) * c;
+    }
+    (void)il;
+    Mc *= norm3(Oijt.x, Oijt.y, Oijt.z);
+    Sc += norm3(Mijt.x, Mijt.y, Mijt.z) * 4.0f * b.br;
+    Mc += norm3(Mijn.x, Mijn.y, Mijn.z) * 2.0f * b.br;
+    if ((Sc > b.sc) || (Mc > b.tc)) {
+        Oijt = mk3(0.f, 0.f, 0.f);
+        Mijn = mk3(0.f, 0.f, 0.f);
+        Mijt = mk3(0.f, 0.f, 0.f);
+        return true;
+    }
+    return false;
+}
+
+// Overlapping pair of the extended model (rlen < ri + rj). mi, mj are the masses.
+__device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r, const float rijm, const float ri,
+                                                 const float rj, const float mi, const float mj, const f3 vi,
+                                                 const f3 vj, const f3 wi, const f3 wj, f3& Oijt, f3& fs, f3& ms) {
+    const float inv_rm = __frcp_rn(rijm);
+    const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
+    const float Rs = ri * rj / (ri + rj);               // equivalent radius (rP/2 for equal sizes)
+    const float ms_ = mi * mj / (mi + mj);             // equivalent mass (mP/2 for equal masses)
+    const float delta = ri + rj - rijm;
+    float c1 = __fsqrt_rn(Rs * fabsf(delta));
+    const float Kn = 2.0f * p.hm_E * c1;
+    const float Kt = 8.0f * p.hm_G * c1;
+    // relative velocity of the contact point: vj - vi + n x (ri wi + rj wj)
+    const float ax = ri * wi.x + rj * wj.x, ay = ri * wi.y + rj * wj.y, az = ri * wi.z + rj * wj.z;
+    const float vx = vj.x - vi.x + (ny * az - nz * ay);
+    const float vy = vj.y - vi.y + (nz * ax - nx * az);
+    const float vz = vj.z - vi.z + (nx * ay - ny * ax);
+    const float vn = nx * vx + ny * vy + nz * vz;
+    const float fn = -delta * Kn * RF_2D3_F;
+    c1 = -1.8257f * p.p_A * vn * __fsqrt_rn(Kn * ms_);
+    fs.x += nx * (fn + c1); fs.y += ny * (fn + c1); fs.z += nz * (fn + c1);
+    const float vtx = vx - nx * vn, vty = vy - ny * vn, vtz = vz - nz * vn;
+    const f3 o = Oijt;
+    float c = nx * o.x + ny * o.y + nz * o.z;
+    float ox = o.x - nx * c, oy = o.y - ny * c, oz = o.z - nz * c;
+    c = ox * ox + oy * oy + oz * oz;
+    if ((double)c > 1e-18) {
+        c = __frcp_rn(c);
+        c *= o.x * o.x + o.y * o.y + o.z * o.z;
+        c = __fsqrt_rn(c);
+        ox *= c; oy *= c; oz *= c;
+    }
+    ox += vtx * p.dt; oy += vty * p.dt; oz += vtz * p.dt;
+    float ftx = ox * Kt, fty = oy * Kt, ftz = oz * Kt;
+    const float ftm = ftx * ftx + fty * fty + ftz * ftz;
+    if (ftm > p.mu * p.mu * fn * fn) {
+        c = p.mu * fabsf(fn) * __frsqrt_rn(ftm);
+        ftx *= c; fty *= c; ftz *= c;
+        c = __frcp_rn(Kt);
+        ox = ftx * c; oy = fty * c; oz = ftz * c;
+    } else {
+        c = -1.8257f * p.p_A * __fsqrt_rn(Kt * ms_);
+        ftx += vtx * c; fty += vty * c; ftz += vtz * c;
+    }
+    Oijt = mk3(ox, oy, oz);
+    fs.x += ftx; fs.y += fty; fs.z += ftz;
+    ms.x += (ny * ftz - nz * fty) * ri;
+    ms.y += (nz * ftx - nx * ftz) * ri;
+    ms.z += (nx * fty - ny * ftx) * ri;
+    const float wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
+    if ((double)wim > 1e-18) {
+        const float cr = -p.mur * fabsf(fn) * __frsqrt_rn(wim);
+        ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
+    } else {
+        ms = mk3(0.f, 0.f, 0.f);
+    }
+}
+
+}  // namespace rf

@@ -91,6 +91,12 @@ class RunResult(C.Structure):
                 ("broken_bonds", C.c_uint64), ("bonds_initial", C.c_uint64), ("error", C.c_int)]
 
 
+class ExtParams(C.Structure):
+    """rf_ext_params: bond constants and strength distribution of the extended model."""
+    _fields_ = [("kn", C.c_double), ("ks", C.c_double), ("bond_lambda", C.c_double), ("gap_frac", C.c_double),
+                ("weibull_m", C.c_double), ("sigma_c", C.c_double), ("tau_c", C.c_double), ("seed", C.c_uint64)]
+
+
 # --- prototypes ---------------------------------------------------------------
 P = C.c_void_p
 ID = C.c_uint64 if lib.rf_id_bytes() == 8 else C.c_uint32     # uint_fast32_t
@@ -134,6 +140,9 @@ _proto = {
     "rf_engine_launches_per_step": (i32, []),
     "rf_engine_stream": (P, [P]),
     "rf_engine_uses_graph": (i32, [P]),
+    "rf_engine_create_ext": (i32, [C.POINTER(Task), C.POINTER(ExtParams), P, P, C.POINTER(P)]),
+    "rf_engine_positions_f64": (i32, [P, P]),
+    "rf_pack_cylinder": (i32, [u64, u64, f64, f64, f64, f64, f64, P, P, P, P, P, P]),
     "rf_specimen_lattice_cylinder": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
     "rf_specimen_lattice_disc": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
 }
@@ -231,18 +240,96 @@ def make_test(kind, diameter, height, seed=0xB2000000, potential=None, K=32, gap
     return t, R
 
 
+# --- extended model: packed polydisperse specimens ------------------------------
+def pack_cylinder(N, r0, rmin=0.8, rmax=1.2, aspect=2.0, phi=0.6, seed=0xB2000000, center=(0.0, 0.0, 0.0)):
+    """Seeded FIRE packing on the GPU (rf_pack_cylinder). Returns (R float64[3N] planar,
+    radius float64[N], diameter, height, max relative overlap); sizes in mm."""
+    R = np.zeros(3 * N, np.float64)
+    rad = np.zeros(N, np.float64)
+    D, H, mo = C.c_double(0), C.c_double(0), C.c_double(0)
+    c = (C.c_double * 3)(*center)
+    check(lib.rf_pack_cylinder(seed, N, r0, rmin, rmax, aspect, phi, c, R.ctypes.data, rad.ctypes.data,
+                               C.byref(D), C.byref(H), C.byref(mo)), "rf_pack_cylinder")
+    return R, rad, D.value, H.value, mo.value
+
+
+def ext_params_si(kn=1e11, ks=None, bond_lambda=0.330015, gap_frac=0.05, weibull_m=5.0, sigma_c=10e6, tau_c=30e6,
+                  seed=0xB2000000):
+    """rf_ext_params from SI values: kn, ks in N/m^3 (ks defaults to kn/2.5), strengths in Pa.
+    bond_lambda defaults to the reference's b_r / p_r."""
+    x = ExtParams()
+    x.kn = kn / (STRESS / LENGTH)
+    x.ks = (ks if ks is not None else kn / 2.5) / (STRESS / LENGTH)
+    x.bond_lambda = bond_lambda
+    x.gap_frac = gap_frac
+    x.weibull_m = weibull_m
+    x.sigma_c = sigma_c / STRESS
+    x.tau_c = tau_c / STRESS
+    x.seed = seed
+    return x
+
+
+def make_test_ext(kind, R0, radius, r0, K=32, potential=None, margin=None, v_load=None, min_stress=None,
+                  max_strain=0.1, dt=None):
+    """A prepared task for a packed specimen centred at the origin (kind as make_test:
+    uniaxial along z, or Brazilian disc of axis z loaded along y). Returns (Task, R)
+    with R shifted to the task's centre. dt (microseconds) overrides the derived step."""
+    po = potential or granite_potential()
+    po.p_r = r0
+    po.b_r = 0.330015 * r0
+    po.b_d = 2.0 * r0 + 0.0593169 * r0 * 2.0
+    po.a_farcut = 2.9 * r0
+    N = radius.size
+    P3 = R0.reshape(3, N)
+    L = [2.0 * float(np.max(np.abs(P3[a]))) for a in range(3)]
+    if margin is None:
+        margin = 4.0 * r0 + 0.25 * max(L)
+    space = [x + 2 * r0 + 2 * margin for x in L]
+    t = Task()
+    t.kind = kind
+    t.K = K
+    t.Po = po
+    if v_load is None:
+        v_load = (-10.0 if kind == RF_TEST_UNIAXIAL else -100.0) * 0.02 / 1e3
+    if min_stress is None:
+        min_stress = (15e6 if kind == RF_TEST_UNIAXIAL else 2.1e6) / STRESS
+    ss = (C.c_double * 3)(*[x * LENGTH for x in space])
+    ls = (C.c_double * 3)(*[(x + 2 * r0) * LENGTH for x in L])
+    t.N = N
+    check(lib.rf_task_prepare(C.byref(t), ss, ls, 2.0 * po.a_farcut, v_load, min_stress, max_strain), "rf_task_prepare")
+    if dt is not None:
+        t.Po.dt = dt
+    ctr = np.array([t.S.center.x, t.S.center.y, t.S.center.z], np.float64)
+    R = (P3 + ctr[:, None]).reshape(-1).copy()
+    t.bloks = N // 1024 + 1
+    return t, R
+
+
 class Engine:
     """The fused engine on the current CUDA device."""
 
-    def __init__(self, task, R):
+    def __init__(self, task, R, ext=None, radius=None):
         self.task = task
         self.N = int(task.N)
         self.K = int(task.K)
-        R = np.ascontiguousarray(R, np.float32)
-        assert R.size == 3 * self.N
+        self.ext = ext is not None
         h = P()
-        check(lib.rf_engine_create(C.byref(task), R.ctypes.data, C.byref(h)), "rf_engine_create")
+        if self.ext:
+            R = np.ascontiguousarray(R, np.float64)
+            rad = np.ascontiguousarray(radius, np.float64)
+            assert R.size == 3 * self.N and rad.size == self.N
+            check(lib.rf_engine_create_ext(C.byref(task), C.byref(ext), R.ctypes.data, rad.ctypes.data, C.byref(h)),
+                  "rf_engine_create_ext")
+        else:
+            R = np.ascontiguousarray(R, np.float32)
+            assert R.size == 3 * self.N
+            check(lib.rf_engine_create(C.byref(task), R.ctypes.data, C.byref(h)), "rf_engine_create")
         self.h = h
+
+    def positions_f64(self):
+        R = np.zeros(3 * self.N, np.float64)
+        check(lib.rf_engine_positions_f64(self.h, R.ctypes.data), "rf_engine_positions_f64")
+        return R
 
     def close(self):
         if self.h:

@@ -1,0 +1,63 @@
+"""The extended model's oracle on the CPU: the float-force instance (the engine's
+arithmetic) against the FP64 instance, bond formation and the strength draws."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import extspec
+import mdcall as mc
+import oracle
+import rfdem
+
+
+@pytest.mark.parametrize("kind,d,h", [(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0), (rfdem.RF_TEST_BRAZIL, 10.0, 4.0)],
+                         ids=["uniaxial", "brazil"])
+def test_ext_float_vs_fp64(kind, d, h):
+    t, R, rad, x = extspec.ext_case(kind, d, h, min_stress=1e3)    # no fracture stop in this window
+    N, K = int(t.N), int(t.K)
+    steps = 150
+    f = oracle.run_ext(mc.clone(t), x, R, rad, steps)
+    g = oracle.run_ext(mc.clone(t), x, R, rad, steps, fp64=True)
+    assert f["steps"] == steps and g["steps"] == steps
+    assert f["status"] == 0 and g["status"] == 0
+    bonds = int(np.count_nonzero(f["ILtype"]))
+    assert bonds > 3 * N, "lattice neighbours within 0.05 r_min should bond (%d bonds, %d particles)" % (bonds, N)
+    # FP32 forces with FP64 positions track the FP64 oracle closely over a short run
+    ext = float(np.max(R) - np.min(R))
+    err = np.max(np.abs(f["R"] - g["R"]))
+    assert err < 1e-6 * ext, err
+    # both instances keep the same lists and bond states here (no threshold bonds)
+    assert np.array_equal(f["IL"], g["IL"])
+    assert np.array_equal(f["ILtype"], g["ILtype"])
+
+
+def test_ext_bond_rule_and_rest_length():
+    """Step 0 bonds exactly the listed pairs whose gap is below gap_frac * min radius."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 5.0, 6.0)
+    N, K = int(t.N), int(t.K)
+    f = oracle.run_ext(mc.clone(t), x, R, rad, 0)
+    IL = f["IL"].reshape(N, K)
+    ty = f["ILtype"].reshape(N, K)
+    P = R.reshape(3, N).T
+    E = np.iinfo(np.uint64).max
+    for i in range(N):
+        for k in range(K):
+            j = IL[i, k]
+            if j == E:
+                assert ty[i, k] == 0
+                continue
+            L = np.sqrt(np.sum((P[j] - P[i]) ** 2))
+            want = (L - rad[i] - rad[j]) < x.gap_frac * min(rad[i], rad[j])
+            assert bool(ty[i, k]) == want, (i, k, j)
+
+
+def test_ext_directed_bonds_pair_up():
+    """Both directions of a pair are bonded together (the rule is symmetric)."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_BRAZIL, 8.0, 3.0)
+    N, K = int(t.N), int(t.K)
+    f = oracle.run_ext(mc.clone(t), x, R, rad, 0)
+    IL = f["IL"].reshape(N, K)
+    ty = f["ILtype"].reshape(N, K)
+    pairs = {(i, int(IL[i, k])) for i in range(N) for k in range(K) if ty[i, k]}
+    assert pairs and all((j, i) in pairs for (i, j) in pairs)

@@ -1,0 +1,91 @@
+"""Extended model on the GPU: the packer, and the engine's extended-model step
+against the oracle's float-force restatement (bit for bit) and the FP64 oracle."""
+import numpy as np
+import pytest
+
+import extspec
+import mdcall as mc
+import oracle
+import rfdem
+
+pytestmark = pytest.mark.gpu
+
+
+def run_engine_ext(t, x, R, rad, steps, no_graph=False, monkeypatch=None):
+    if no_graph:
+        monkeypatch.setenv("RF_ENGINE_NO_GRAPH", "1")
+    e = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    assert e.uses_graph() == (not no_graph)
+    e.step(steps)
+    _, res = e.sync()
+    st = e.export()
+    st["R64"] = e.positions_f64()
+    e.close()
+    return res, st
+
+
+@pytest.mark.parametrize("kind,d,h,steps", [(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, 300),
+                                            (rfdem.RF_TEST_BRAZIL, 10.0, 4.0, 300)], ids=["uniaxial", "brazil"])
+def test_ext_engine_bitexact_vs_oracle(cuda, kind, d, h, steps):
+    t, R, rad, x = extspec.ext_case(kind, d, h, min_stress=1e3)
+    o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
+    res, st = run_engine_ext(t, x, R, rad, steps)
+    assert res.steps == o["steps"] == steps
+    assert res.error == 0 and o["status"] == 0
+    assert np.array_equal(st["R64"], o["R"]), np.max(np.abs(st["R64"] - o["R"]))
+    assert np.array_equal(st["V"], o["V"])
+    assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
+    assert np.array_equal(st["ILtype"], o["ILtype"])
+    assert res.broken_bonds == o["broken"]
+
+
+def test_ext_engine_stream_equals_graph(cuda, monkeypatch):
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 8.0, min_stress=1e3)
+    _, a = run_engine_ext(t, x, R, rad, 120)
+    _, b = run_engine_ext(t, x, R, rad, 120, no_graph=True, monkeypatch=monkeypatch)
+    assert np.array_equal(a["R64"], b["R64"])
+    assert np.array_equal(a["IL"], b["IL"]) and np.array_equal(a["ILtype"], b["ILtype"])
+
+
+def test_pack_cylinder_overlap_container_determinism(cuda):
+    N, r0 = 3000, 0.25
+    R, rad, D, H, mo = rfdem.pack_cylinder(N, r0, aspect=2.0, phi=0.55, seed=0xB2000000 + 11)
+    assert mo < 2e-4
+    assert np.all(rad >= 0.8 * r0 - 1e-12) and np.all(rad <= 1.2 * r0 + 1e-12)
+    P = R.reshape(3, N)
+    rho = np.sqrt(P[0] ** 2 + P[1] ** 2)
+    # the wall is a soft contact too: allow the same relative overlap
+    assert np.all(rho + rad <= 0.5 * D + 2e-4 * rad + 1e-9)
+    assert np.all(np.abs(P[2]) + rad <= 0.5 * H + 2e-4 * rad + 1e-9)
+    assert abs(H / D - 2.0) < 1e-12
+    # pairwise overlap check (brute force over a cell-free O(N^2) in blocks)
+    X = P.T
+    worst = 0.0
+    for s in range(0, N, 500):
+        dd = np.sqrt(((X[s:s + 500, None, :] - X[None, :, :]) ** 2).sum(-1))
+        rr = rad[s:s + 500, None] + rad[None, :]
+        np.fill_diagonal(dd[:, s:s + 500], np.inf)
+        ov = (rr - dd) / np.minimum(rad[s:s + 500, None], rad[None, :])
+        worst = max(worst, float(ov.max()))
+    assert worst < 2e-4 + 1e-9
+    R2, rad2, _, _, _ = rfdem.pack_cylinder(N, r0, aspect=2.0, phi=0.55, seed=0xB2000000 + 11)
+    assert np.array_equal(R, R2) and np.array_equal(rad, rad2)
+
+
+def test_ext_packed_specimen_vs_oracle_and_fp64(cuda):
+    """A packed polydisperse cylinder: engine == float oracle bit for bit; the FP64
+    oracle stays within a small position error over the window."""
+    N, r0 = 2500, 0.25
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, r0, aspect=2.0, phi=0.55, seed=0xB2000000 + 2001)
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, r0, min_stress=1e3)
+    x = rfdem.ext_params_si()
+    steps = 400
+    o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
+    res, st = run_engine_ext(t, x, R, rad, steps)
+    assert res.steps == steps and res.error == 0
+    assert np.array_equal(st["R64"], o["R"])
+    assert np.array_equal(st["ILtype"], o["ILtype"])
+    g = oracle.run_ext(mc.clone(t), x, R, rad, steps, fp64=True)
+    err = float(np.max(np.abs(o["R"] - g["R"])))
+    print("packed N=%d bonds=%d max |R_f32force - R_fp64| = %.3e mm" % (N, int(o["ILtype"].sum()), err))
+    assert err < 1e-6 * (H + D)

@@ -272,6 +272,22 @@ rf_status md_CalculateDecrementsHalfStepFIRE(const float* V, float* R, uint_fast
 rf_status md_FdotVEntire(const float* V, const float* F, double* FdotV, uint64_t nblocks, uint_fast32_t N,
                          rf_stream stream);
 
+/* firerelax_data (md_data_types.h:296-301) without its buffers; FdotV is kept in double. */
+typedef struct rf_fire {
+    uint64_t bloks4, NPpositiveMax, NPnegativeMax, NPpositive, NPnegative, Ndelay, MaxStepsRelaxation;
+    float dtmax, dtmin, dt0, dt, alpha0, alpha, dtgrow, dtshrink, alphashrink;
+    double FdotV;
+} rf_fire;
+/* SetFIREData (md_firerelaxation.cu:72-84), plus what CalculateGPUStepsContractRelaxFIRE
+   sets before its loop (NPpositive = NPnegative = 0, dt = dt0, :89-91). The reference
+   never initialises alpha; here it starts at alpha0. */
+rf_status md_SetFIREData(rf_fire* f, uint_fast32_t N, const rf_potential* Po);
+/* The host FIRE decision of one relaxation step (md_firerelaxation.cu:266-301) given the
+   summed power FdotV: updates NPpositive / NPnegative, dt and alpha. *half_step = 1 when
+   the caller must run md_CalculateDecrementsHalfStepFIRE(0.5 * dt) and zero V before the
+   increments; *stop = 1 when NPnegative exceeded NPnegativeMax (the loop breaks). */
+rf_status md_FireDecide(rf_fire* f, double FdotV, uint64_t step, int* half_step, int* stop);
+
 /* ------------------------------------------------------------------------ */
 /* Whole-test drivers (h_CalculationBrazilTest / h_CalculationUniaxialCompression). */
 /* ------------------------------------------------------------------------ */
@@ -340,6 +356,45 @@ rf_status rf_engine_create_ext(const rf_task* t, const rf_ext_params* x, const d
                                const double* h_radius, rf_engine** out);
 /* FP64 positions of an extended-model engine, double[3N] planar (host). */
 rf_status rf_engine_positions_f64(rf_engine* e, double* R);
+
+/*
+ * Quasi-static loading (extended model; no reference counterpart: the reference's FIRE
+ * relaxes a sample-preparation potential, md_firerelaxation.cu:85-368). Each load
+ * increment advances the loading platen by strain_inc * initial size (0: relax in place)
+ * and relaxes the specimen with FIRE (Bitzek et al. 2006) on the conservative part of the
+ * bond and contact model, on the device, until the RMS net particle force is at most tol
+ * times the mean normal pair force, or max_iter iterations.
+ */
+typedef struct rf_relax_params {
+    double strain_inc;              /* platen advance per increment / initial specimen size */
+    double tol;                     /* residual target (1e-6) */
+    double dt0, dt_max, dt_min;     /* FIRE steps of the stiffness-scaled dynamics (each particle's
+                                       mass is its summed pair stiffness, so the steps are
+                                       dimensionless; stable below about 1.4) */
+    double alpha0, f_inc, f_dec, f_alpha;
+    uint32_t n_delay;
+    uint64_t max_iter;              /* FIRE iterations per increment */
+} rf_relax_params;
+typedef struct rf_relax_result {
+    uint64_t iterations;            /* FIRE iterations of this increment */
+    int32_t converged;
+    double residual;                /* RMS net force / mean normal pair force at exit */
+    double mean_force;              /* mean normal pair force (model force units) */
+    double stress, strain;          /* platen stress and specimen strain after the increment */
+    uint64_t broken_bonds;          /* directed bond slots broken so far */
+    rf_status error;
+} rf_relax_result;
+/* Defaults: strain_inc 2.5e-5, tol 1e-6, dt0 0.1, dt_max 1.0, dt_min 1e-3, alpha0 0.1,
+   f_inc 1.1, f_dec 0.5, f_alpha 0.99, n_delay 5, max_iter 200000. */
+rf_status rf_relax_default_params(rf_relax_params* p, const rf_task* t);
+/* One load increment. warm (device pointer, may be NULL): float[N][6] per-particle
+   predicted displacement (x, y, z) and rotation of the increment, applied before FIRE
+   (the rotation as the first iteration's angular velocity, rotation / dt0). */
+rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const float* warm,
+                                   rf_relax_result* r);
+/* The last increment's start positions, relaxed displacement and accumulated rotation,
+   each double[N][3] (host; any may be NULL): training pairs for the warm start. */
+rf_status rf_engine_increment_fields(rf_engine* e, double* x0, double* dx, double* rot);
 rf_status rf_engine_destroy(rf_engine* e);
 
 /* Advance nsteps explicit steps (stops early, on device, at fracture / max strain). */

@@ -57,6 +57,11 @@ def _declare(L):
         "rfo_sum_forces": (None, [T, f64, f64, f64]),
         "rfo_run_f": (u64, [T, P, u64, P, P, P, P, P, P, P, P, P, P, P, u64, P, P]),
         "rfo_run_d": (u64, [T, P, u64, P, P, u64, P, P, P]),
+        "rfo_fire_increments_f": (None, [P, P, P, u64, f32, f32, f32]),
+        "rfo_fire_half_f": (None, [P, P, u64, f32]),
+        "rfo_fdotv_f": (f64, [P, P, u64]),
+        "rfo_qs_ext_f": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
+        "rfo_qs_ext_d": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
         "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
         "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
     }
@@ -123,6 +128,23 @@ def run_ext(task, x, R0, radius, max_steps, fp64=False):
                C.byref(status), C.byref(broken))
     return dict(steps=int(steps), R=R, V=V, IL=IL, ILtype=ty, curve=curve[:3 * min(ns.value, cap)].reshape(-1, 3),
                 status=status.value, broken=int(broken.value))
+
+
+def qs_ext(task, x, R0, radius, params, n_inc, fp64=False, trace_cap=0):
+    """Quasi-static FIRE load increments of the extended model; returns dict(R, iters,
+    converged, residual, stress, trace, status)."""
+    L = load()
+    R = np.array(R0, np.float64, copy=True)
+    rad = np.ascontiguousarray(radius, np.float64)
+    it = np.zeros(n_inc, np.uint64)
+    cv = np.zeros(n_inc, np.int32)
+    rs = np.zeros(n_inc, np.float64)
+    st = np.zeros(n_inc, np.float64)
+    tr = np.zeros(max(trace_cap, 1), np.float64)
+    fn = L.rfo_qs_ext_d if fp64 else L.rfo_qs_ext_f
+    status = fn(C.byref(task), C.byref(x), p(R), p(rad), C.byref(params), n_inc, p(it), p(cv), p(rs), p(st),
+                p(tr) if trace_cap else None, trace_cap)
+    return dict(R=R, iters=it, converged=cv, residual=rs, stress=st, trace=tr[:trace_cap], status=status)
 
 
 def ref_gpu():

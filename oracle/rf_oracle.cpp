@@ -985,7 +985,7 @@ struct RunExt {
 
     // One bond slot (engine bond_slot_ext).
     bool bond(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& vi, const V3<TF>& vj, const V3<TF>& wi,
-              const V3<TF>& wj, TF br, V3<TF>& fs, V3<TF>& ms) {
+              const V3<TF>& wj, TF br, V3<TF>& fs, V3<TF>& ms, double& fnsum, double* kt, double* kr) {
         const TF PI = pi_t<TF>();
         const TF rijm = (TF)rlen;
         const TF inv_rm = rcp(rijm);
@@ -993,9 +993,14 @@ struct RunExt {
         const TF stretch = (TF)(rlen - L0[k]);
         const TF A = br * br * PI;
         const TF J = PI * br * br * br * br;
+        if (kt) {
+            *kt += (double)((kn + ks) * A);
+            *kr += (double)((TF)0.25f * kn * J + (TF)0.5f * ks * J + (TF)0.25f * ks * A * rijm * rijm);
+        }
         TF cef = kn * stretch;
         TF Sc = cef;
         cef *= A;
+        fnsum += std::fabs((double)cef);
         fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
         V3<TF>& Rk = Rij[k];
         const TF tx = Rk.y * nz - Rk.z * ny, ty = Rk.z * nx - Rk.x * nz, tz = Rk.x * ny - Rk.y * nx;
@@ -1025,8 +1030,7 @@ struct RunExt {
             const TF my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
             const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
             Mijt[k] = {mx, my, mz};
-            c2 *= J;
-            ms.x += mx * c2; ms.y += my * c2; ms.z += mz * c2;
+            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;    // no Q1 factor in this model
         }
         TF Mc;
         {
@@ -1062,22 +1066,24 @@ struct RunExt {
     }
 
     // One overlapping pair (engine contact_pair_ext).
-    void contact(uint64_t k, const V3<TF>& r, TF rijm, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
-                 const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms) {
+    void contact(uint64_t k, const V3<TF>& r, TF rijm, TF delta, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
+                 const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms, double& fnsum,
+                 double* kt, double* kr) {
         const TF inv_rm = rcp(rijm);
         const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
         const TF Rs = ri * rj / (ri + rj);
         const TF ms_ = mi * mj / (mi + mj);
-        const TF delta = ri + rj - rijm;
         TF c1 = std::sqrt(Rs * std::fabs(delta));
         const TF Kn = (TF)2.0f * hm_E * c1;
         const TF Kt = (TF)8.0f * hm_G * c1;
+        if (kt) { *kt += (double)(Kn + Kt); *kr += (double)(Kt * ri * ri); }
         const TF ax = ri * wi.x + rj * wj.x, ay = ri * wi.y + rj * wj.y, az = ri * wi.z + rj * wj.z;
         const TF vx = vj.x - vi.x + (ny * az - nz * ay);
         const TF vy = vj.y - vi.y + (nz * ax - nx * az);
         const TF vz = vj.z - vi.z + (nx * ay - ny * ax);
         const TF vn = nx * vx + ny * vy + nz * vz;
         const TF fn = -delta * Kn * two_thirds_t<TF>();
+        fnsum += std::fabs((double)fn);
         c1 = (TF)-1.8257f * p_A * vn * std::sqrt(Kn * ms_);
         fs.x += nx * (fn + c1); fs.y += ny * (fn + c1); fs.z += nz * (fn + c1);
         const TF vtx = vx - nx * vn, vty = vy - ny * vn, vtz = vz - nz * vn;
@@ -1108,23 +1114,28 @@ struct RunExt {
         ms.x += (ny * ftz - nz * fty) * ri;
         ms.y += (nz * ftx - nx * ftz) * ri;
         ms.z += (nx * fty - ny * ftx) * ri;
-        const TF wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
-        if ((double)wim > 1e-18) {
-            const TF cr = -mur * std::fabs(fn) * rsqrt_rn<TF>(wim);
-            ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
-        } else {
-            ms = {0, 0, 0};    // QUIRK (md_calculateforcesdem3.cu:316-336): clears the contact sum
+        if (mur != (TF)0) {
+            const TF wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
+            if ((double)wim > 1e-18) {
+                const TF cr = -mur * std::fabs(fn) * rsqrt_rn<TF>(wim);
+                ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
+            } else {
+                ms = {0, 0, 0};    // QUIRK (md_calculateforcesdem3.cu:316-336): clears the contact sum
+            }
         }
     }
 
     bool running() const { return t->Compress.Strain < t->Compress.MaxStrain && !t->Compress.Fracture; }
 
-    void step(double* curve, uint64_t cap, uint64_t* nsaved) {
-        rf_compression& Kc = t->Compress;
-        delete_far();                       // the previous step's DeleteFarLinks
-        add_links();
-        std::vector<V3<TF>> Fn(N), Mn(N);
+    // Forces and moments of every particle (the _22 then _21 slot orders), and the sums
+    // of |normal pair force| and of the pair count over bonds and overlapping contacts.
+    void pair_forces(std::vector<V3<TF>>& Fn, std::vector<V3<TF>>& Mn, double& fnsum, double& npair,
+                     std::vector<double>* KT = nullptr, std::vector<double>* KR = nullptr) {
+        fnsum = 0; npair = 0;
         for (uint64_t i = 0; i < N; ++i) {
+            double* kt = KT ? &(*KT)[i] : nullptr;
+            double* kr = KR ? &(*KR)[i] : nullptr;
+            if (kt) { *kt = 0; *kr = 0; }
             const V3<TF> vi = {V[i], V[i + N], V[i + 2 * N]}, wi = {W[i], W[i + N], W[i + 2 * N]};
             const TF ri = (TF)rad[i];
             const TF mi = cmass * ri * ri * ri;
@@ -1138,7 +1149,8 @@ struct RunExt {
                 const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
                 const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
                 const TF br = lambda * std::min(ri, (TF)rad[j]);
-                if (bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb)) { type[k] = 0; ++broken; }
+                if (bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb, fnsum, kt, kr)) { type[k] = 0; ++broken; }
+                npair += 1;
             }
             for (uint64_t q = 0; q < K; ++q) {                   // _21 order: type-0 slots by slot
                 const uint64_t k = i * K + q;
@@ -1147,11 +1159,13 @@ struct RunExt {
                 const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const TF rj = (TF)rad[j];
-                const TF rijm = (TF)std::sqrt(d2);
-                if (!(rijm < ri + rj)) { Oijt[k] = {0, 0, 0}; continue; }
+                const double rl = std::sqrt(d2), dl = (rad[i] + rad[j]) - rl;   // overlap in double
+                if (!(dl > 0.0)) { Oijt[k] = {0, 0, 0}; continue; }
+                const TF rijm = (TF)rl;
                 const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
                 const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
-                contact(k, r, rijm, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsc, msc);
+                contact(k, r, rijm, (TF)dl, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsc, msc, fnsum, kt, kr);
+                npair += 1;
             }
             TF Fx = (TF)0 + fsb.x, Fy = (TF)0 + fsb.y, Fz = (TF)0 + fsb.z;
             Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
@@ -1159,62 +1173,79 @@ struct RunExt {
             Mx += msc.x; My += msc.y; Mz += msc.z;
             Fn[i] = {Fx, Fy, Fz}; Mn[i] = {Mx, My, Mz};
         }
-        // platen, increments, cut (per particle, in particle order)
-        double sfb = 0, sft = 0;
+    }
+
+    // Platen of one particle (the extended model's d_braziltest_simple2 /
+    // d_UniaxialCompression3_simple on FP64 coordinates).
+    void platen(uint64_t i, TF& Fx, TF& Fy, TF& Fz, double& Rx, double& Ry, double& Rz, TF& Vx, TF& Vy, TF& Vz,
+                TF vt, double& sfb, double& sft) const {
+        const rf_compression& Kc = t->Compress;
         const float cx = Kc.center.x, cy = Kc.center.y, cz = Kc.center.z, RR = Kc.RR;
         const double Top = Kc.Top, Bottom = Kc.Bottom, TopR = Kc.TopR, BottomR = Kc.BottomR;
-        const TF vt = (TF)(float)Kc.V;
         const bool brz = t->kind == RF_TEST_BRAZIL;
         const double Zcut = brz ? (double)(float)((double)t->S.center.y + (double)t->S.spacesized2.y)
                                 : (double)(float)((double)t->S.center.z + (double)t->S.spacesized2.z);
+        (void)i;
+        if (brz) {
+            const TF rx = (TF)(float)(Rx - cx), rz = (TF)(float)(Rz - cz);
+            if (rx * rx + rz * rz < (TF)RR && (double)rz < Zcut) {
+                if (Ry - TopR > -1e-9) {
+                    const TF fy = Fy;
+                    if (fy > 0) {
+                        sft += (double)fy;
+                        TF iv = Vx * Vx + Vz * Vz;
+                        if ((double)iv > 1e-9) {
+                            iv = rsqrt_rn<TF>(iv);
+                            Fx -= (TF)0.45f * fy * Vx * iv;
+                            Fz -= (TF)0.45f * fy * Vz * iv;
+                        }
+                    }
+                    if (Ry - Top > -1e-9) { Ry = Top; Vy = vt; Fy = 0; }
+                }
+                if (Ry - BottomR < 1e-9) {
+                    const TF fy = Fy;
+                    if (fy < 0) {
+                        sfb += (double)fy;
+                        TF iv = Vx * Vx + Vz * Vz;
+                        if ((double)iv > 1e-9) {
+                            iv = rsqrt_rn<TF>(iv);
+                            Fx += (TF)0.45f * fy * Vx * iv;
+                            Fz += (TF)0.45f * fy * Vz * iv;
+                        }
+                    }
+                    if (Ry - Bottom < 1e-9) { Ry = Bottom; Vy = 0; Fy = 0; }
+                }
+            }
+        } else {
+            const TF rx = (TF)(float)(Rx - cx), ry = (TF)(float)(Ry - cy);
+            if (rx * rx + ry * ry < (TF)RR && Rz < Zcut) {
+                if (Rz - TopR > -1e-9) {
+                    if (Fz > 0) sft += (double)Fz;
+                    if (Rz - Top > -1e-9) { Rz = Top; Vz = vt; Fz = 0; }
+                }
+                if (Rz - BottomR < 1e-9) {
+                    if (Fz < 0) sfb += (double)Fz;
+                    if (Rz - Bottom < 1e-9) { Rz = Bottom; Vz = 0; Fz = 0; }
+                }
+            }
+        }
+    }
+
+    void step(double* curve, uint64_t cap, uint64_t* nsaved) {
+        rf_compression& Kc = t->Compress;
+        delete_far();                       // the previous step's DeleteFarLinks
+        add_links();
+        std::vector<V3<TF>> Fn(N), Mn(N);
+        double fnsum, npair;
+        pair_forces(Fn, Mn, fnsum, npair);
+        double sfb = 0, sft = 0;
+        const TF vt = (TF)(float)Kc.V;
         const rf_sample& S = t->S;
         for (uint64_t i = 0; i < N; ++i) {
             TF Fx = Fn[i].x, Fy = Fn[i].y, Fz = Fn[i].z;
             double Rx = R[i], Ry = R[i + N], Rz = R[i + 2 * N];
             TF Vx = V[i], Vy = V[i + N], Vz = V[i + 2 * N];
-            if (brz) {
-                const TF rx = (TF)(float)(Rx - cx), rz = (TF)(float)(Rz - cz);
-                if (rx * rx + rz * rz < (TF)RR && (double)rz < Zcut) {
-                    if (Ry - TopR > -1e-9) {
-                        const TF fy = Fy;
-                        if (fy > 0) {
-                            sft += (double)fy;
-                            TF iv = Vx * Vx + Vz * Vz;
-                            if ((double)iv > 1e-9) {
-                                iv = rsqrt_rn<TF>(iv);
-                                Fx -= (TF)0.45f * fy * Vx * iv;
-                                Fz -= (TF)0.45f * fy * Vz * iv;
-                            }
-                        }
-                        if (Ry - Top > -1e-9) { Ry = Top; Vy = vt; Fy = 0; }
-                    }
-                    if (Ry - BottomR < 1e-9) {
-                        const TF fy = Fy;
-                        if (fy < 0) {
-                            sfb += (double)fy;
-                            TF iv = Vx * Vx + Vz * Vz;
-                            if ((double)iv > 1e-9) {
-                                iv = rsqrt_rn<TF>(iv);
-                                Fx += (TF)0.45f * fy * Vx * iv;
-                                Fz += (TF)0.45f * fy * Vz * iv;
-                            }
-                        }
-                        if (Ry - Bottom < 1e-9) { Ry = Bottom; Vy = 0; Fy = 0; }
-                    }
-                }
-            } else {
-                const TF rx = (TF)(float)(Rx - cx), ry = (TF)(float)(Ry - cy);
-                if (rx * rx + ry * ry < (TF)RR && Rz < Zcut) {
-                    if (Rz - TopR > -1e-9) {
-                        if (Fz > 0) sft += (double)Fz;
-                        if (Rz - Top > -1e-9) { Rz = Top; Vz = vt; Fz = 0; }
-                    }
-                    if (Rz - BottomR < 1e-9) {
-                        if (Fz < 0) sfb += (double)Fz;
-                        if (Rz - Bottom < 1e-9) { Rz = Bottom; Vz = 0; Fz = 0; }
-                    }
-                }
-            }
+            platen(i, Fx, Fy, Fz, Rx, Ry, Rz, Vx, Vy, Vz, vt, sfb, sft);
             const TF ri = (TF)rad[i];
             const TF mi = cmass * ri * ri * ri;
             const TF dtm = dt / mi, dtI = dt / ((TF)0.4f * mi * ri * ri);
@@ -1233,6 +1264,111 @@ struct RunExt {
         sum_forces(t, sfb, sft, sz0, curve, cap, nsaved);
         compress(t, Kc.Stress);
         ++steps;
+    }
+
+    // One quasi-static load increment relaxed by FIRE, as the engine runs it
+    // (rf_engine_load_increment): platen advance, rest start, then iterations of
+    // [delete, add, forces with the FIRE dt and without damping or rolling resistance,
+    // platen clamp at rest, FIRE decision on FP64 sums, mixing and semi-implicit Euler].
+    // trace (may be null) receives the residual of every iteration.
+    uint64_t fire_increment(const rf_relax_params& p, int* converged, double* residual, double* trace,
+                            uint64_t trace_cap) {
+        rf_compression& Kc = t->Compress;
+        const int ax = t->kind == RF_TEST_BRAZIL ? 1 : 2;
+        const double delta = p.strain_inc * Kc.Size0;
+        double* sz = ax == 1 ? &Kc.size_d.y : &Kc.size_d.z;
+        double* cd = ax == 1 ? &Kc.center_d.y : &Kc.center_d.z;
+        *sz -= delta;
+        Kc.Top -= delta;
+        Kc.TopR = Kc.Top - 2.0 * t->Po.p_r;
+        *cd -= delta;
+        if (ax == 1) { Kc.size.y = (float)*sz; Kc.sized2.y = (float)(0.5 * *sz); Kc.center.y = (float)*cd; Kc.Hd2 = Kc.sized2.y; }
+        else { Kc.size.z = (float)*sz; Kc.sized2.z = (float)(0.5 * *sz); Kc.center.z = (float)*cd; Kc.Hd2 = Kc.sized2.z; }
+        Kc.Strain = (*sz - Kc.Size0) / Kc.Size0;
+        std::fill(V.begin(), V.end(), (TF)0);
+        std::fill(W.begin(), W.end(), (TF)0);
+        // the platen pushes the particles it passed: clamp them now, so the first force
+        // pass (and its convergence test) sees the loaded configuration
+        for (uint64_t i = 0; i < N; ++i) {
+            TF f0 = 0, f1 = 0, f2 = 0, v0 = 0, v1 = 0, v2 = 0;
+            double sb = 0, st = 0;
+            platen(i, f0, f1, f2, R[i], R[i + N], R[i + 2 * N], v0, v1, v2, (TF)0, sb, st);
+        }
+        const TF dt_keep = dt, pA_keep = p_A, mur_keep = mur;
+        p_A = 0; mur = 0;
+        double fdt = p.dt0, alpha = p.alpha0, cv = 1, cf = 0, cm = 0;
+        uint64_t npos = 0, it = 0;
+        bool uphill = false;
+        *converged = 0;
+        std::vector<V3<TF>> Fn(N), Mn(N);
+        std::vector<double> KT(N), KR(N);
+        for (;;) {
+            dt = (TF)(float)fdt;
+            delete_far();
+            add_links();
+            double fnsum, npair;
+            pair_forces(Fn, Mn, fnsum, npair, &KT, &KR);
+            double P = 0, FF = 0, VV = 0, MM = 0, WW = 0, sfb = 0, sft = 0;
+            for (uint64_t i = 0; i < N; ++i) {
+                TF Fx = Fn[i].x, Fy = Fn[i].y, Fz = Fn[i].z;
+                double Rx = R[i], Ry = R[i + N], Rz = R[i + 2 * N];
+                TF Vx = V[i], Vy = V[i + N], Vz = V[i + 2 * N];
+                platen(i, Fx, Fy, Fz, Rx, Ry, Rz, Vx, Vy, Vz, (TF)0, sfb, sft);
+                R[i] = Rx; R[i + N] = Ry; R[i + 2 * N] = Rz;
+                V[i] = Vx; V[i + N] = Vy; V[i + 2 * N] = Vz;
+                Fn[i] = {Fx, Fy, Fz};
+                const TF wx = W[i], wy = W[i + N], wz = W[i + 2 * N];
+                const V3<TF> M = Mn[i];
+                P += (double)Fx * Vx + (double)Fy * Vy + (double)Fz * Vz + (double)M.x * wx + (double)M.y * wy +
+                     (double)M.z * wz;
+                FF += (double)Fx * Fx + (double)Fy * Fy + (double)Fz * Fz;
+                VV += (double)Vx * Vx + (double)Vy * Vy + (double)Vz * Vz;
+                MM += (double)M.x * M.x + (double)M.y * M.y + (double)M.z * M.z;
+                WW += (double)wx * wx + (double)wy * wy + (double)wz * wz;
+            }
+            const double mean = npair > 0 ? fnsum / npair : 0.0;
+            const double res = mean > 0 ? std::sqrt(FF / (double)N) / mean : (FF > 0 ? 1e300 : 0.0);
+            Kc.Stress = 0.5 * (std::fabs(sfb) + std::fabs(sft)) * (double)Kc._1d_Area;
+            if (trace && it < trace_cap) trace[it] = res;
+            ++it;
+            *residual = res;
+            if (res <= p.tol) { *converged = 1; break; }
+            if (it >= p.max_iter) break;
+            if (it == 1) {                  // first pass of the increment: start from rest
+                npos = 0;
+                uphill = true;
+            } else if (P > 0) {
+                cv = 1 - alpha;
+                cf = FF > 0 ? alpha * std::sqrt(VV / FF) : 0;
+                cm = MM > 0 ? alpha * std::sqrt(WW / MM) : 0;
+                uphill = false;
+                if (++npos > p.n_delay) { fdt = std::fmin(fdt * p.f_inc, p.dt_max); alpha *= p.f_alpha; }
+            } else {
+                npos = 0;
+                fdt = std::fmax(fdt * p.f_dec, p.dt_min);
+                alpha = p.alpha0;
+                uphill = true;
+            }
+            const TF dtf = (TF)(float)fdt;
+            for (uint64_t i = 0; i < N; ++i) {
+                TF v[3] = {V[i], V[i + N], V[i + 2 * N]}, w[3] = {W[i], W[i + N], W[i + 2 * N]};
+                const TF F[3] = {Fn[i].x, Fn[i].y, Fn[i].z}, M[3] = {Mn[i].x, Mn[i].y, Mn[i].z};
+                // stiffness-scaled (Jacobi) masses: every particle's own frequency is 1
+                const TF mt = (TF)std::max(KT[i], 1e-30), mr = (TF)std::max(KR[i], 1e-30);
+                const TF dtm = dtf / mt, dtI = dtf / mr;
+                for (int a = 0; a < 3; ++a) {
+                    if (uphill) { v[a] = 0; w[a] = 0; }
+                    else { v[a] = (TF)(float)cv * v[a] + (TF)(float)cf * F[a]; w[a] = (TF)(float)cv * w[a] + (TF)(float)cm * M[a]; }
+                    v[a] += F[a] * dtm;
+                    w[a] += M[a] * dtI;
+                    R[i + a * N] += (double)v[a] * (double)dtf;
+                    V[i + a * N] = v[a];
+                    W[i + a * N] = w[a];
+                }
+            }
+        }
+        dt = dt_keep; p_A = pA_keep; mur = mur_keep;
+        return it;
     }
 };
 
@@ -1259,7 +1395,40 @@ static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const
 
 }  // namespace rfo
 
+namespace rfo {
+// Quasi-static run: n_inc increments; per increment its iteration count, convergence,
+// residual and platen stress. trace: residual per iteration of the last increment.
+template <class TF>
+static int qs_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const double* rad, const rf_relax_params* p,
+                  uint64_t n_inc, uint64_t* iters, int* conv, double* res, double* stress, double* trace,
+                  uint64_t trace_cap) {
+    RunExt<TF> r;
+    r.t = t;
+    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed};
+    r.init(R_io, rad);
+    for (uint64_t k = 0; k < n_inc; ++k) {
+        int c = 0;
+        double rr = 0;
+        const bool last = k + 1 == n_inc;
+        iters[k] = r.fire_increment(*p, &c, &rr, last ? trace : nullptr, trace_cap);
+        conv[k] = c; res[k] = rr; stress[k] = t->Compress.Stress;
+    }
+    std::memcpy(R_io, r.R.data(), sizeof(double) * 3 * r.N);
+    return r.status;
+}
+}  // namespace rfo
+
 extern "C" {
+int rfo_qs_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, const rf_relax_params* p,
+                 uint64_t n_inc, uint64_t* iters, int* conv, double* res, double* stress, double* trace,
+                 uint64_t trace_cap) {
+    return rfo::qs_ext<float>(t, x, R_io, rad, p, n_inc, iters, conv, res, stress, trace, trace_cap);
+}
+int rfo_qs_ext_d(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, const rf_relax_params* p,
+                 uint64_t n_inc, uint64_t* iters, int* conv, double* res, double* stress, double* trace,
+                 uint64_t trace_cap) {
+    return rfo::qs_ext<double>(t, x, R_io, rad, p, n_inc, iters, conv, res, stress, trace, trace_cap);
+}
 // Extended model, float forces (the engine's arithmetic) and FP64 (the FP64 oracle).
 // R_io: double[3N] planar in, final positions out (after the pending delete pass).
 uint64_t rfo_run_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,
@@ -1394,6 +1563,35 @@ void rfo_cut_restriction_f(float* R, float* V, float* F, uint64_t N, rf_float3 c
                            rf_float3 hp) {
     rfo::cut_restriction<float>(R, V, F, N, {center.x, center.y, center.z}, {sized2.x, sized2.y, sized2.z},
                                 {hp.x, hp.y, hp.z});
+}
+// d_CalculateIncrementsFIRE (md_firerelaxation.cu:18-56): V is replaced by F * dt0/m
+// (QUIRK: no memory of the previous V), mixed with F by the per-particle ratio |v|/|F|
+// (also a no-op, v being parallel to F), and R advances by V * dt.
+void rfo_fire_increments_f(const float* F, float* V, float* R, uint64_t N, float dtm, float dt, float a) {
+    for (uint64_t i = 0; i < N; ++i) {
+        const float Fx = F[i], Fy = F[i + N], Fz = F[i + 2 * N];
+        float vx = Fx * dtm, vy = Fy * dtm, vz = Fz * dtm;
+        const float vv = vx * vx + vy * vy + vz * vz;
+        const float f = Fx * Fx + Fy * Fy + Fz * Fz;
+        float vdf;
+        if (f > 1e-12f) vdf = a * std::sqrt(vv * (1.0f / f));
+        else vdf = a * std::sqrt(vv) * (float)1e6;
+        vx = (1.0f - a) * vx + vdf * Fx;
+        vy = (1.0f - a) * vy + vdf * Fy;
+        vz = (1.0f - a) * vz + vdf * Fz;
+        V[i] = vx; V[i + N] = vy; V[i + 2 * N] = vz;
+        R[i] += vx * dt; R[i + N] += vy * dt; R[i + 2 * N] += vz * dt;
+    }
+}
+// d_CalculateDecrementsHalfStepFIRE (md_firerelaxation.cu:58-70)
+void rfo_fire_half_f(const float* V, float* R, uint64_t N, float dt2) {
+    for (uint64_t q = 0; q < 3 * N; ++q) R[q] -= V[q] * dt2;
+}
+// d_FdotVEntire (md_firerelaxation.cu:372-490), summed in double.
+double rfo_fdotv_f(const float* V, const float* F, uint64_t N) {
+    double s = 0.0;
+    for (uint64_t q = 0; q < 3 * N; ++q) s += (double)F[q] * (double)V[q];
+    return s;
 }
 float rfo_rsqrt_rn_f(float x) { return rfo::rsqrt_rn<float>(x); }
 void rfo_rsqrt_rn_array_f(const float* x, float* y, uint64_t n) {

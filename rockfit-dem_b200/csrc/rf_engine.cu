@@ -52,6 +52,11 @@ struct DevScalars {
     int32_t Loading, Fracture;
     unsigned long long steps, target, rebuilds, curve_n, broken;
     uint32_t done, err, rebuild, moved, block_counter, pad;
+    // FIRE relaxation of a quasi-static load increment (extended model)
+    double fdt, falpha, fdt0, fdtmax, fdtmin, finc, fdec, falpha0, fshrink, ftol;
+    double fresidual, fmean, fpower, fcv, fcf, fcm;
+    unsigned long long fiter, fmax_iter, fnpos, fiter_total;
+    uint32_t fndelay, fuphill, fconverged, fstop, fcounter, fwarm;
 };
 
 struct Consts {
@@ -114,6 +119,12 @@ struct Dev {
     uint32_t* cg_bsum;
     uint32_t* cg_sorted;   // [N]
     double2* partial;   // [blocks]
+    // FIRE relaxation (allocated on first use)
+    float4* frc;        // [N] net force after the platen clamp
+    float4* mom;        // [N] net moment
+    double* fpart;      // [blocks][FIRE_SUMS] FP64 block partial sums
+    double4* rot;       // [N] accumulated rotation of the increment (sum of w dt)
+    double4* x0;        // [N] positions at the start of the increment
     unsigned long long n_particles;
     uint32_t QB;
     double* curve;      // [cap][3]
@@ -761,11 +772,21 @@ __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, doub
     }
 }
 
+#define FIRE_SUMS 9     // F.v + M.w, |F|^2, |v|^2, |M|^2, |w|^2, sum |f_n|, pair count, platen sums (2)
+
 template <int KIND>
+__device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c, double (&acc)[FIRE_SUMS]);
+
+// MODE 0: explicit step (Verlet increments, platen moving at V). MODE 1: force evaluation
+// of one FIRE iteration: the same forces with the FIRE time step, platens at rest; net
+// force and moment are stored for k_fire_update and FP64 sums of the FIRE power, the
+// squared norms and the mean normal pair force are reduced for the FIRE decision.
+template <int KIND, int MODE>
 __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Consts c) {
     DevScalars* sc = d.sc;
     if (c.use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c.h_loop, 0u);
-    if (sc->done) return;
+    if (MODE == 0 && sc->done) return;
+    if (MODE == 1 && sc->fstop) return;
     const uint32_t cur = (uint32_t)(sc->steps & 1ull), nxt = cur ^ 1u;
     const double4* __restrict__ P = d.posd[cur];
     const float4* __restrict__ Vv = d.vel[cur];
@@ -775,9 +796,20 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
     const bool valid = i < N;
     const uint32_t FULL = 0xffffffffu;
     const double Top = sc->Top, Bottom = sc->Bottom, TopR = sc->TopR, BottomR = sc->BottomR;
-    const float vt = (float)sc->V, RR = sc->RR;
+    const float vt = MODE == 0 ? (float)sc->V : 0.f, RR = sc->RR;
     rf_float3 cc;
     cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
+    ExtParams ep = c.ep;
+    if (MODE == 1) {
+        // FIRE minimises the conservative part of the model: its own velocity mixing
+        // and restarts replace the viscous contact damping, and the constant-torque
+        // rolling resistance (a set-valued term at rest) is left out.
+        ep.dt = (float)sc->fdt;
+        ep.p_A = 0.f;
+        ep.mur = 0.f;
+    }
+    float fnabs = 0.f, kt = 0.f, kr = 0.f;
+    uint32_t npair = 0;
 
     double4 xi = make_double4(0, 0, 0, 1);
     f3 vi = mk3(0.f, 0.f, 0.f), wi = vi;
@@ -794,7 +826,6 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
     const uint32_t live0 = live, bond0 = bond, cm0 = cm, bmask0 = bmask;
     const unsigned long long mem0 = mem;
     const size_t QN = (size_t)d.QB * N;
-    const ExtParams& ep = c.ep;
 
     f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
     uint32_t nbroken = 0;
@@ -821,7 +852,8 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
             f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
             f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
             const bool broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(__ldg(&Vv[j])), wi, f4to3(__ldg(&Wv[j])),
-                                             rij, oijt, mijn, mijt, fsb, msb);
+                                             rij, oijt, mijn, mijt, fsb, msb, fnabs, kt, kr);
+            ++npair;
             d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
             d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
             d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
@@ -834,6 +866,8 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
     float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
     f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
     uint32_t cm_out = 0;
+    float fnc = 0.f, ktc = 0.f, krc = 0.f;   // contact force magnitudes and stiffness (recounted on a replay)
+    uint32_t npc = 0;
     auto contact_pass = [&](bool with_delete) {
         uint32_t m = live & ~bond;
         while (m) {
@@ -848,14 +882,16 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
                 continue;
             }
             const float rj = (float)xj.w;
-            const float rijm = (float)sqrt(rr);
-            if (!(rijm < ri + rj)) continue;
+            const double rl = sqrt(rr), dl = (xi.w + xj.w) - rl;
+            if (!(dl > 0.0)) continue;
+            const float rijm = (float)rl;
             const uint32_t bit = 1u << k;
             // cm: step-start contacts minus slots deleted this step (a refilled slot starts at zero)
             f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
             const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
-            contact_pair_ext(ep, r, rijm, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(__ldg(&Vv[j])), wi,
-                             f4to3(__ldg(&Wv[j])), o, fsc, msc);
+            contact_pair_ext(ep, r, rijm, (float)dl, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(__ldg(&Vv[j])), wi,
+                             f4to3(__ldg(&Wv[j])), o, fsc, msc, fnc, ktc, krc);
+            ++npc;
             oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
             cm_out |= bit;
         }
@@ -895,17 +931,24 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
             live |= 1u << k;
             mem |= 1ull << best_q;
             const double4 xj = ldg_d4(&P[j]);
-            if ((float)sqrt(dlen2(dsub(xj, xi))) < ri + (float)xj.w) replay = true;
+            if ((xi.w + xj.w) - sqrt(dlen2(dsub(xj, xi))) > 0.0) replay = true;
         }
     }
     if (replay) {
-        fsc = mk3(0.f, 0.f, 0.f); msc = fsc; cm_out = 0;
+        fsc = mk3(0.f, 0.f, 0.f); msc = fsc; cm_out = 0; fnc = 0.f; ktc = 0.f; krc = 0.f; npc = 0;
         contact_pass(false);
     }
     cm = cm_out;
+    fnabs += fnc;
+    npair += npc;
+    kt += ktc;
+    kr += krc;
 
     double sfb = 0.0, sft = 0.0;
     uint32_t moved = 0;
+    double acc[FIRE_SUMS];
+#pragma unroll
+    for (int q = 0; q < FIRE_SUMS; ++q) acc[q] = 0.0;
     if (valid) {
         if (live != live0) d.live[i] = live;
         if (bond != bond0) d.bond[i] = bond;
@@ -924,6 +967,25 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         else
             uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)c.zcut, sfb,
                                   sft);
+        if (MODE == 1) {
+            // FIRE: keep the clamped state for the update kernel; reduce the FIRE sums
+            d.posd[nxt][i] = make_double4(Rx, Ry, Rz, xi.w);
+            d.vel[nxt][i] = make_float4(Vx, Vy, Vz, 0.f);
+            d.ang[nxt][i] = make_float4(wi.x, wi.y, wi.z, 0.f);
+            d.frc[i] = make_float4(Fx, Fy, Fz, kt);
+            d.mom[i] = make_float4(Mx, My, Mz, kr);
+            acc[0] = (double)Fx * Vx + (double)Fy * Vy + (double)Fz * Vz + (double)Mx * wi.x + (double)My * wi.y +
+                     (double)Mz * wi.z;
+            acc[1] = (double)Fx * Fx + (double)Fy * Fy + (double)Fz * Fz;
+            acc[2] = (double)Vx * Vx + (double)Vy * Vy + (double)Vz * Vz;
+            acc[3] = (double)Mx * Mx + (double)My * My + (double)Mz * Mz;
+            acc[4] = (double)wi.x * wi.x + (double)wi.y * wi.y + (double)wi.z * wi.z;
+            acc[5] = (double)fnabs;
+            acc[6] = (double)npair;
+            acc[7] = sfb;
+            acc[8] = sft;
+        }
+        if (MODE == 0) {
         const float dtm = ep.dt / mi, dtI = ep.dt / (0.4f * mi * ri * ri);
         Vx += Fx * dtm; Vy += Fy * dtm; Vz += Fz * dtm;
         Rx += (double)(Vx * ep.dt); Ry += (double)(Vy * ep.dt); Rz += (double)(Vz * ep.dt);
@@ -940,8 +1002,244 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         const float4 pr = d.pos_ref[i];
         const float ex = (float)Rx - pr.x, ey = (float)Ry - pr.y, ez = (float)Rz - pr.z;
         moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+        }
     }
-    step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
+    if (MODE == 0) {
+        step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
+    } else {
+        const uint32_t nb = __reduce_add_sync(FULL, nbroken);
+        if ((threadIdx.x & 31) == 0 && nb) atomicAdd(&sc->broken, (unsigned long long)nb);
+        fire_force_finish<KIND>(d, c, acc);
+    }
+}
+
+// Block sums of the FIRE accumulators (fixed tree); the last block adds the block
+// partials in block order and makes the FIRE decision (Bitzek et al. 2006), in FP64:
+//   residual = sqrt(sum |F_i|^2 / N) / (mean normal pair force); converged when <= tol;
+//   P = F.v + M.w > 0: mixing v <- (1-a) v + a (|v|/|F|) F (same for w with M), and after
+//   n_delay such steps dt <- min(dt f_inc, dt_max), a <- a f_alpha;
+//   P <= 0: dt <- max(dt f_dec, dt_min), a <- a0, v = w = 0.
+template <int KIND>
+__device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c, double (&acc)[FIRE_SUMS]) {
+    DevScalars* sc = d.sc;
+    const uint32_t FULL = 0xffffffffu;
+    __shared__ double s_acc[4][FIRE_SUMS];
+    __shared__ bool s_last;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < FIRE_SUMS; ++q) {
+        double v = acc[q];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+        if (l == 0) s_acc[w][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < FIRE_SUMS) {
+        const int q = threadIdx.x;
+        d.fpart[(size_t)blockIdx.x * FIRE_SUMS + q] = (s_acc[0][q] + s_acc[1][q]) + (s_acc[2][q] + s_acc[3][q]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&sc->fcounter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    __shared__ double tot[FIRE_SUMS];
+    if (threadIdx.x < FIRE_SUMS) {
+        double v = 0.0;
+        for (uint32_t b = 0; b < gridDim.x; ++b) v += __ldcg(&d.fpart[(size_t)b * FIRE_SUMS + threadIdx.x]);
+        tot[threadIdx.x] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    sc->fcounter = 0;
+    const double P = tot[0], FF = tot[1], VV = tot[2], MM = tot[3], WW = tot[4], FN = tot[5], NP = tot[6];
+    const double mean = NP > 0.0 ? FN / NP : 0.0;
+    const double rms = sqrt(FF / (double)c.N);
+    sc->fmean = mean;
+    sc->fresidual = mean > 0.0 ? rms / mean : (FF > 0.0 ? 1e300 : 0.0);
+    sc->fpower = P;
+    // platen stress of this configuration (SumForcesULoading's formula)
+    const double a1 = (double)sc->_1d_Area;
+    sc->Stress = 0.5 * (fabs(tot[7]) + fabs(tot[8])) * a1;
+    sc->fiter += 1;
+    sc->fiter_total += 1;
+    sc->steps += 1;                     // buffer parity: the update works on what this pass wrote
+    if (sc->fresidual <= sc->ftol) { sc->fconverged = 1; sc->fstop = 1; return; }
+    if (sc->fiter >= sc->fmax_iter) { sc->fstop = 1; return; }
+    if (sc->fwarm) {
+        // first pass of an increment: the velocities only carried the start motion into
+        // the state; the dynamics starts from rest
+        sc->fwarm = 0;
+        sc->fuphill = 1;
+        sc->fnpos = 0;
+        sc->fcv = 0.0; sc->fcf = 0.0; sc->fcm = 0.0;
+    } else if (P > 0.0) {
+        const double a = sc->falpha;
+        sc->fcv = 1.0 - a;
+        sc->fcf = FF > 0.0 ? a * sqrt(VV / FF) : 0.0;
+        sc->fcm = MM > 0.0 ? a * sqrt(WW / MM) : 0.0;
+        sc->fuphill = 0;
+        sc->fnpos += 1;
+        if (sc->fnpos > sc->fndelay) {
+            sc->fdt = fmin(sc->fdt * sc->finc, sc->fdtmax);
+            sc->falpha = a * sc->fshrink;
+        }
+    } else {
+        sc->fnpos = 0;
+        sc->fdt = fmax(sc->fdt * sc->fdec, sc->fdtmin);
+        sc->falpha = sc->falpha0;
+        sc->fuphill = 1;
+        sc->fcv = 0.0; sc->fcf = 0.0; sc->fcm = 0.0;
+    }
+}
+
+// FIRE update of one iteration, in place on the buffers the force pass wrote:
+// mixing (or, on uphill power, stop), then semi-implicit Euler in FP64
+// positions; the rotation of the increment is accumulated for the warm-start data.
+__global__ void k_fire_update(Dev d, Consts c) {
+    DevScalars* sc = d.sc;
+    const uint32_t cur = (uint32_t)(sc->steps & 1ull);
+    const bool stop = sc->fstop != 0;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t moved = 0;
+    if (!stop && i < c.N) {
+        double4 x = d.posd[cur][i];
+        float4 v = d.vel[cur][i], w = d.ang[cur][i];
+        const float4 F = d.frc[i], M = d.mom[i];
+        const float dt = (float)sc->fdt;
+        const double dtd = (double)dt;
+        if (sc->fuphill) {
+            // stop (no half step back: the bond and contact state integrates v dt, so every
+            // position change must be a v dt of the force pass that follows)
+            v = make_float4(0.f, 0.f, 0.f, 0.f);
+            w = v;
+        } else {
+            const float cv = (float)sc->fcv, cf = (float)sc->fcf, cm = (float)sc->fcm;
+            v.x = cv * v.x + cf * F.x; v.y = cv * v.y + cf * F.y; v.z = cv * v.z + cf * F.z;
+            w.x = cv * w.x + cm * M.x; w.y = cv * w.y + cm * M.y; w.z = cv * w.z + cm * M.z;
+        }
+        // stiffness-scaled (Jacobi) masses: every particle's own frequency is 1, so the
+        // FIRE step is dimensionless and stiffness contrasts do not slow the relaxation
+        const float dtm = dt / fmaxf(F.w, 1e-30f), dtI = dt / fmaxf(M.w, 1e-30f);
+        v.x += F.x * dtm; v.y += F.y * dtm; v.z += F.z * dtm;
+        w.x += M.x * dtI; w.y += M.y * dtI; w.z += M.z * dtI;
+        x.x += (double)v.x * dtd; x.y += (double)v.y * dtd; x.z += (double)v.z * dtd;
+        double4 r = d.rot[i];
+        r.x += (double)w.x * dtd; r.y += (double)w.y * dtd; r.z += (double)w.z * dtd;
+        d.rot[i] = r;
+        d.posd[cur][i] = x;
+        d.vel[cur][i] = v;
+        d.ang[cur][i] = w;
+        const float4 pr = d.pos_ref[i];
+        const float ex = (float)x.x - pr.x, ey = (float)x.y - pr.y, ez = (float)x.z - pr.z;
+        moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+    }
+    __shared__ bool s_last;
+    __shared__ uint32_t s_m;
+    if (threadIdx.x == 0) s_m = 0;
+    __syncthreads();
+    if (__reduce_or_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(&s_m, 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_m) atomicOr(&sc->moved, 1u);
+        __threadfence();
+        s_last = (atomicAdd(&sc->block_counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    sc->block_counter = 0;
+    const uint32_t mv = sc->moved;
+    sc->moved = 0;
+    sc->rebuild = mv;
+    if (c.use_graph) {
+        cudaGraphSetConditional(c.h_rebuild, (mv && !sc->fstop) ? 1u : 0u);
+        cudaGraphSetConditional(c.h_loop, sc->fstop ? 0u : 1u);
+    }
+}
+
+// Start of a quasi-static load increment: advance the loading platen by the increment
+// (CompressU / CompressB with V dt replaced by -delta), reset the FIRE state, start
+// from rest, remember the start positions, and apply a warm start if given:
+// warm[i*6 + 0..2] is added to the position, warm[i*6 + 3..5] / dt0 becomes the
+// initial angular velocity (so the first iteration's bond and contact state advance
+// by that rotation).
+template <int KIND>
+__global__ void k_qs_begin_scalars(Dev d, Consts c, double delta) {
+    DevScalars* sc = d.sc;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+        sc->V = 0.0;
+        sc->size_d[ax] -= delta;
+        sc->Top -= delta;
+        sc->TopR = sc->Top - 2.0 * c.p_r_d;
+        sc->size[ax] = (float)sc->size_d[ax];
+        sc->sized2[ax] = (float)(0.5 * sc->size_d[ax]);
+        sc->center_d[ax] -= delta;
+        sc->center[ax] = (float)sc->center_d[ax];
+        sc->Hd2 = sc->sized2[ax];
+        sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
+        sc->fdt = sc->fdt0;
+        sc->falpha = sc->falpha0;
+        sc->fnpos = 0; sc->fiter = 0; sc->fuphill = 0; sc->fconverged = 0; sc->fstop = 0; sc->fcounter = 0;
+        sc->fcv = 1.0; sc->fcf = 0.0; sc->fcm = 0.0;
+        sc->fwarm = 1;
+        sc->done = 0;
+        sc->rebuild = 1;          // positions jumped (platen clamp, warm start): rebuild the candidates
+    }
+}
+template <int KIND>
+__global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm) {
+    DevScalars* sc = d.sc;
+    const uint32_t cur = (uint32_t)(sc->steps & 1ull);
+    const float idt0 = (float)(1.0 / sc->fdt0);
+    const double Top = sc->Top, Bottom = sc->Bottom, TopR = sc->TopR, BottomR = sc->BottomR;
+    const float RR = sc->RR;
+    rf_float3 cc;
+    cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        double4 x = d.posd[cur][i];
+        d.x0[i] = x;
+        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+        double4 rot = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (warm) {
+            // predicted displacement and rotation; as velocities over dt0 they make the first
+            // force pass advance the bond and contact state by exactly that motion (the
+            // first update then starts from rest)
+            const float* q = warm + (size_t)i * 6;
+            x.x += (double)q[0]; x.y += (double)q[1]; x.z += (double)q[2];
+            v0 = q[0] * idt0; v1 = q[1] * idt0; v2 = q[2] * idt0;
+            w = make_float4(q[3] * idt0, q[4] * idt0, q[5] * idt0, 0.f);
+            rot = make_double4(q[3], q[4], q[5], 0.0);
+        }
+        // the platen pushes the particles it passed: clamp them now, so the first force
+        // pass (and its convergence test) sees the loaded configuration
+        float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+        double sb = 0.0, st = 0.0;
+        if (KIND == RF_TEST_BRAZIL)
+            brazil_particle_ext(x.x, x.y, x.z, v0, v1, v2, f0, f1, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f,
+                                (double)c.zcut, sb, st);
+        else
+            uniaxial_particle_ext(x.x, x.y, x.z, v2, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f, (double)c.zcut, sb,
+                                  st);
+        d.posd[cur][i] = x;
+        d.vel[cur][i] = make_float4(v0, v1, v2, 0.f);
+        d.ang[cur][i] = w;
+        d.rot[i] = rot;
+    }
+}
+
+// Sets the FIRE loop's graph conditions at the start of a launch.
+__global__ void k_fire_prologue(Dev d, Consts c) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        DevScalars* sc = d.sc;
+        const bool go = !sc->fstop;
+        cudaGraphSetConditional(c.h_rebuild, (go && sc->rebuild) ? 1u : 0u);
+        cudaGraphSetConditional(c.h_loop, go ? 1u : 0u);
+    }
 }
 
 // Sets both graph conditions at the start of a launch.
@@ -1205,6 +1503,11 @@ struct rf_engine {
     float* staging;
     uint64_t bonds_initial;
     uint32_t* maxq_dev;
+    // FIRE relaxation graph (built on the first load increment)
+    Consts cf;
+    cudaGraph_t fgraph;
+    cudaGraphExec_t fexec;
+    bool fire_ready;
 };
 
 namespace {
@@ -1221,7 +1524,7 @@ template <class T> rf_status dalloc(rf_engine* e, T** p, size_t n) {
 
 void* step_kernel(const rf_engine* e) {
     const bool br = e->task.kind == RF_TEST_BRAZIL;
-    if (e->c.ext) return br ? (void*)k_step_ext<RF_TEST_BRAZIL> : (void*)k_step_ext<RF_TEST_UNIAXIAL>;
+    if (e->c.ext) return br ? (void*)k_step_ext<RF_TEST_BRAZIL, 0> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0>;
     return br ? (void*)k_step<RF_TEST_BRAZIL> : (void*)k_step<RF_TEST_UNIAXIAL>;
 }
 
@@ -1282,6 +1585,99 @@ rf_status build_graph(rf_engine* e) {
     kp = kparams(fn, e->nblocks, 128);
     RF_CUDA(cudaGraphAddKernelNode(&step, body, &inode, 1, &kp));
     RF_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
+    return RF_OK;
+}
+
+// FIRE loop graph: prologue -> WHILE(not stopped) { IF(moved) {candidate rebuild}; forces; update }.
+rf_status build_fire_graph(rf_engine* e) {
+    cudaGraph_t g;
+    RF_CUDA(cudaGraphCreate(&g, 0));
+    e->fgraph = g;
+    Consts& c = e->cf;
+    RF_CUDA(cudaGraphConditionalHandleCreate(&c.h_loop, g, 0, 0));
+    RF_CUDA(cudaGraphConditionalHandleCreate(&c.h_rebuild, g, 0, 0));
+    c.use_graph = 1;
+    Dev d = e->d;
+    Consts cc = c;
+    void* args[] = {&d, &cc};
+    auto kparams = [&](void* fn, unsigned grid, unsigned block) {
+        cudaKernelNodeParams kp = {};
+        kp.func = fn; kp.gridDim = dim3(grid); kp.blockDim = dim3(block);
+        kp.sharedMemBytes = 0; kp.kernelParams = args; kp.extra = nullptr;
+        return kp;
+    };
+    cudaGraphNode_t pro;
+    cudaKernelNodeParams kp = kparams((void*)k_fire_prologue, 1, 32);
+    RF_CUDA(cudaGraphAddKernelNode(&pro, g, nullptr, 0, &kp));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = c.h_loop;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    RF_CUDA(cudaGraphAddNode(&wnode, g, &pro, 1, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = c.h_rebuild;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    RF_CUDA(cudaGraphAddNode(&inode, body, nullptr, 0, &ip));
+    cudaGraph_t rb = ip.conditional.phGraph_out[0];
+    const unsigned gN = (c.N + 255) / 256;
+    const unsigned gC = (c.cg_cells + 1 + 255) / 256;
+    struct { void* fn; unsigned grid, block; } seq[] = {
+        {(void*)k_rb_zero, gC, 256},      {(void*)k_rb_bin, gN, 256},
+        {(void*)k_rb_scan_sums, e->cg_nb, 1024}, {(void*)k_rb_scan_totals, 1, 32},
+        {(void*)k_rb_scan_apply, e->cg_nb, 1024}, {(void*)k_rb_scatter, gN, 256},
+        {(void*)k_rb_cand, (c.N + 127) / 128, 128},
+    };
+    cudaGraphNode_t prev = nullptr;
+    for (auto& q : seq) {
+        cudaGraphNode_t n;
+        kp = kparams(q.fn, q.grid, q.block);
+        RF_CUDA(cudaGraphAddKernelNode(&n, rb, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
+        prev = n;
+    }
+    cudaGraphNode_t fnode, unode;
+    void* ff = (e->task.kind == RF_TEST_BRAZIL) ? (void*)k_step_ext<RF_TEST_BRAZIL, 1> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 1>;
+    kp = kparams(ff, e->nblocks, 128);
+    RF_CUDA(cudaGraphAddKernelNode(&fnode, body, &inode, 1, &kp));
+    kp = kparams((void*)k_fire_update, e->nblocks, 128);
+    RF_CUDA(cudaGraphAddKernelNode(&unode, body, &fnode, 1, &kp));
+    RF_CUDA(cudaGraphInstantiate(&e->fexec, g, 0));
+    return RF_OK;
+}
+
+// The FIRE loop on a plain stream (no conditional graph nodes): chunks of iterations,
+// each kernel returning early once the device has stopped the loop.
+rf_status launch_stream_fire(rf_engine* e, uint64_t max_iter) {
+    Dev d = e->d;
+    Consts c = e->cf;
+    c.use_graph = 0;
+    const unsigned gN = (c.N + 255) / 256, gC = (c.cg_cells + 1 + 255) / 256;
+    cudaStream_t s = e->stream;
+    void* ff = (e->task.kind == RF_TEST_BRAZIL) ? (void*)k_step_ext<RF_TEST_BRAZIL, 1> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 1>;
+    void* args[] = {&d, &c};
+    for (uint64_t q = 0; q < max_iter + 1;) {
+        for (int u = 0; u < 32; ++u, ++q) {
+            k_rb_zero<<<gC, 256, 0, s>>>(d, c);
+            k_rb_bin<<<gN, 256, 0, s>>>(d, c);
+            k_rb_scan_sums<<<e->cg_nb, 1024, 0, s>>>(d, c);
+            k_rb_scan_totals<<<1, 32, 0, s>>>(d, c);
+            k_rb_scan_apply<<<e->cg_nb, 1024, 0, s>>>(d, c);
+            k_rb_scatter<<<gN, 256, 0, s>>>(d, c);
+            k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
+            RF_CUDA(cudaLaunchKernel(ff, dim3(e->nblocks), dim3(128), args, 0, s));
+            k_fire_update<<<e->nblocks, 128, 0, s>>>(d, c);
+        }
+        RF_CHECK_LAUNCH("engine stream FIRE");
+        uint32_t stop = 0;
+        RF_CUDA(cudaMemcpyAsync(&stop, &e->d.sc->fstop, sizeof(stop), cudaMemcpyDeviceToHost, s));
+        RF_CUDA(cudaStreamSynchronize(s));
+        if (stop) break;
+    }
     return RF_OK;
 }
 
@@ -1346,6 +1742,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     e->task = *t;
     e->graph = nullptr; e->exec = nullptr; e->graph_ok = false; e->staging = nullptr; e->bonds_initial = 0;
     e->stream = nullptr; e->counters_dev = nullptr; e->maxq_dev = nullptr;
+    e->fgraph = nullptr; e->fexec = nullptr; e->fire_ready = false;
     cudaGetDevice(&e->device);
     rf_status st = RF_OK;
     auto fail = [&](rf_status s) { rf_engine_destroy(e); return s; };
@@ -1578,11 +1975,107 @@ rf_status rf_engine_positions_f64(rf_engine* e, double* R) {
     return RF_OK;
 }
 
+rf_status rf_relax_default_params(rf_relax_params* p, const rf_task* t) {
+    if (!p || !t) { set_error("rf_relax_default_params: bad arguments"); return RF_ERR_INVALID; }
+    std::memset(p, 0, sizeof(*p));
+    p->strain_inc = 2.5e-5;
+    p->tol = 1e-6;
+    p->dt0 = 0.1;
+    p->dt_max = 1.0;
+    p->dt_min = 1e-3;
+    p->alpha0 = 0.1;
+    p->f_inc = 1.1;
+    p->f_dec = 0.5;
+    p->f_alpha = 0.99;
+    p->n_delay = 5;
+    p->max_iter = 200000;
+    return RF_OK;
+}
+
+rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const float* warm, rf_relax_result* r) {
+    if (!e || !p) { set_error("rf_engine_load_increment: bad arguments"); return RF_ERR_INVALID; }
+    if (!e->c.ext) { set_error("rf_engine_load_increment: quasi-static relaxation needs the extended model"); return RF_ERR_STATE; }
+    if (!(p->dt0 > 0) || !(p->dt_max >= p->dt0) || !(p->dt_min > 0) || !(p->dt_min <= p->dt0) || !(p->tol > 0) ||
+        p->max_iter == 0 || !(p->alpha0 >= 0 && p->alpha0 < 1) || !(p->f_inc >= 1) || !(p->f_dec > 0 && p->f_dec < 1)) {
+        set_error("rf_engine_load_increment: bad FIRE parameters");
+        return RF_ERR_INVALID;
+    }
+    cudaStream_t s = e->stream;
+    Dev& d = e->d;
+    const uint32_t N = e->c.N;
+    if (!e->fire_ready) {
+        rf_status st;
+        if ((st = dalloc(e, &d.frc, N)) || (st = dalloc(e, &d.mom, N)) ||
+            (st = dalloc(e, &d.fpart, (size_t)e->nblocks * FIRE_SUMS)) || (st = dalloc(e, &d.rot, N)) ||
+            (st = dalloc(e, &d.x0, N)))
+            return st;
+        e->cf = e->c;
+        if (!getenv("RF_ENGINE_NO_GRAPH")) {
+            if (build_fire_graph(e) != RF_OK) { cudaGetLastError(); e->cf.use_graph = 0; }
+        } else {
+            e->cf.use_graph = 0;
+        }
+        e->fire_ready = true;
+    }
+    // FIRE constants into the scalar block (host read-modify-write, stream ordered)
+    DevScalars h;
+    RF_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    h.fdt0 = p->dt0; h.fdtmax = p->dt_max; h.fdtmin = p->dt_min; h.falpha0 = p->alpha0; h.finc = p->f_inc;
+    h.fdec = p->f_dec; h.fshrink = p->f_alpha; h.fndelay = p->n_delay; h.ftol = p->tol; h.fmax_iter = p->max_iter;
+    RF_CUDA(cudaMemcpyAsync(d.sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
+    const double delta = p->strain_inc * h.Size0;
+    if (e->task.kind == RF_TEST_BRAZIL) {
+        k_qs_begin_scalars<RF_TEST_BRAZIL><<<1, 32, 0, s>>>(d, e->cf, delta);
+        k_qs_begin<RF_TEST_BRAZIL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm);
+    } else {
+        k_qs_begin_scalars<RF_TEST_UNIAXIAL><<<1, 32, 0, s>>>(d, e->cf, delta);
+        k_qs_begin<RF_TEST_UNIAXIAL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm);
+    }
+    RF_CHECK_LAUNCH("k_qs_begin");
+    if (e->cf.use_graph) RF_CUDA(cudaGraphLaunch(e->fexec, s));
+    else if (rf_status st = launch_stream_fire(e, p->max_iter)) return st;
+    RF_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    if (r) {
+        r->iterations = h.fiter;
+        r->converged = (int32_t)h.fconverged;
+        r->residual = h.fresidual;
+        r->mean_force = h.fmean;
+        r->stress = h.Stress;
+        r->strain = h.Strain;
+        r->broken_bonds = h.broken;
+        r->error = (rf_status)h.err;
+    }
+    return RF_OK;
+}
+
+rf_status rf_engine_increment_fields(rf_engine* e, double* x0, double* dx, double* rot) {
+    if (!e || !e->fire_ready) { set_error("rf_engine_increment_fields: no load increment run yet"); return RF_ERR_STATE; }
+    const uint32_t N = e->c.N;
+    cudaStream_t s = e->stream;
+    DevScalars h;
+    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    std::vector<double4> a(N), b(N), c(N);
+    RF_CUDA(cudaMemcpy(a.data(), e->d.x0, N * sizeof(double4), cudaMemcpyDeviceToHost));
+    RF_CUDA(cudaMemcpy(b.data(), e->d.posd[h.steps & 1ull], N * sizeof(double4), cudaMemcpyDeviceToHost));
+    RF_CUDA(cudaMemcpy(c.data(), e->d.rot, N * sizeof(double4), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < N; ++i) {
+        if (x0) { x0[3 * i] = a[i].x; x0[3 * i + 1] = a[i].y; x0[3 * i + 2] = a[i].z; }
+        if (dx) { dx[3 * i] = b[i].x - a[i].x; dx[3 * i + 1] = b[i].y - a[i].y; dx[3 * i + 2] = b[i].z - a[i].z; }
+        if (rot) { rot[3 * i] = c[i].x; rot[3 * i + 1] = c[i].y; rot[3 * i + 2] = c[i].z; }
+    }
+    return RF_OK;
+}
+
 rf_status rf_engine_destroy(rf_engine* e) {
     if (!e) return RF_OK;
     if (e->stream) cudaStreamSynchronize(e->stream);
     if (e->exec) cudaGraphExecDestroy(e->exec);
     if (e->graph) cudaGraphDestroy(e->graph);
+    if (e->fexec) cudaGraphExecDestroy(e->fexec);
+    if (e->fgraph) cudaGraphDestroy(e->fgraph);
     for (void* p : e->allocs) cudaFree(p);
     if (e->staging) cudaFree(e->staging);
     if (e->stream) cudaStreamDestroy(e->stream);

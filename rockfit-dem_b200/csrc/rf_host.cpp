@@ -222,6 +222,51 @@ rf_status md_SumForcesULoading(rf_task* t, const float* h_FL, uint64_t nblocks, 
     return RF_OK;
 }
 
+rf_status md_SetFIREData(rf_fire* f, uint_fast32_t N, const rf_potential* Po) {
+    if (!f || !Po) { set_error("md_SetFIREData: bad arguments"); return RF_ERR_INVALID; }
+    std::memset(f, 0, sizeof(*f));
+    f->bloks4 = N / (4 * 256) + 1;          // SMEMDIM = 256
+    f->dt0 = (float)Po->dt;
+    f->dtmax = (float)(100.0 * (double)f->dt0);
+    f->dtmin = (float)(0.001 * (double)f->dt0);
+    f->dtgrow = 1.1f;
+    f->dtshrink = 0.5f;
+    f->alpha0 = 0.25f;
+    f->alphashrink = 0.99f;
+    f->NPnegativeMax = 30000;
+    f->Ndelay = 20;
+    f->NPpositive = 0;
+    f->NPnegative = 0;
+    f->dt = f->dt0;
+    f->alpha = f->alpha0;
+    return RF_OK;
+}
+
+rf_status md_FireDecide(rf_fire* f, double FdotV, uint64_t step, int* half_step, int* stop) {
+    if (!f || !half_step || !stop) { set_error("md_FireDecide: bad arguments"); return RF_ERR_INVALID; }
+    f->FdotV = FdotV;
+    *half_step = 0;
+    *stop = 0;
+    if (FdotV > 0) {
+        ++f->NPpositive;
+        f->NPnegative = 0;
+        if (f->NPpositive > f->Ndelay) {
+            f->dt = (f->dt * f->dtgrow < f->dtmax) ? f->dt * f->dtgrow : f->dtmax;
+            f->alpha *= f->alphashrink;
+        }
+    } else {
+        f->NPpositive = 0;
+        ++f->NPnegative;
+        if (f->NPnegative > f->NPnegativeMax) { *stop = 1; return RF_OK; }
+        if (step > f->Ndelay) {
+            f->dt = (f->dt * f->dtshrink > f->dtmin) ? f->dt * f->dtshrink : f->dtmin;
+            f->alpha = f->alpha0;
+        }
+        *half_step = 1;
+    }
+    return RF_OK;
+}
+
 static rf_status run_test(rf_task* t, const float* h_R, uint64_t max_steps, double* curve, uint64_t curve_cap,
                           float* h_R_out, rf_run_result* result) {
     if (!t || !h_R) { set_error("md_Calculation*: bad arguments"); return RF_ERR_INVALID; }

@@ -350,17 +350,21 @@ struct ExtParams {
 // rlen = |r| in double; r is the float rounding of the double separation.
 __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt& b, const f3 r, const double rlen,
                                               const f3 vi, const f3 vj, const f3 wi, const f3 wj, f3& Rij, f3& Oijt,
-                                              f3& Mijn, f3& Mijt, f3& fs, f3& ms) {
+                                              f3& Mijn, f3& Mijt, f3& fs, f3& ms, float& fnabs, float& kt,
+                                              float& kr) {
     const float rijm = (float)rlen;
     const float inv_rm = __frcp_rn(rijm);
     const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
-    const float il = (float)(1.0 / b.L0);
-    const float stretch = (float)(rlen - b.L0);
+    const float stretch = (float)(rlen - b.L0);     // in double: no cancellation at small strains
     const float A = b.br * b.br * RF_PI_F;
     const float J = RF_PI_F * b.br * b.br * b.br * b.br;
+    // translational and rotational stiffness of the bond (FIRE mass scaling)
+    kt += (b.kn + b.ks) * A;
+    kr += 0.25f * b.kn * J + 0.5f * b.ks * J + 0.25f * b.ks * A * rijm * rijm;
     float cef = b.kn * stretch;
     float Sc = cef;
     cef *= A;
+    fnabs += fabsf(cef);
     fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
     const float tx = Rij.y * nz - Rij.z * ny;
     const float ty = Rij.z * nx - Rij.x * nz;
@@ -397,8 +401,9 @@ __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt&
         const float my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
         const float mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
         Mijt = mk3(mx, my, mz);
-        c2 *= J;
-        ms.x += mx * c2; ms.y += my * c2; ms.z += mz * c2;
+        // bending moment kn * (pi br^4 / 4) * angle = Mijt * J; the reference's extra
+        // factor dt*E/(4 L0) here (its Q1) is not carried into this model
+        ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
     }
     float Mc;
     {
@@ -420,7 +425,6 @@ __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt&
         ms.y += 0.5f * (r.z * ox - r.x * oz) * c;
         ms.z += 0.5f * (r.x * oy - r.y * ox) * c;
     }
-    (void)il;
     Mc *= norm3(Oijt.x, Oijt.y, Oijt.z);
     Sc += norm3(Mijt.x, Mijt.y, Mijt.z) * 4.0f * b.br;
     Mc += norm3(Mijn.x, Mijn.y, Mijn.z) * 2.0f * b.br;
@@ -433,18 +437,22 @@ __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt&
     return false;
 }
 
-// Overlapping pair of the extended model (rlen < ri + rj). mi, mj are the masses.
-__device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r, const float rijm, const float ri,
-                                                 const float rj, const float mi, const float mj, const f3 vi,
-                                                 const f3 vj, const f3 wi, const f3 wj, f3& Oijt, f3& fs, f3& ms) {
+// Overlapping pair of the extended model. delta = r_i + r_j - |r| is formed in double
+// by the caller (in float it would cancel to a few significant bits at small overlaps);
+// mi, mj are the masses.
+__device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r, const float rijm, const float delta,
+                                                 const float ri, const float rj, const float mi, const float mj,
+                                                 const f3 vi, const f3 vj, const f3 wi, const f3 wj, f3& Oijt, f3& fs,
+                                                 f3& ms, float& fnabs, float& kt, float& kr) {
     const float inv_rm = __frcp_rn(rijm);
     const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
     const float Rs = ri * rj / (ri + rj);               // equivalent radius (rP/2 for equal sizes)
     const float ms_ = mi * mj / (mi + mj);             // equivalent mass (mP/2 for equal masses)
-    const float delta = ri + rj - rijm;
     float c1 = __fsqrt_rn(Rs * fabsf(delta));
     const float Kn = 2.0f * p.hm_E * c1;
     const float Kt = 8.0f * p.hm_G * c1;
+    kt += Kn + Kt;                                      // contact stiffness (FIRE mass scaling)
+    kr += Kt * ri * ri;
     // relative velocity of the contact point: vj - vi + n x (ri wi + rj wj)
     const float ax = ri * wi.x + rj * wj.x, ay = ri * wi.y + rj * wj.y, az = ri * wi.z + rj * wj.z;
     const float vx = vj.x - vi.x + (ny * az - nz * ay);
@@ -452,6 +460,7 @@ __device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r,
     const float vz = vj.z - vi.z + (nx * ay - ny * ax);
     const float vn = nx * vx + ny * vy + nz * vz;
     const float fn = -delta * Kn * RF_2D3_F;
+    fnabs += fabsf(fn);
     c1 = -1.8257f * p.p_A * vn * __fsqrt_rn(Kn * ms_);
     fs.x += nx * (fn + c1); fs.y += ny * (fn + c1); fs.z += nz * (fn + c1);
     const float vtx = vx - nx * vn, vty = vy - ny * vn, vtz = vz - nz * vn;
@@ -482,12 +491,14 @@ __device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r,
     ms.x += (ny * ftz - nz * fty) * ri;
     ms.y += (nz * ftx - nx * ftz) * ri;
     ms.z += (nx * fty - ny * ftx) * ri;
-    const float wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
-    if ((double)wim > 1e-18) {
-        const float cr = -p.mur * fabsf(fn) * __frsqrt_rn(wim);
-        ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
-    } else {
-        ms = mk3(0.f, 0.f, 0.f);
+    if (p.mur != 0.f) {           // rolling resistance, with the reference's zero-spin clear
+        const float wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
+        if ((double)wim > 1e-18) {
+            const float cr = -p.mur * fabsf(fn) * __frsqrt_rn(wim);
+            ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
+        } else {
+            ms = mk3(0.f, 0.f, 0.f);
+        }
     }
 }
 

@@ -91,10 +91,30 @@ class RunResult(C.Structure):
                 ("broken_bonds", C.c_uint64), ("bonds_initial", C.c_uint64), ("error", C.c_int)]
 
 
+class Fire(C.Structure):
+    """rf_fire: firerelax_data without its buffers."""
+    _fields_ = [(n, C.c_uint64) for n in ("bloks4", "NPpositiveMax", "NPnegativeMax", "NPpositive", "NPnegative",
+                                          "Ndelay", "MaxStepsRelaxation")] + \
+               [(n, C.c_float) for n in ("dtmax", "dtmin", "dt0", "dt", "alpha0", "alpha", "dtgrow", "dtshrink",
+                                         "alphashrink")] + [("FdotV", C.c_double)]
+
+
 class ExtParams(C.Structure):
     """rf_ext_params: bond constants and strength distribution of the extended model."""
     _fields_ = [("kn", C.c_double), ("ks", C.c_double), ("bond_lambda", C.c_double), ("gap_frac", C.c_double),
                 ("weibull_m", C.c_double), ("sigma_c", C.c_double), ("tau_c", C.c_double), ("seed", C.c_uint64)]
+
+
+class RelaxParams(C.Structure):
+    _fields_ = [("strain_inc", C.c_double), ("tol", C.c_double), ("dt0", C.c_double), ("dt_max", C.c_double),
+                ("dt_min", C.c_double), ("alpha0", C.c_double), ("f_inc", C.c_double), ("f_dec", C.c_double),
+                ("f_alpha", C.c_double), ("n_delay", C.c_uint32), ("max_iter", C.c_uint64)]
+
+
+class RelaxResult(C.Structure):
+    _fields_ = [("iterations", C.c_uint64), ("converged", C.c_int32), ("residual", C.c_double),
+                ("mean_force", C.c_double), ("stress", C.c_double), ("strain", C.c_double),
+                ("broken_bonds", C.c_uint64), ("error", C.c_int)]
 
 
 # --- prototypes ---------------------------------------------------------------
@@ -126,6 +146,8 @@ _proto = {
     "md_CalculateIncrementsFIRE": (i32, [P, P, P, ID, f32, f32, f32, P]),
     "md_CalculateDecrementsHalfStepFIRE": (i32, [P, P, ID, f32, P]),
     "md_FdotVEntire": (i32, [P, P, P, u64, ID, P]),
+    "md_SetFIREData": (i32, [C.POINTER(Fire), ID, C.POINTER(Potential)]),
+    "md_FireDecide": (i32, [C.POINTER(Fire), f64, u64, C.POINTER(i32), C.POINTER(i32)]),
     "md_CalculationBrazilTest": (i32, [C.POINTER(Task), P, u64, P, u64, P, C.POINTER(RunResult)]),
     "md_CalculationUniaxialCompression": (i32, [C.POINTER(Task), P, u64, P, u64, P, C.POINTER(RunResult)]),
     "rf_engine_create": (i32, [C.POINTER(Task), P, C.POINTER(P)]),
@@ -142,6 +164,9 @@ _proto = {
     "rf_engine_uses_graph": (i32, [P]),
     "rf_engine_create_ext": (i32, [C.POINTER(Task), C.POINTER(ExtParams), P, P, C.POINTER(P)]),
     "rf_engine_positions_f64": (i32, [P, P]),
+    "rf_relax_default_params": (i32, [C.POINTER(RelaxParams), C.POINTER(Task)]),
+    "rf_engine_load_increment": (i32, [P, C.POINTER(RelaxParams), P, C.POINTER(RelaxResult)]),
+    "rf_engine_increment_fields": (i32, [P, P, P, P]),
     "rf_pack_cylinder": (i32, [u64, u64, f64, f64, f64, f64, f64, P, P, P, P, P, P]),
     "rf_specimen_lattice_cylinder": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
     "rf_specimen_lattice_disc": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
@@ -325,6 +350,25 @@ class Engine:
             assert R.size == 3 * self.N
             check(lib.rf_engine_create(C.byref(task), R.ctypes.data, C.byref(h)), "rf_engine_create")
         self.h = h
+
+    def relax_params(self, **kw):
+        p = RelaxParams()
+        check(lib.rf_relax_default_params(C.byref(p), C.byref(self.task)), "rf_relax_default_params")
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+    def load_increment(self, params, warm=None):
+        """One quasi-static load increment; warm: device tensor float32 [N, 6] or None."""
+        r = RelaxResult()
+        check(lib.rf_engine_load_increment(self.h, C.byref(params), ptr(warm), C.byref(r)), "rf_engine_load_increment")
+        return r
+
+    def increment_fields(self):
+        x0, dx, rot = (np.zeros((self.N, 3), np.float64) for _ in range(3))
+        check(lib.rf_engine_increment_fields(self.h, x0.ctypes.data, dx.ctypes.data, rot.ctypes.data),
+              "rf_engine_increment_fields")
+        return x0, dx, rot
 
     def positions_f64(self):
         R = np.zeros(3 * self.N, np.float64)

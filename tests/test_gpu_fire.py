@@ -1,0 +1,66 @@
+"""Quasi-static FIRE load increments of the extended model on the GPU: against the
+oracle's restatement of the same relaxation (float forces, and the FP64 oracle), and
+the warm-start path with an exact predictor."""
+import numpy as np
+import pytest
+
+import extspec
+import mdcall as mc
+import oracle
+import rfdem
+
+pytestmark = pytest.mark.gpu
+
+
+def test_fire_increments_vs_oracle(cuda):
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
+    e = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    p = e.relax_params(max_iter=20000)
+    n = 5
+    res = [e.load_increment(p) for _ in range(n)]
+    Re = e.positions_f64()
+    e.close()
+    assert all(r.converged == 1 and r.residual <= p.tol and r.error == 0 for r in res)
+    of = oracle.qs_ext(mc.clone(t), x, R, rad, p, n)
+    od = oracle.qs_ext(mc.clone(t), x, R, rad, p, n, fp64=True)
+    assert np.all(of["converged"] == 1) and np.all(od["converged"] == 1)
+    ext = float(np.ptp(R))
+    # same relaxation in the same arithmetic up to the order of the FP64 sums
+    assert np.max(np.abs(Re - of["R"])) < 1e-7 * ext
+    # against the FP64 oracle: relaxed positions and platen stress of the loaded increment
+    assert np.max(np.abs(Re - od["R"])) < 1e-6 * ext
+    s_e, s_d = res[-1].stress, od["stress"][-1]
+    assert s_d > 0 and abs(s_e - s_d) <= 5e-3 * s_d, (s_e, s_d)
+    # iteration counts agree closely (the decision sequence is the same but for rounding)
+    it_e = np.array([r.iterations for r in res], float)
+    assert np.all(np.abs(it_e - of["iters"]) <= 0.05 * of["iters"] + 5)
+
+
+def test_fire_exact_warm_start_cuts_iterations(cuda):
+    """Warm start with the relaxed answer of the same increment (two engines in lockstep)."""
+    import torch
+    N, r0 = 4000, 0.25
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, r0, aspect=2.0, phi=0.58, seed=0xB2000000 + 77)
+    x = extspec.stiff_params()
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, r0, min_stress=1e3)
+    A = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    B = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    p = A.relax_params(max_iter=60000)
+    loaded = 0
+    for k in range(30):                      # until the platen carries load
+        a, b = A.load_increment(p), B.load_increment(p)
+        assert a.iterations == b.iterations and a.stress == b.stress
+        if a.stress > 1e-7 and a.converged:
+            loaded += 1
+        if loaded >= 2:
+            break
+    assert loaded >= 2
+    a = A.load_increment(p)
+    _, dx, rot = A.increment_fields()
+    warm = torch.from_numpy(np.concatenate([dx, rot], 1).astype(np.float32)).cuda()
+    b = B.load_increment(p, warm)
+    print("plain %d iterations, exact warm start %d" % (a.iterations, b.iterations))
+    assert a.converged == 1 and b.converged == 1
+    assert b.iterations * 2 < a.iterations
+    assert abs(b.stress - a.stress) <= 1e-3 * a.stress
+    A.close(); B.close()

@@ -468,6 +468,31 @@ rf_status rf_pack_cylinder(uint64_t seed, uint64_t N, double r0, double rmin, do
                            double phi, const double center[3], double* R, double* radius,
                            double* diameter, double* height, double* max_overlap);
 
+/* ------------------------------------------------------------------------ */
+/* BF16 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory) and the */
+/* warm-start MLP. No reference counterpart.                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Epilogues of rf_gemm_bf16. */
+typedef enum rf_gemm_epilogue {
+    RF_EPI_RELU_BF16 = 0,   /* out_h = bf16(relu(acc + bias)), out_ht = its transpose (optional) */
+    RF_EPI_LINEAR_F32 = 1,  /* out_f = (acc + bias) * scale, first ncols_f columns */
+    RF_EPI_MASK_BF16 = 2,   /* out_h = bf16(mask > 0 ? acc : 0) (+ transpose): ReLU backward */
+    RF_EPI_ATOMIC_F32 = 3   /* out_f += scale * acc (split-K over `splits` CTAs) */
+} rf_gemm_epilogue;
+/*
+ * C[M x N] = A[M x K] * B[N x K]^T on the device. A, B: bf16, row-major with K
+ * contiguous (leading dimensions lda, ldb in elements, multiples of 8; 16-byte aligned
+ * bases); N a multiple of 16 up to 256; K a multiple of 8. bias: float[N] or NULL;
+ * mask: bf16 [M x ldm]. Outputs as the epilogue says; out_ht is [N x ld_ht] (ld_ht >= M).
+ * Asynchronous on `stream`; rf_gemm_status reports a tensor-core wait that timed out.
+ */
+rf_status rf_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int N, int K, int mode,
+                       const float* bias, const void* mask, int ldm, void* out_h, int ld_h, void* out_ht,
+                       int ld_ht, float* out_f, int ld_f, int ncols_f, float scale, int splits,
+                       rf_stream stream);
+rf_status rf_gemm_status(rf_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

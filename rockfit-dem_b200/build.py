@@ -18,7 +18,7 @@ LIB = os.path.join(LIB_DIR, "librfdem.so")
 INCLUDE = os.path.join(HERE, "..", "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CU_SOURCES = ["rf_md_kernels.cu", "rf_engine.cu", "rf_pack.cu"]
+CU_SOURCES = ["rf_md_kernels.cu", "rf_engine.cu", "rf_pack.cu", "rf_mlp.cu"]
 CXX_SOURCES = ["rf_host.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",

@@ -91,6 +91,9 @@ class RunResult(C.Structure):
                 ("broken_bonds", C.c_uint64), ("bonds_initial", C.c_uint64), ("error", C.c_int)]
 
 
+RF_EPI_RELU_BF16, RF_EPI_LINEAR_F32, RF_EPI_MASK_BF16, RF_EPI_ATOMIC_F32 = 0, 1, 2, 3
+
+
 class Fire(C.Structure):
     """rf_fire: firerelax_data without its buffers."""
     _fields_ = [(n, C.c_uint64) for n in ("bloks4", "NPpositiveMax", "NPnegativeMax", "NPpositive", "NPnegative",
@@ -168,6 +171,8 @@ _proto = {
     "rf_engine_load_increment": (i32, [P, C.POINTER(RelaxParams), P, C.POINTER(RelaxResult)]),
     "rf_engine_increment_fields": (i32, [P, P, P, P]),
     "rf_pack_cylinder": (i32, [u64, u64, f64, f64, f64, f64, f64, P, P, P, P, P, P]),
+    "rf_gemm_bf16": (i32, [P, i32, P, i32, i32, i32, i32, i32, P, P, i32, P, i32, P, i32, P, i32, i32, f32, i32, P]),
+    "rf_gemm_status": (i32, [P]),
     "rf_specimen_lattice_cylinder": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
     "rf_specimen_lattice_disc": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
 }

@@ -395,6 +395,24 @@ rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const
 /* The last increment's start positions, relaxed displacement and accumulated rotation,
    each double[N][3] (host; any may be NULL): training pairs for the warm start. */
 rf_status rf_engine_increment_fields(rf_engine* e, double* x0, double* dx, double* rot);
+
+/*
+ * Warm-start features and targets (device buffers). Features of each particle for the
+ * next increment of size strain_inc, from the last increment's motion: bf16 [rows][64],
+ * rows = N rounded up to 128 (padding rows zero). With D = strain_inc * initial size:
+ *   0-2 displacement / D; 3-5 rotation * r / D; 6 position along the load axis and
+ *   7 distance from it, both relative to the specimen's half sizes; 8-55 up to 12
+ *   intact bonds in record order: the partner's displacement minus this one's / D
+ *   (3) and the bond strain / strain_inc (1); 56 intact bonds / 12; 57 at a platen;
+ *   58 one; 59-63 zero.
+ * Targets of the last increment, fp32 [N][6]: displacement / D, rotation * r / D.
+ */
+rf_status rf_engine_warm_features(rf_engine* e, double strain_inc, void* feat);
+rf_status rf_engine_warm_targets(rf_engine* e, double strain_inc, float* targets);
+/* rf_engine_load_increment with the MLP's output: pred[i * ldp + 0..5] in the units of
+   the targets (scaled back to a displacement and rotation before the increment). */
+rf_status rf_engine_load_increment_pred(rf_engine* e, const rf_relax_params* p, const float* pred, int ldp,
+                                        rf_relax_result* r);
 rf_status rf_engine_destroy(rf_engine* e);
 
 /* Advance nsteps explicit steps (stops early, on device, at fracture / max strain). */
@@ -492,6 +510,30 @@ rf_status rf_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, in
                        int ld_ht, float* out_f, int ld_f, int ncols_f, float scale, int splits,
                        rf_stream stream);
 rf_status rf_gemm_status(rf_stream stream);
+
+/*
+ * Warm-start MLP (per particle): 64 features -> 128 -> 128 -> 128 -> 6, ReLU, BF16
+ * weights and activations, FP32 accumulation on the tensor cores, FP32 master weights
+ * trained with Adam on mean((y - t)^2). Layer l's weights W[l] are [out][in] (the last
+ * layer stored as 16 x 128, rows 6..15 zero).
+ */
+typedef struct rf_mlp rf_mlp;
+rf_status rf_mlp_create(uint64_t seed, rf_mlp** out);
+rf_status rf_mlp_destroy(rf_mlp* m);
+rf_stream rf_mlp_stream(rf_mlp* m);
+/* Y[rows][ldy] (first ncols <= 16 outputs, fp32, device) from X (bf16 [rows][64], device). */
+rf_status rf_mlp_forward(rf_mlp* m, const void* X, int rows, float* Y, int ldy, int ncols);
+/* One training step on X (bf16 [rows][64]) and targets T (fp32 [rows][6]), both on the
+   device: loss before the step into *loss; an Adam step with rate lr when lr > 0. */
+rf_status rf_mlp_train_step(rf_mlp* m, const void* X, const float* T, int rows, float lr, double* loss);
+/* Residual mode: outputs are x[0:6] + network(x), i.e. the network learns the correction
+   to the last increment's motion (features 0-5). Off by default. */
+rf_status rf_mlp_set_residual(rf_mlp* m, int on);
+/* Host copies of layer `layer`'s fp32 weights / bias, and of the last step's gradients
+   (gT is [in][out]). */
+rf_status rf_mlp_get(rf_mlp* m, int layer, float* W, float* b);
+rf_status rf_mlp_set(rf_mlp* m, int layer, const float* W, const float* b);
+rf_status rf_mlp_grad(rf_mlp* m, int layer, float* gT, float* gb);
 
 #ifdef __cplusplus
 }

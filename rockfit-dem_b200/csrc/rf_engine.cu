@@ -33,6 +33,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <cuda_bf16.h>
 #include "rf_physics.cuh"
 
 #ifndef RF_STEP_MIN_BLOCKS
@@ -1191,7 +1192,7 @@ __global__ void k_qs_begin_scalars(Dev d, Consts c, double delta) {
     }
 }
 template <int KIND>
-__global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm) {
+__global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int ldw, int scaled, double D) {
     DevScalars* sc = d.sc;
     const uint32_t cur = (uint32_t)(sc->steps & 1ull);
     const float idt0 = (float)(1.0 / sc->fdt0);
@@ -1209,11 +1210,17 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm) {
             // predicted displacement and rotation; as velocities over dt0 they make the first
             // force pass advance the bond and contact state by exactly that motion (the
             // first update then starts from rest)
-            const float* q = warm + (size_t)i * 6;
-            x.x += (double)q[0]; x.y += (double)q[1]; x.z += (double)q[2];
-            v0 = q[0] * idt0; v1 = q[1] * idt0; v2 = q[2] * idt0;
-            w = make_float4(q[3] * idt0, q[4] * idt0, q[5] * idt0, 0.f);
-            rot = make_double4(q[3], q[4], q[5], 0.0);
+            const float* q = warm + (size_t)i * ldw;
+            float u[6];
+            for (int a = 0; a < 6; ++a) u[a] = q[a];
+            if (scaled) {                   // MLP units: displacement / D, rotation * r / D
+                const float sd = (float)D, sr = (float)(D / x.w);
+                u[0] *= sd; u[1] *= sd; u[2] *= sd; u[3] *= sr; u[4] *= sr; u[5] *= sr;
+            }
+            x.x += (double)u[0]; x.y += (double)u[1]; x.z += (double)u[2];
+            v0 = u[0] * idt0; v1 = u[1] * idt0; v2 = u[2] * idt0;
+            w = make_float4(u[3] * idt0, u[4] * idt0, u[5] * idt0, 0.f);
+            rot = make_double4(u[3], u[4], u[5], 0.0);
         }
         // the platen pushes the particles it passed: clamp them now, so the first force
         // pass (and its convergence test) sees the loaded configuration
@@ -1229,6 +1236,83 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm) {
         d.vel[cur][i] = make_float4(v0, v1, v2, 0.f);
         d.ang[cur][i] = w;
         d.rot[i] = rot;
+    }
+}
+
+// Warm-start features of each particle from the last increment's motion (layout in the
+// header); D = strain_inc * initial size, sinc = strain_inc.
+template <int KIND>
+__global__ void k_warm_features(Dev d, Consts c, double D, double sinc, __nv_bfloat16* __restrict__ feat) {
+    const DevScalars* sc = d.sc;
+    const uint32_t cur = (uint32_t)(sc->steps & 1ull);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+    const double iD = 1.0 / D;
+    const double4 x = d.posd[cur][i], x0 = d.x0[i], r = d.rot[i];
+    float f[64];
+#pragma unroll
+    for (int q = 0; q < 64; ++q) f[q] = 0.f;
+    const double dxi = x.x - x0.x, dyi = x.y - x0.y, dzi = x.z - x0.z;
+    f[0] = (float)(dxi * iD); f[1] = (float)(dyi * iD); f[2] = (float)(dzi * iD);
+    f[3] = (float)(r.x * x.w * iD); f[4] = (float)(r.y * x.w * iD); f[5] = (float)(r.z * x.w * iD);
+    const double p[3] = {x.x - sc->center_d[0], x.y - sc->center_d[1], x.z - sc->center_d[2]};
+    f[6] = (float)(p[ax] / (0.5 * sc->size_d[ax]));
+    const double o0 = p[ax == 2 ? 0 : 0], o1 = p[ax == 2 ? 1 : 2];
+    f[7] = (float)(sqrt(o0 * o0 + o1 * o1) / (0.5 * sc->size_d[0]));
+    const size_t QN = (size_t)d.QB * c.N;
+    (void)QN;
+    const uint32_t bm = d.bmask[i], nq = d.nbq[i];
+    int nb = 0;
+    for (uint32_t q = 0; q < nq && nb < 12; ++q) {
+        if (!((bm >> q) & 1u)) continue;
+        const size_t s = (size_t)q * c.N + i;
+        const uint32_t j = d.bj[s];
+        const double4 xj = d.posd[cur][j], xj0 = d.x0[j];
+        const double ex = (xj.x - xj0.x) - dxi, ey = (xj.y - xj0.y) - dyi, ez = (xj.z - xj0.z) - dzi;
+        const double rx = xj.x - x.x, ry = xj.y - x.y, rz = xj.z - x.z;
+        const double L0 = d.bL0[s];
+        float* g = f + 8 + 4 * nb;
+        g[0] = (float)(ex * iD); g[1] = (float)(ey * iD); g[2] = (float)(ez * iD);
+        g[3] = (float)((sqrt(rx * rx + ry * ry + rz * rz) - L0) / (L0 * sinc));
+        ++nb;
+    }
+    f[56] = (float)nb * (1.0f / 12.0f);
+    const double xa = ax == 1 ? x.y : x.z;
+    f[57] = (xa - sc->Top > -1e-9 || xa - sc->Bottom < 1e-9) ? 1.f : 0.f;
+    f[58] = 1.f;
+    uint4* out = reinterpret_cast<uint4*>(feat + (size_t)i * 64);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        __nv_bfloat162 h0 = __floats2bfloat162_rn(f[8 * q + 0], f[8 * q + 1]);
+        __nv_bfloat162 h1 = __floats2bfloat162_rn(f[8 * q + 2], f[8 * q + 3]);
+        __nv_bfloat162 h2 = __floats2bfloat162_rn(f[8 * q + 4], f[8 * q + 5]);
+        __nv_bfloat162 h3 = __floats2bfloat162_rn(f[8 * q + 6], f[8 * q + 7]);
+        uint4 u;
+        u.x = *reinterpret_cast<uint32_t*>(&h0); u.y = *reinterpret_cast<uint32_t*>(&h1);
+        u.z = *reinterpret_cast<uint32_t*>(&h2); u.w = *reinterpret_cast<uint32_t*>(&h3);
+        out[q] = u;
+    }
+}
+
+// Targets of the last increment: displacement / D and rotation * r / D.
+__global__ void k_warm_targets(Dev d, Consts c, double D, float* __restrict__ t) {
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const double iD = 1.0 / D;
+    const double4 x = d.posd[cur][i], x0 = d.x0[i], r = d.rot[i];
+    float* o = t + (size_t)i * 6;
+    o[0] = (float)((x.x - x0.x) * iD); o[1] = (float)((x.y - x0.y) * iD); o[2] = (float)((x.z - x0.z) * iD);
+    o[3] = (float)(r.x * x.w * iD); o[4] = (float)(r.y * x.w * iD); o[5] = (float)(r.z * x.w * iD);
+}
+
+// Start positions of the first increment: x0 = x, no rotation.
+__global__ void k_fire_buffers_init(Dev d, Consts c) {
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        d.x0[i] = d.posd[cur][i];
+        d.rot[i] = make_double4(0.0, 0.0, 0.0, 0.0);
     }
 }
 
@@ -1992,7 +2076,32 @@ rf_status rf_relax_default_params(rf_relax_params* p, const rf_task* t) {
     return RF_OK;
 }
 
-rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const float* warm, rf_relax_result* r) {
+}  // extern "C"
+
+namespace {
+rf_status fire_setup(rf_engine* e) {
+    if (e->fire_ready) return RF_OK;
+    Dev& d = e->d;
+    const uint32_t N = e->c.N;
+    rf_status st;
+    if ((st = dalloc(e, &d.frc, N)) || (st = dalloc(e, &d.mom, N)) ||
+        (st = dalloc(e, &d.fpart, (size_t)e->nblocks * FIRE_SUMS)) || (st = dalloc(e, &d.rot, N)) ||
+        (st = dalloc(e, &d.x0, N)))
+        return st;
+    e->cf = e->c;
+    if (!getenv("RF_ENGINE_NO_GRAPH")) {
+        if (build_fire_graph(e) != RF_OK) { cudaGetLastError(); e->cf.use_graph = 0; }
+    } else {
+        e->cf.use_graph = 0;
+    }
+    k_fire_buffers_init<<<(N + 255) / 256, 256, 0, e->stream>>>(d, e->cf);
+    RF_CHECK_LAUNCH("k_fire_buffers_init");
+    e->fire_ready = true;
+    return RF_OK;
+}
+
+rf_status load_increment(rf_engine* e, const rf_relax_params* p, const float* warm, int ldw, int scaled,
+                         rf_relax_result* r) {
     if (!e || !p) { set_error("rf_engine_load_increment: bad arguments"); return RF_ERR_INVALID; }
     if (!e->c.ext) { set_error("rf_engine_load_increment: quasi-static relaxation needs the extended model"); return RF_ERR_STATE; }
     if (!(p->dt0 > 0) || !(p->dt_max >= p->dt0) || !(p->dt_min > 0) || !(p->dt_min <= p->dt0) || !(p->tol > 0) ||
@@ -2003,20 +2112,7 @@ rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const
     cudaStream_t s = e->stream;
     Dev& d = e->d;
     const uint32_t N = e->c.N;
-    if (!e->fire_ready) {
-        rf_status st;
-        if ((st = dalloc(e, &d.frc, N)) || (st = dalloc(e, &d.mom, N)) ||
-            (st = dalloc(e, &d.fpart, (size_t)e->nblocks * FIRE_SUMS)) || (st = dalloc(e, &d.rot, N)) ||
-            (st = dalloc(e, &d.x0, N)))
-            return st;
-        e->cf = e->c;
-        if (!getenv("RF_ENGINE_NO_GRAPH")) {
-            if (build_fire_graph(e) != RF_OK) { cudaGetLastError(); e->cf.use_graph = 0; }
-        } else {
-            e->cf.use_graph = 0;
-        }
-        e->fire_ready = true;
-    }
+    if (rf_status st = fire_setup(e)) return st;
     // FIRE constants into the scalar block (host read-modify-write, stream ordered)
     DevScalars h;
     RF_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -2027,10 +2123,10 @@ rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const
     const double delta = p->strain_inc * h.Size0;
     if (e->task.kind == RF_TEST_BRAZIL) {
         k_qs_begin_scalars<RF_TEST_BRAZIL><<<1, 32, 0, s>>>(d, e->cf, delta);
-        k_qs_begin<RF_TEST_BRAZIL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm);
+        k_qs_begin<RF_TEST_BRAZIL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm, ldw, scaled, delta);
     } else {
         k_qs_begin_scalars<RF_TEST_UNIAXIAL><<<1, 32, 0, s>>>(d, e->cf, delta);
-        k_qs_begin<RF_TEST_UNIAXIAL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm);
+        k_qs_begin<RF_TEST_UNIAXIAL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm, ldw, scaled, delta);
     }
     RF_CHECK_LAUNCH("k_qs_begin");
     if (e->cf.use_graph) RF_CUDA(cudaGraphLaunch(e->fexec, s));
@@ -2047,6 +2143,51 @@ rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const
         r->broken_bonds = h.broken;
         r->error = (rf_status)h.err;
     }
+    return RF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const float* warm, rf_relax_result* r) {
+    return load_increment(e, p, warm, 6, 0, r);
+}
+
+rf_status rf_engine_load_increment_pred(rf_engine* e, const rf_relax_params* p, const float* pred, int ldp,
+                                        rf_relax_result* r) {
+    if (!pred || ldp < 6) { set_error("rf_engine_load_increment_pred: bad prediction buffer"); return RF_ERR_INVALID; }
+    return load_increment(e, p, pred, ldp, 1, r);
+}
+
+rf_status rf_engine_warm_features(rf_engine* e, double strain_inc, void* feat) {
+    if (!e || !feat || !(strain_inc > 0)) { set_error("rf_engine_warm_features: bad arguments"); return RF_ERR_INVALID; }
+    if (!e->c.ext) { set_error("rf_engine_warm_features: needs the extended model"); return RF_ERR_STATE; }
+    if (rf_status st = fire_setup(e)) return st;
+    const uint32_t N = e->c.N, rows = (N + 127) / 128 * 128;
+    cudaStream_t s = e->stream;
+    DevScalars h;
+    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    const double D = strain_inc * h.Size0;
+    if (rows > N) RF_CUDA(cudaMemsetAsync((__nv_bfloat16*)feat + (size_t)N * 64, 0, (size_t)(rows - N) * 64 * 2, s));
+    if (e->task.kind == RF_TEST_BRAZIL)
+        k_warm_features<RF_TEST_BRAZIL><<<(N + 127) / 128, 128, 0, s>>>(e->d, e->cf, D, strain_inc, (__nv_bfloat16*)feat);
+    else
+        k_warm_features<RF_TEST_UNIAXIAL><<<(N + 127) / 128, 128, 0, s>>>(e->d, e->cf, D, strain_inc, (__nv_bfloat16*)feat);
+    RF_CHECK_LAUNCH("k_warm_features");
+    return RF_OK;
+}
+
+rf_status rf_engine_warm_targets(rf_engine* e, double strain_inc, float* targets) {
+    if (!e || !targets || !(strain_inc > 0)) { set_error("rf_engine_warm_targets: bad arguments"); return RF_ERR_INVALID; }
+    if (!e->fire_ready) { set_error("rf_engine_warm_targets: no load increment run yet"); return RF_ERR_STATE; }
+    cudaStream_t s = e->stream;
+    DevScalars h;
+    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaStreamSynchronize(s));
+    k_warm_targets<<<(e->c.N + 127) / 128, 128, 0, s>>>(e->d, e->cf, strain_inc * h.Size0, targets);
+    RF_CHECK_LAUNCH("k_warm_targets");
     return RF_OK;
 }
 

@@ -173,6 +173,18 @@ _proto = {
     "rf_pack_cylinder": (i32, [u64, u64, f64, f64, f64, f64, f64, P, P, P, P, P, P]),
     "rf_gemm_bf16": (i32, [P, i32, P, i32, i32, i32, i32, i32, P, P, i32, P, i32, P, i32, P, i32, i32, f32, i32, P]),
     "rf_gemm_status": (i32, [P]),
+    "rf_mlp_create": (i32, [u64, C.POINTER(P)]),
+    "rf_mlp_destroy": (i32, [P]),
+    "rf_mlp_stream": (P, [P]),
+    "rf_mlp_forward": (i32, [P, P, i32, P, i32, i32]),
+    "rf_mlp_train_step": (i32, [P, P, P, i32, f32, C.POINTER(C.c_double)]),
+    "rf_mlp_get": (i32, [P, i32, P, P]),
+    "rf_mlp_set_residual": (i32, [P, i32]),
+    "rf_mlp_set": (i32, [P, i32, P, P]),
+    "rf_mlp_grad": (i32, [P, i32, P, P]),
+    "rf_engine_warm_features": (i32, [P, f64, P]),
+    "rf_engine_warm_targets": (i32, [P, f64, P]),
+    "rf_engine_load_increment_pred": (i32, [P, C.POINTER(RelaxParams), P, i32, C.POINTER(RelaxResult)]),
     "rf_specimen_lattice_cylinder": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
     "rf_specimen_lattice_disc": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
 }
@@ -375,6 +387,19 @@ class Engine:
               "rf_engine_increment_fields")
         return x0, dx, rot
 
+    def warm_features(self, strain_inc, out):
+        """Features for the next increment into a device bf16 tensor [rows, 64]."""
+        check(lib.rf_engine_warm_features(self.h, strain_inc, ptr(out)), "rf_engine_warm_features")
+
+    def warm_targets(self, strain_inc, out):
+        check(lib.rf_engine_warm_targets(self.h, strain_inc, ptr(out)), "rf_engine_warm_targets")
+
+    def load_increment_pred(self, params, pred, ldp=16):
+        r = RelaxResult()
+        check(lib.rf_engine_load_increment_pred(self.h, C.byref(params), ptr(pred), ldp, C.byref(r)),
+              "rf_engine_load_increment_pred")
+        return r
+
     def positions_f64(self):
         R = np.zeros(3 * self.N, np.float64)
         check(lib.rf_engine_positions_f64(self.h, R.ctypes.data), "rf_engine_positions_f64")
@@ -450,3 +475,62 @@ def run_test(task, R, max_steps=0, curve_cap=0, want_positions=False):
     check(fn(C.byref(task), R.ctypes.data, max_steps, curve.ctypes.data if curve_cap else None, curve_cap,
              ptr(Rout), C.byref(res)), "md_Calculation")
     return res, curve[:3 * curve_cap].reshape(-1, 3), Rout
+
+
+MLP_DIN = (64, 128, 128, 128)
+MLP_DOUT = (128, 128, 128, 16)
+
+
+class MLP:
+    """The warm-start MLP (rf_mlp_*) on the current CUDA device."""
+
+    def __init__(self, seed=0xB2000000):
+        h = P()
+        check(lib.rf_mlp_create(seed, C.byref(h)), "rf_mlp_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.rf_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_residual(self, on=True):
+        check(lib.rf_mlp_set_residual(self.h, 1 if on else 0), "rf_mlp_set_residual")
+
+    def forward(self, X, rows, Y, ldy=16, ncols=16):
+        check(lib.rf_mlp_forward(self.h, ptr(X), rows, ptr(Y), ldy, ncols), "rf_mlp_forward")
+
+    def train_step(self, X, T, rows, lr):
+        loss = C.c_double(0)
+        check(lib.rf_mlp_train_step(self.h, ptr(X), ptr(T), rows, lr, C.byref(loss)), "rf_mlp_train_step")
+        return loss.value
+
+    def weights(self):
+        out = []
+        for l in range(4):
+            W = np.zeros((MLP_DOUT[l], MLP_DIN[l]), np.float32)
+            b = np.zeros(MLP_DOUT[l], np.float32)
+            check(lib.rf_mlp_get(self.h, l, W.ctypes.data, b.ctypes.data), "rf_mlp_get")
+            out.append((W, b))
+        return out
+
+    def set_weights(self, ws):
+        for l, (W, b) in enumerate(ws):
+            W = np.ascontiguousarray(W, np.float32)
+            b = np.ascontiguousarray(b, np.float32)
+            check(lib.rf_mlp_set(self.h, l, W.ctypes.data, b.ctypes.data), "rf_mlp_set")
+
+    def grads(self):
+        out = []
+        for l in range(4):
+            gT = np.zeros((MLP_DIN[l], MLP_DOUT[l]), np.float32)
+            gb = np.zeros(MLP_DOUT[l], np.float32)
+            check(lib.rf_mlp_grad(self.h, l, gT.ctypes.data, gb.ctypes.data), "rf_mlp_grad")
+            out.append((gT, gb))
+        return out

@@ -1,21 +1,27 @@
-"""Benchmark: explicit BPM uniaxial compression, particle-steps/s.
+"""Benchmark: particle-steps/s of the explicit bonded-particle step, and wall time per
+relaxed quasi-static load step (FIRE, warm-started by the MLP vs plain).
 
-Workload: a 198,061-particle seeded lattice cylinder (D 52 mm x H 104 mm, particle
-radius 0.5 mm) of the reference's granite bonded-particle model (parameters of
-mp_determineconjgradient.cu:15-38), loaded by the uniaxial platens, reference
-precision (FP32 state). One bench "step" is STEPS_PER_BENCH_STEP explicit DEM steps
-of the whole specimen (bin/list maintenance, bond and contact forces with break
-check, platen, integration, cut, load reduction).
+Workload: a 200,000-particle polydisperse cylinder packed on the GPU (radii U[0.8, 1.2]
+x 0.25 mm, aspect 2, packing fraction 0.58: D 24.6 x H 49.3 mm), bonded where the gap is
+below 0.05 r_min, kn = 1e11 N/m^3, ks = kn / 2.5, Weibull(m = 5) tensile / shear
+strengths with scales 10 / 30 MPa, granite contacts, FP64 positions and FP32 forces,
+dt = 1e-8 s, platen strain rate 0.1/s. One bench "step" is STEPS_PER_BENCH_STEP
+explicit steps of the whole specimen (list maintenance, bond and contact forces with
+the break check, platen, integration, cut, load reduction).
 
-value : particle-steps/s of the fused engine, state resident in HBM, timed with
-        CUDA events on the engine's stream (max over ranks for N > 1).
-e2e   : the same metric through the reference-facing driver call
-        md_CalculationUniaxialCompression with host buffers (pinned upload of the
-        positions, build of cells/rows/bonds, the steps, download of the result),
-        timed on the host around each call.
+value : particle-steps/s of the fused engine, state resident in HBM, CUDA events on the
+        engine's stream (max over ranks for N > 1).
+e2e   : the same metric through the public API with host buffers: rf_engine_create_ext
+        from pinned host positions and radii (bond construction included), the steps,
+        and the FP64 positions read back.
+fire  : quasi-static load increments (strain 2.5e-5) relaxed by FIRE to a residual of
+        1e-6 x the mean normal pair force, on a 20,000-particle specimen of the same
+        kind: plain FIRE vs FIRE warm-started by the MLP trained on plain-FIRE pairs
+        of the same run; wall time per load step of each.
 --impl reference : the reference's own CPU force path (h_CalculateForceElastic,
-        md_calculateforcesbpm_cpu.cpp, built from its source into oracle/_ref) on
-        the same specimen's bonds, all host threads (one specimen copy per thread).
+        md_calculateforcesbpm_cpu.cpp, built from its source into oracle/_ref) on a
+        198k-particle lattice specimen of the reference's own (mono-sized, FP32) model,
+        all host threads. The extended model has no reference implementation.
 
 Multi-GPU: independent specimens per rank (different seeds), no data-path
 collective; only the elapsed time is max-reduced.
@@ -39,9 +45,13 @@ for _p in (ROOT, PKG):
 import numpy as np
 
 STEPS_PER_BENCH_STEP = 1000
-DIAMETER, HEIGHT = 52.0, 104.0
-METRIC = "particle-steps/s"
-WORKLOAD = "explicit BPM uniaxial compression, 198k-particle lattice cylinder D52xH104 mm, granite, fp32 state"
+N_PARTICLES, R0, PHI = 200000, 0.25, 0.58
+DIAMETER, HEIGHT = 52.0, 104.0          # the reference-model lattice specimen (198,061 particles)
+METRIC = "particle-steps/s; wall time per relaxed load step, warm-start vs plain FIRE"
+REF_WORKLOAD = ("reference model (mono-sized granite BPM, FP32): 198k-particle lattice cylinder D52xH104 mm; "
+                "the reference has no polydisperse / FP64 / Weibull model, so its own model is timed")
+WORKLOAD = ("explicit BPM uniaxial compression, 200k-particle polydisperse cylinder (radii U[0.8,1.2] x 0.25 mm, "
+            "D 24.6 x H 49.3 mm), Weibull bond strengths, FP64 positions / FP32 forces, dt 1e-8 s, 0.1/s")
 
 
 def peaks():
@@ -52,9 +62,9 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_particle_step():
+def traffic_per_particle_step(name="k_step_ext_uniaxial-200k.md"):
     """dram read+write bytes per particle-step of the step kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_step_uniaxial-200k.md")
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -196,28 +206,42 @@ def run_reference(args):
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "impl": "reference", "n_gpus": ws,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "particles": N, "cpu_threads": threads},
+           "config": {"workload": REF_WORKLOAD, "particles": N, "cpu_threads": threads},
            "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
                             "sample": sample},
            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
 
-def run_engine(args):
-    import torch
-    rank, ws, dist = dist_init()
-    dev = torch.cuda.current_device()
-    import rfdem
+def ext_specimen(rfdem, N, seed):
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, R0_MM, aspect=2.0, phi=PHI, seed=seed)
+    v = -0.1 * H * 1e-6                        # strain rate 0.1/s in mm per microsecond
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, R0_MM, dt=0.01, v_load=v, max_strain=1.0)
+    return t, R, rad, D, H
+
+
+R0_MM = R0
+
+
+def ext_bytes_per_particle_step(K, bbar, cbar):
+    """Algorithmic bytes per particle-step of the fused extended-model step: FP64
+    position (32 B) and FP32 velocity and spin (32 B) read and written, the K-slot row
+    (id + type) once, the binning share, per bond record its partner id and slot (5),
+    state read and written (96), rest length and strengths (16), per active contact its
+    tangential overlap read and written (24)."""
+    return 128 + 5 * K + 32 + 117 * bbar + 24 * cbar
+
+
+def run_explicit(rfdem, torch, t, R, rad, x, args, dist, stream_of):
     S = STEPS_PER_BENCH_STEP
-    t, R = rfdem.make_test(rfdem.RF_TEST_UNIAXIAL, DIAMETER, HEIGHT, seed=0xB2000000 + 2000 + rank, max_strain=1.0)
     N = int(t.N)
-    e = rfdem.Engine(t, R)
+    e = rfdem.Engine(t, R, ext=x, radius=rad)
     stream = torch.cuda.ExternalStream(e.stream())
     for _ in range(args.warmup):
         e.step(S)
     torch.cuda.synchronize()
     c0 = e.counters()
-    clocks = Clocks(dev)
+    clocks = Clocks(torch.cuda.current_device())
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -234,16 +258,83 @@ def run_engine(args):
         dist.barrier()
     ms = ev0.elapsed_time(ev1)
     c1 = e.counters()
+    _, res = e.sync()
     done_steps = c1["steps"] - c0["steps"]
     if done_steps != S * args.steps:
         raise SystemExit("bench: the specimen finished early (%d of %d steps)" % (done_steps, S * args.steps))
+    graph = e.uses_graph()
+    e.close()
+    return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, error=res.error)
+
+
+FIRE_N, FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 20000, 1, 5, 3
+
+
+def run_fire(rfdem, torch, seed):
+    """Quasi-static load steps on a 20k-particle specimen of the benchmark's kind: two
+    engines in lockstep take FIRE_PRE + FIRE_COLLECT plain increments (the MLP is trained
+    on the plain engine's FIRE_COLLECT relaxation pairs), then FIRE_EVAL increments each:
+    one plain, one warm-started by the MLP. Wall time per relaxed load step of each."""
+    from rfdem.warm import WarmStart
+    t, R, rad, Dm, Hm = ext_specimen(rfdem, FIRE_N, seed)
+    x = rfdem.ext_params_si()
+    A = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
+    B = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
+    p = A.relax_params(max_iter=60000)
+    ws = WarmStart(FIRE_N, p.strain_inc, seed=seed)
+    for k in range(FIRE_PRE + FIRE_COLLECT):
+        collect = k >= FIRE_PRE
+        if collect:
+            ws.features(A)
+        A.load_increment(p)
+        B.load_increment(p)
+        if collect:
+            ws.collect(A)
+    t0 = time.perf_counter()
+    losses = ws.train()
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    plain, warm = [], []
+    for k in range(FIRE_EVAL):
+        t0 = time.perf_counter()
+        ra = A.load_increment(p)
+        ta = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Y = ws.predict(B)
+        rb = B.load_increment_pred(p, Y, 16)
+        tb = time.perf_counter() - t0
+        plain.append((ta, ra.iterations, ra.converged, ra.stress))
+        warm.append((tb, rb.iterations, rb.converged, rb.stress))
+    A.close(); B.close(); ws.close()
+    tp = sum(a[0] for a in plain) / FIRE_EVAL
+    tw = sum(a[0] for a in warm) / FIRE_EVAL
+    return {"workload": "quasi-static uniaxial load steps of strain 2.5e-5, %d-particle cylinder of the same kind, "
+                        "FIRE (stiffness-scaled masses) to RMS net force <= 1e-6 x mean normal pair force" % FIRE_N,
+            "wall_s_per_load_step_plain": tp, "wall_s_per_load_step_warm": tw, "speedup_warm_vs_plain": tp / tw,
+            "iterations_plain": [a[1] for a in plain], "iterations_warm": [a[1] for a in warm],
+            "converged_plain": [a[2] for a in plain], "converged_warm": [a[2] for a in warm],
+            "stress_plain": [a[3] for a in plain], "stress_warm": [a[3] for a in warm],
+            "training_pairs": ws.pairs(), "training_loss": [losses[0], losses[-1]], "training_s": t_train,
+            "warm_start_includes": "feature build + MLP forward (tcgen05 BF16) per load step"}
+
+
+def run_engine(args):
+    import torch
+    rank, ws, dist = dist_init()
+    import rfdem
+    S = STEPS_PER_BENCH_STEP
+    t, R, rad, Dm, Hm = ext_specimen(rfdem, N_PARTICLES, 0xB2000000 + 2000 + rank)
+    x = rfdem.ext_params_si()
+    N = int(t.N)
+    K = int(t.K)
+    r = run_explicit(rfdem, torch, t, R, rad, x, args, dist, None)
+    ms = r["ms"]
     ms_max = max_over_ranks(ms, dist)
     total_particles = sum_over_ranks(float(N), dist)
     value = total_particles * S * args.steps / (ms_max * 1e-3)
+    c1, c0 = r["c1"], r["c0"]
     bbar, cbar = c1["bonds"] / N, c1["contacts"] / N
-    K = int(t.K)
-    # algorithmic bytes per particle-step (fused explicit step, FP32 state, K slots)
-    b_step = 72 + 5 * K + 32 + 105 * bbar + 24 * cbar
+    b_step = ext_bytes_per_particle_step(K, bbar, cbar)
     per_step_s = (ms * 1e-3) / (S * args.steps)
     achieved = b_step * N / per_step_s / 1e9
     peak, peak_kind = peaks()
@@ -251,25 +342,23 @@ def run_engine(args):
     rebuilds = c1["rebuilds"] - c0["rebuilds"]
     launches = S * args.steps + 7 * rebuilds + 2 * args.steps
 
-    # e2e through the reference-facing driver call with host buffers
-    graph_used = e.uses_graph()
-    e.close()
-    e2e_steps = S
-    pinned = torch.from_numpy(R).pin_memory()
-    Rout = torch.empty_like(pinned).pin_memory()
-    curve = torch.empty(3 * e2e_steps, dtype=torch.float64).pin_memory()
+    # e2e through the public API with host buffers (pinned)
     import ctypes as C
-    e2e_calls = 0 if args.no_e2e else 3
-
-    def e2e_call():
-        tt = rfdem.Task.from_buffer_copy(t)
-        res = rfdem.RunResult()
-        rfdem.check(rfdem.lib.md_CalculationUniaxialCompression(C.byref(tt), pinned.data_ptr(), e2e_steps,
-                                                                 curve.data_ptr(), e2e_steps, Rout.data_ptr(),
-                                                                 C.byref(res)), "e2e")
-        return res
     e2e_value = None
+    e2e_calls = 0 if args.no_e2e else 3
     if e2e_calls:
+        hR = torch.from_numpy(R).pin_memory()
+        hrad = torch.from_numpy(rad).pin_memory()
+        hout = torch.empty_like(hR).pin_memory()
+
+        def e2e_call():
+            tt = rfdem.Task.from_buffer_copy(t)
+            h = rfdem.P()
+            rfdem.check(rfdem.lib.rf_engine_create_ext(C.byref(tt), C.byref(x), hR.data_ptr(), hrad.data_ptr(),
+                                                       C.byref(h)), "e2e create")
+            rfdem.check(rfdem.lib.rf_engine_step(h, S), "e2e step")
+            rfdem.check(rfdem.lib.rf_engine_positions_f64(h, hout.data_ptr()), "e2e positions")
+            rfdem.lib.rf_engine_destroy(h)
         e2e_call()
         torch.cuda.synchronize()
         if dist is not None:
@@ -279,43 +368,92 @@ def run_engine(args):
             e2e_call()
         torch.cuda.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
-        e2e_value = total_particles * e2e_steps * e2e_calls / e2e_s
+        e2e_value = total_particles * S * e2e_calls / e2e_s
+
+    # the reference's own model (mono-sized lattice, FP32 state), reference-exact engine
+    refmodel = None
+    if not args.no_reference_model:
+        tr_, Rr = rfdem.make_test(rfdem.RF_TEST_UNIAXIAL, DIAMETER, HEIGHT, seed=0xB2000000 + 2000 + rank,
+                                  max_strain=1.0)
+        er = rfdem.Engine(tr_, Rr)
+        sr = torch.cuda.ExternalStream(er.stream())
+        for _ in range(args.warmup):
+            er.step(S)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(sr)
+        for _ in range(args.steps):
+            er.step(S)
+        a1.record(sr)
+        a1.synchronize()
+        mr = max_over_ranks(a0.elapsed_time(a1), dist)
+        Nr = int(tr_.N)
+        cr = er.counters()
+        er.close()
+        refmodel = {"workload": "reference model (mono-sized granite BPM, FP32 state, bit-exact with the reference), "
+                                "198k-particle lattice cylinder D52xH104 mm",
+                    "particles": Nr, "value": sum_over_ranks(float(Nr), dist) * S * args.steps / (mr * 1e-3),
+                    "unit": "particle-steps/s", "ms_per_step": mr / args.steps,
+                    "bytes_per_particle_step": round(72 + 5 * K + 32 + 105 * cr["bonds"] / Nr
+                                                     + 24 * cr["contacts"] / Nr, 1)}
+        trr = traffic_per_particle_step("k_step_uniaxial-200k.md")
+        if trr:
+            refmodel["traffic_bytes_per_particle_step"] = trr
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        reps = 3
-        secs, bonds = cpu_reference(t, R, reps, threads)
-        if secs is not None:
-            cpu = {"value": threads * N * reps / secs, "unit": "particle-steps/s", "cores": threads,
-                   "kind": "reference",
-                   "sample": "reference h_CalculateForceElastic (bond slots only) over the %d bond slots of the "
-                             "same specimen, %d passes x %d threads, one specimen copy per thread" % (bonds, reps,
-                                                                                                     threads)}
+        cpu = cpu_port_sample(t, x, R, rad)
+
+    fire = None
+    if rank == 0 and ws == 1 and not args.no_fire:
+        fire = run_fire(rfdem, torch, 0xB2000000 + 3000)
     if rank != 0:
         return
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "particles": N, "explicit_steps_per_bench_step": S, "slots_K": K,
+           "vs_baseline": None, "dtype": "f32 forces, f64 positions", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "particles": N, "specimen_mm": [round(Dm, 2), round(Hm, 2)],
+                      "explicit_steps_per_bench_step": S, "slots_K": K,
                       "bonds_per_particle": round(bbar, 3), "contacts_per_particle": round(cbar, 3),
-                      "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 57 + N * 100) / 1e6),
-                      "parallelism": "specimen-per-gpu" if ws > 1 else "single"},
-           "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 12 * N,
-                   "d2h_bytes_per_step": 12 * N + 24 * e2e_steps,
-                   "path": "md_CalculationUniaxialCompression, %d explicit steps per call incl. build" % e2e_steps},
+                      "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 16 + N * 300 + c1["bonds"] * 129) / 1e6),
+                      "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": r["graph"]},
+           "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * N,
+                   "d2h_bytes_per_step": 24 * N,
+                   "path": "rf_engine_create_ext (host positions + radii, bond build) + %d explicit steps + "
+                           "rf_engine_positions_f64 per call" % S},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": (tr * N) if tr else None, "peak_source": peak_kind,
-                        "kernel": "k_step (fused explicit step)",
+                        "kernel": "k_step_ext (fused explicit step, extended model)",
                         "bytes_per_particle_step": round(b_step, 1)},
            "cpu_baseline": cpu,
            "gpu_launches": launches,
            "rebuilds": rebuilds,
-           "clocks": clk}
-    out["config"]["graph"] = graph_used
+           "clocks": r["clocks"],
+           "fire": fire,
+           "reference_model": refmodel}
     print(json.dumps(out))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def cpu_port_sample(t, x, R, rad):
+    """The oracle's restatement of the extended-model step (the engine's arithmetic, one
+    host thread) on the same specimen: bond construction once, then explicit steps;
+    the per-step time excludes the construction."""
+    import oracle
+    import rfdem
+    t1 = time.perf_counter()
+    oracle.run_ext(rfdem.Task.from_buffer_copy(t), x, R, rad, 0)
+    t_init = time.perf_counter() - t1
+    steps = 3
+    t1 = time.perf_counter()
+    oracle.run_ext(rfdem.Task.from_buffer_copy(t), x, R, rad, steps)
+    t_run = time.perf_counter() - t1 - t_init
+    N = int(t.N)
+    return {"value": N * steps / t_run, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+            "sample": "oracle restatement of the extended-model explicit step (float forces, FP64 positions), "
+                      "%d steps of the same %d-particle specimen on one host thread (construction excluded)"
+                      % (steps, N)}
 
 
 def main():
@@ -326,6 +464,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the driver-call leg (profiling runs)")
+    ap.add_argument("--no-fire", action="store_true", help="skip the quasi-static FIRE comparison")
+    ap.add_argument("--no-reference-model", action="store_true", help="skip the reference-model line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

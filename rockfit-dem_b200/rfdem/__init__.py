@@ -313,17 +313,20 @@ def ext_params_si(kn=1e11, ks=None, bond_lambda=0.330015, gap_frac=0.05, weibull
 
 def make_test_ext(kind, R0, radius, r0, K=32, potential=None, margin=None, v_load=None, min_stress=None,
                   max_strain=0.1, dt=None):
-    """A prepared task for a packed specimen centred at the origin (kind as make_test:
-    uniaxial along z, or Brazilian disc of axis z loaded along y). Returns (Task, R)
-    with R shifted to the task's centre. dt (microseconds) overrides the derived step."""
+    """A prepared task for a packed specimen (kind as make_test: uniaxial along z, or
+    Brazilian disc of axis z loaded along y). The particle-centre box is centred on the
+    task's centre, so the platens start on the outermost particles. Returns (Task, R).
+    dt (microseconds) overrides the derived step."""
     po = potential or granite_potential()
     po.p_r = r0
     po.b_r = 0.330015 * r0
     po.b_d = 2.0 * r0 + 0.0593169 * r0 * 2.0
     po.a_farcut = 2.9 * r0
     N = radius.size
-    P3 = R0.reshape(3, N)
-    L = [2.0 * float(np.max(np.abs(P3[a]))) for a in range(3)]
+    P3 = R0.reshape(3, N).copy()
+    mid = 0.5 * (P3.max(axis=1) + P3.min(axis=1))
+    P3 -= mid[:, None]                 # centre the particle-centre box: the platens start on the outer particles
+    L = [float(P3[a].max() - P3[a].min()) for a in range(3)]
     if margin is None:
         margin = 4.0 * r0 + 0.25 * max(L)
     space = [x + 2 * r0 + 2 * margin for x in L]

@@ -14,10 +14,10 @@ value : particle-steps/s of the fused engine, state resident in HBM, CUDA events
 e2e   : the same metric through the public API with host buffers: rf_engine_create_ext
         from pinned host positions and radii (bond construction included), the steps,
         and the FP64 positions read back.
-fire  : quasi-static load increments (strain 2.5e-5) relaxed by FIRE to a residual of
-        1e-6 x the mean normal pair force, on a 20,000-particle specimen of the same
-        kind: plain FIRE vs FIRE warm-started by the MLP trained on plain-FIRE pairs
-        of the same run; wall time per load step of each.
+fire  : quasi-static load increments (strain 2.5e-5) of the same specimen relaxed by
+        FIRE to a residual of 1e-6 x the mean normal pair force: plain FIRE vs FIRE
+        warm-started by the MLP trained on plain-FIRE pairs of the same run; wall time
+        per load step of each.
 --impl reference : the reference's own CPU force path (h_CalculateForceElastic,
         md_calculateforcesbpm_cpu.cpp, built from its source into oracle/_ref) on a
         198k-particle lattice specimen of the reference's own (mono-sized, FP32) model,
@@ -267,17 +267,16 @@ def run_explicit(rfdem, torch, t, R, rad, x, args, dist, stream_of):
     return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, error=res.error)
 
 
-FIRE_N, FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 20000, 1, 5, 3
+FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 1, 2, 4
 
 
-def run_fire(rfdem, torch, seed):
-    """Quasi-static load steps on a 20k-particle specimen of the benchmark's kind: two
-    engines in lockstep take FIRE_PRE + FIRE_COLLECT plain increments (the MLP is trained
-    on the plain engine's FIRE_COLLECT relaxation pairs), then FIRE_EVAL increments each:
-    one plain, one warm-started by the MLP. Wall time per relaxed load step of each."""
+def run_fire(rfdem, torch, t, R, rad, x, seed):
+    """Quasi-static load steps on the benchmark specimen: two engines in lockstep take
+    FIRE_PRE + FIRE_COLLECT plain increments (the MLP is trained on the plain engine's
+    FIRE_COLLECT relaxation pairs), then FIRE_EVAL increments each: one plain, one
+    warm-started by the MLP. Wall time per relaxed load step of each."""
     from rfdem.warm import WarmStart
-    t, R, rad, Dm, Hm = ext_specimen(rfdem, FIRE_N, seed)
-    x = rfdem.ext_params_si()
+    FIRE_N = int(t.N)
     A = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
     B = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
     p = A.relax_params(max_iter=60000)
@@ -308,7 +307,7 @@ def run_fire(rfdem, torch, seed):
     A.close(); B.close(); ws.close()
     tp = sum(a[0] for a in plain) / FIRE_EVAL
     tw = sum(a[0] for a in warm) / FIRE_EVAL
-    return {"workload": "quasi-static uniaxial load steps of strain 2.5e-5, %d-particle cylinder of the same kind, "
+    return {"workload": "quasi-static uniaxial load steps of strain 2.5e-5 of the same %d-particle specimen, "
                         "FIRE (stiffness-scaled masses) to RMS net force <= 1e-6 x mean normal pair force" % FIRE_N,
             "wall_s_per_load_step_plain": tp, "wall_s_per_load_step_warm": tw, "speedup_warm_vs_plain": tp / tw,
             "iterations_plain": [a[1] for a in plain], "iterations_warm": [a[1] for a in warm],
@@ -406,7 +405,7 @@ def run_engine(args):
 
     fire = None
     if rank == 0 and ws == 1 and not args.no_fire:
-        fire = run_fire(rfdem, torch, 0xB2000000 + 3000)
+        fire = run_fire(rfdem, torch, t, R, rad, x, 0xB2000000 + 3000)
     if rank != 0:
         return
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,

@@ -1185,11 +1185,11 @@ struct RunExt {
         const bool brz = t->kind == RF_TEST_BRAZIL;
         const double Zcut = brz ? (double)(float)((double)t->S.center.y + (double)t->S.spacesized2.y)
                                 : (double)(float)((double)t->S.center.z + (double)t->S.spacesized2.z);
-        (void)i;
+        const double off = rad[i] - t->Po.p_r;    // the platens act on the particle surfaces
         if (brz) {
             const TF rx = (TF)(float)(Rx - cx), rz = (TF)(float)(Rz - cz);
             if (rx * rx + rz * rz < (TF)RR && (double)rz < Zcut) {
-                if (Ry - TopR > -1e-9) {
+                if (Ry + off - TopR > -1e-9) {
                     const TF fy = Fy;
                     if (fy > 0) {
                         sft += (double)fy;
@@ -1200,9 +1200,9 @@ struct RunExt {
                             Fz -= (TF)0.45f * fy * Vz * iv;
                         }
                     }
-                    if (Ry - Top > -1e-9) { Ry = Top; Vy = vt; Fy = 0; }
+                    if (Ry + off - Top > -1e-9) { Ry = Top - off; Vy = vt; Fy = 0; }
                 }
-                if (Ry - BottomR < 1e-9) {
+                if (Ry - off - BottomR < 1e-9) {
                     const TF fy = Fy;
                     if (fy < 0) {
                         sfb += (double)fy;
@@ -1213,19 +1213,19 @@ struct RunExt {
                             Fz += (TF)0.45f * fy * Vz * iv;
                         }
                     }
-                    if (Ry - Bottom < 1e-9) { Ry = Bottom; Vy = 0; Fy = 0; }
+                    if (Ry - off - Bottom < 1e-9) { Ry = Bottom + off; Vy = 0; Fy = 0; }
                 }
             }
         } else {
             const TF rx = (TF)(float)(Rx - cx), ry = (TF)(float)(Ry - cy);
             if (rx * rx + ry * ry < (TF)RR && Rz < Zcut) {
-                if (Rz - TopR > -1e-9) {
+                if (Rz + off - TopR > -1e-9) {
                     if (Fz > 0) sft += (double)Fz;
-                    if (Rz - Top > -1e-9) { Rz = Top; Vz = vt; Fz = 0; }
+                    if (Rz + off - Top > -1e-9) { Rz = Top - off; Vz = vt; Fz = 0; }
                 }
-                if (Rz - BottomR < 1e-9) {
+                if (Rz - off - BottomR < 1e-9) {
                     if (Fz < 0) sfb += (double)Fz;
-                    if (Rz - Bottom < 1e-9) { Rz = Bottom; Vz = 0; Fz = 0; }
+                    if (Rz - off - Bottom < 1e-9) { Rz = Bottom + off; Vz = 0; Fz = 0; }
                 }
             }
         }

@@ -720,31 +720,36 @@ __global__ void k_delete_pending_ext(Dev d, Consts c) {
 }
 
 // Platen contact and clamp with FP64 positions (d_UniaxialCompression3_simple /
-// d_braziltest_simple2 with the coordinates kept in double).
+// d_braziltest_simple2 with the coordinates kept in double). The platens act on the
+// particle surfaces: the coordinate tested and clamped along the load axis is the
+// centre plus (radius - p_r) towards the top platen and minus it towards the bottom
+// one, so a polydisperse specimen meets a flat platen with every particle that
+// touches it; for radius p_r this is the reference's centre rule.
 __device__ __forceinline__ void uniaxial_particle_ext(double& Rx, double& Ry, double& Rz, float& Vz, float& Fz,
                                                       const rf_float3 c, float RR, double Zt, double Zb, double Ztr,
-                                                      double Zbr, float vt, double Zcut, double& sfb, double& sft) {
+                                                      double Zbr, float vt, double Zcut, double off, double& sfb,
+                                                      double& sft) {
     const float rx = (float)(Rx - c.x), ry = (float)(Ry - c.y);
     const double rz = Rz;
     if (rx * rx + ry * ry < RR && rz < Zcut) {
-        if (rz - Ztr > -1e-9) {
+        if (rz + off - Ztr > -1e-9) {
             if (Fz > 0) sft += (double)Fz;
-            if (rz - Zt > -1e-9) { Rz = Zt; Vz = vt; Fz = 0.f; }
+            if (rz + off - Zt > -1e-9) { Rz = Zt - off; Vz = vt; Fz = 0.f; }
         }
-        if (rz - Zbr < 1e-9) {
+        if (rz - off - Zbr < 1e-9) {
             if (Fz < 0) sfb += (double)Fz;
-            if (rz - Zb < 1e-9) { Rz = Zb; Vz = 0.f; Fz = 0.f; }
+            if (rz - off - Zb < 1e-9) { Rz = Zb + off; Vz = 0.f; Fz = 0.f; }
         }
     }
 }
 __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, double& Rz, float& Vx, float& Vy,
                                                     float& Vz, float& Fx, float& Fy, float& Fz, const rf_float3 c,
                                                     float RR, double Yt, double Yb, double Ytr, double Ybr, float vt,
-                                                    double Zcut, double& sfb, double& sft) {
+                                                    double Zcut, double off, double& sfb, double& sft) {
     const float rx = (float)(Rx - c.x), rz = (float)(Rz - c.z);
     const double ry = Ry;
     if (rx * rx + rz * rz < RR && (double)rz < Zcut) {
-        if (ry - Ytr > -1e-9) {
+        if (ry + off - Ytr > -1e-9) {
             const float fy = Fy;
             if (fy > 0) {
                 sft += (double)fy;
@@ -755,9 +760,9 @@ __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, doub
                     Fz -= 0.45f * fy * Vz * iv;
                 }
             }
-            if (ry - Yt > -1e-9) { Ry = Yt; Vy = vt; Fy = 0.f; }
+            if (ry + off - Yt > -1e-9) { Ry = Yt - off; Vy = vt; Fy = 0.f; }
         }
-        if (ry - Ybr < 1e-9) {
+        if (ry - off - Ybr < 1e-9) {
             const float fy = Fy;
             if (fy < 0) {
                 sfb += (double)fy;
@@ -768,7 +773,7 @@ __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, doub
                     Fz += 0.45f * fy * Vz * iv;
                 }
             }
-            if (ry - Yb < 1e-9) { Ry = Yb; Vy = 0.f; Fy = 0.f; }
+            if (ry - off - Yb < 1e-9) { Ry = Yb + off; Vy = 0.f; Fy = 0.f; }
         }
     }
 }
@@ -964,10 +969,10 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         float Vx = vi.x, Vy = vi.y, Vz = vi.z;
         if (KIND == RF_TEST_BRAZIL)
             brazil_particle_ext(Rx, Ry, Rz, Vx, Vy, Vz, Fx, Fy, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt,
-                                (double)c.zcut, sfb, sft);
+                                (double)c.zcut, xi.w - c.p_r_d, sfb, sft);
         else
-            uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)c.zcut, sfb,
-                                  sft);
+            uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)c.zcut,
+                                  xi.w - c.p_r_d, sfb, sft);
         if (MODE == 1) {
             // FIRE: keep the clamped state for the update kernel; reduce the FIRE sums
             d.posd[nxt][i] = make_double4(Rx, Ry, Rz, xi.w);
@@ -1228,10 +1233,10 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int 
         double sb = 0.0, st = 0.0;
         if (KIND == RF_TEST_BRAZIL)
             brazil_particle_ext(x.x, x.y, x.z, v0, v1, v2, f0, f1, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f,
-                                (double)c.zcut, sb, st);
+                                (double)c.zcut, x.w - c.p_r_d, sb, st);
         else
-            uniaxial_particle_ext(x.x, x.y, x.z, v2, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f, (double)c.zcut, sb,
-                                  st);
+            uniaxial_particle_ext(x.x, x.y, x.z, v2, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f, (double)c.zcut,
+                                  x.w - c.p_r_d, sb, st);
         d.posd[cur][i] = x;
         d.vel[cur][i] = make_float4(v0, v1, v2, 0.f);
         d.ang[cur][i] = w;
@@ -1278,8 +1283,8 @@ __global__ void k_warm_features(Dev d, Consts c, double D, double sinc, __nv_bfl
         ++nb;
     }
     f[56] = (float)nb * (1.0f / 12.0f);
-    const double xa = ax == 1 ? x.y : x.z;
-    f[57] = (xa - sc->Top > -1e-9 || xa - sc->Bottom < 1e-9) ? 1.f : 0.f;
+    const double xa = ax == 1 ? x.y : x.z, off = x.w - c.p_r_d;
+    f[57] = (xa + off - sc->Top > -1e-9 || xa - off - sc->Bottom < 1e-9) ? 1.f : 0.f;
     f[58] = 1.f;
     uint4* out = reinterpret_cast<uint4*>(feat + (size_t)i * 64);
 #pragma unroll

@@ -324,9 +324,13 @@ def make_test_ext(kind, R0, radius, r0, K=32, potential=None, margin=None, v_loa
     po.a_farcut = 2.9 * r0
     N = radius.size
     P3 = R0.reshape(3, N).copy()
-    mid = 0.5 * (P3.max(axis=1) + P3.min(axis=1))
-    P3 -= mid[:, None]                 # centre the particle-centre box: the platens start on the outer particles
-    L = [float(P3[a].max() - P3[a].min()) for a in range(3)]
+    # the platens act on the particle surfaces (centre +- (radius - r0)): box the specimen
+    # by those coordinates, centred on the task's centre, so the platens start touching it
+    off = np.asarray(radius, np.float64) - r0
+    hi = (P3 + off[None, :]).max(axis=1)
+    lo = (P3 - off[None, :]).min(axis=1)
+    P3 -= (0.5 * (hi + lo))[:, None]
+    L = [float(hi[a] - lo[a]) for a in range(3)]
     if margin is None:
         margin = 4.0 * r0 + 0.25 * max(L)
     space = [x + 2 * r0 + 2 * margin for x in L]

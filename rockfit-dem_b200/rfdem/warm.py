@@ -29,6 +29,7 @@ class WarmStart:
     def features(self, engine):
         """Features of `engine` for its next increment (kept for collect())."""
         engine.warm_features(self.strain_inc, self.feat)
+        self.torch.cuda.synchronize()
         return self.feat
 
     def collect(self, engine):
@@ -52,9 +53,12 @@ class WarmStart:
         return losses
 
     def predict(self, engine):
-        """The prediction for `engine`'s next increment: float32 [rows, 16] on the device."""
+        """The prediction for `engine`'s next increment: float32 [rows, 16] on the device.
+        The engine and the MLP run on their own streams: each hand-over synchronises."""
         self.features(engine)
+        self.torch.cuda.synchronize()
         self.mlp.forward(self.feat, self.N, self.Y)
+        self.torch.cuda.synchronize()
         return self.Y
 
     def close(self):

@@ -456,6 +456,7 @@ def cpu_port_sample(t, x, R, rad):
 
 
 def main():
+    global STEPS_PER_BENCH_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
@@ -464,10 +465,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the driver-call leg (profiling runs)")
     ap.add_argument("--no-fire", action="store_true", help="skip the quasi-static FIRE comparison")
+    ap.add_argument("--explicit-steps", type=int, default=STEPS_PER_BENCH_STEP,
+                    help="explicit steps per bench step (profiling runs use fewer)")
     ap.add_argument("--no-reference-model", action="store_true", help="skip the reference-model line")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    STEPS_PER_BENCH_STEP = max(1, args.explicit_steps)
     if args.impl == "reference":
         run_reference(args)
     else:

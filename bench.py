@@ -120,34 +120,42 @@ class Clocks:
 
 
 def dist_init():
+    """One process per GPU under torchrun (NCCL); gloo when no GPU is present (tests)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
         return 0, 1, None
     import torch
     import torch.distributed as dist
     rank = int(os.environ["RANK"])
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
     import datetime
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, ws, dist
 
 
-def max_over_ranks(x, dist):
+def _reduce(x, dist, op):
     if dist is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(x, dist):
+    return x if dist is None else _reduce(x, dist, dist.ReduceOp.MAX)
 
 
 def sum_over_ranks(x, dist):
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return x if dist is None else _reduce(x, dist, dist.ReduceOp.SUM)
+
+
+def rank_seed(rank):
+    """Each rank packs its own specimen: weak scaling, no data-path collective."""
+    return 0xB2000000 + 2000 + rank
 
 
 def cpu_reference(task, R, reps, threads):
@@ -322,7 +330,7 @@ def run_engine(args):
     rank, ws, dist = dist_init()
     import rfdem
     S = STEPS_PER_BENCH_STEP
-    t, R, rad, Dm, Hm = ext_specimen(rfdem, N_PARTICLES, 0xB2000000 + 2000 + rank)
+    t, R, rad, Dm, Hm = ext_specimen(rfdem, N_PARTICLES, rank_seed(rank))
     x = rfdem.ext_params_si()
     N = int(t.N)
     K = int(t.K)

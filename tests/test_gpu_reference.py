@@ -92,7 +92,8 @@ def test_bond_construction_vs_reference(cuda, case):
     _, IL = mc.oracle_list_construct(t, R, CIs, pnC)
     ty, iL = np.zeros(N * K, np.uint8), np.zeros(N * K, np.float32)
     ty_r, iL_r = ty.copy(), iL.copy()
-    assert REF.ref_construct_bonds(R.ctypes.data, N, K, to32(IL).ctypes.data, ty_r.ctypes.data, iL_r.ctypes.data,
+    IL32 = to32(IL)                        # kept alive across the call
+    assert REF.ref_construct_bonds(R.ctypes.data, N, K, IL32.ctypes.data, ty_r.ctypes.data, iL_r.ctypes.data,
                                    np.float32(t.Po.b_dd), np.float32(t.Po.b_r)) == 0
     ILo, tyo, iLo, _ = mc.oracle_bonds_delete(t, R, IL, ty, iL, mc.zeros_state(N, K), np.float32(t.Po.b_dd),
                                               np.float32(t.Po.aa_farcut), True, False)
@@ -121,7 +122,8 @@ def test_forces_vs_reference_within_tolerance(cuda, case):
     F, M = np.zeros(3 * N, np.float32), np.zeros(3 * N, np.float32)
     p22 = np.array(mc.bond_params(t), np.float32)
     p21 = np.array(mc.contact_params(t), np.float32)
-    assert REF.ref_forces(st["R"].ctypes.data, V.ctypes.data, W.ctypes.data, N, K, to32(st["IL"]).ctypes.data,
+    IL32 = to32(st["IL"])                  # kept alive across the call
+    assert REF.ref_forces(st["R"].ctypes.data, V.ctypes.data, W.ctypes.data, N, K, IL32.ctypes.data,
                           ty_r.ctypes.data, st["iL"].ctypes.data, ref["Rij"].ctypes.data, ref["Oijt"].ctypes.data,
                           ref["Mijn"].ctypes.data, ref["Mijt"].ctypes.data, F.ctypes.data, M.ctypes.data,
                           p22.ctypes.data, p21.ctypes.data, 3) == 0

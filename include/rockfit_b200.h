@@ -358,6 +358,32 @@ rf_status rf_engine_create_ext(const rf_task* t, const rf_ext_params* x, const d
 rf_status rf_engine_positions_f64(rf_engine* e, double* R);
 
 /*
+ * A batch of specimens in one engine (extended model, explicit steps; no reference
+ * counterpart): nspec specimens of the same test kind, material, time step, slot count
+ * and bond stiffness, each with its own geometry, loading, seed and strength
+ * distribution (xs[q]), and at least 128 particles. They are laid out side by side along
+ * x, each shifted by a whole number of cells with two empty cells between boxes, so
+ * they never interact and each evolves exactly as it would alone on the batch's cell
+ * grid. One step kernel advances all of them; each specimen keeps its own platens, load
+ * reduction, load curve and stop condition (a finished specimen is frozen); the step
+ * loop ends when every specimen is done or the step target is reached.
+ * h_R[q]: double[3 N_q] planar, h_radius[q]: double[N_q]. Particle q of the batch's
+ * arrays (export, rf_engine_positions_f64) are ordered specimen after specimen, with x
+ * shifted by the specimen's offset (rf_engine_spec_info).
+ */
+rf_status rf_engine_create_batch(const rf_task* tasks, const rf_ext_params* xs, const double* const* h_R,
+                                 const double* const* h_radius, int nspec, rf_engine** out);
+/* Number of specimens of an engine (1 unless made by rf_engine_create_batch). */
+int rf_engine_batch_size(rf_engine* e);
+/* Specimen spec's first particle, particle count, x offset, and its task as the engine
+   runs it (shifted, with the batch's cell grid); any output may be NULL. */
+rf_status rf_engine_spec_info(rf_engine* e, int spec, uint64_t* first, uint64_t* count, double* x_offset,
+                              rf_task* task);
+/* rf_engine_sync / rf_engine_curve for one specimen (steps are the specimen's own). */
+rf_status rf_engine_sync_spec(rf_engine* e, int spec, rf_task* t_out, rf_run_result* r_out);
+rf_status rf_engine_curve_spec(rf_engine* e, int spec, double* curve, uint64_t cap, uint64_t* n);
+
+/*
  * Quasi-static loading (extended model; no reference counterpart: the reference's FIRE
  * relaxes a sample-preparation potential, md_firerelaxation.cu:85-368). Each load
  * increment advances the loading platen by strain_inc * initial size (0: relax in place)

@@ -87,7 +87,22 @@ struct Consts {
     double Top_shift;                   // unused (reserved)
 };
 
+// Per-specimen geometry of a batch (constant during a run): the platen's cut height, the
+// cut box and its hidden point, the specimen's particle range and the CTAs touching it.
+struct SpecGeom {
+    float zcut;
+    rf_float3 box_c, box_h, hp;
+    uint32_t p0, p1;
+    uint32_t b0, b1;
+};
+
 struct Dev {
+    // batch of specimens (one specimen: spec == sc, geom[0], blk_spec == nullptr)
+    DevScalars* spec;           // [nspec] per-specimen platen / result scalars
+    const SpecGeom* geom;       // [nspec]
+    const uint16_t* blk_spec;   // [blocks] first specimen of each 128-particle CTA
+    double2* partial2;          // [blocks] load partials of a CTA's second specimen
+    uint32_t nspec;
     double4* posd[2];   // extended model: x, y, z (FP64) and radius
     double* bL0;        // extended model: [QB][N] rest length of each bond record
     float2* bstr;       // extended model: [QB][N] tensile and shear strength of each bond record
@@ -778,6 +793,113 @@ __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, doub
     }
 }
 
+// End of an extended-model step for a batch of specimens. The platen reaction sums of a
+// CTA are kept per specimen (its first and, if it touches one, its second); the last CTA
+// adds each specimen's CTA partials in CTA order and runs SumForcesULoading
+// (md_results.cu:34-74), the fracture test and CompressB/U (md_data_types.h:223-293)
+// for every specimen still running; the loop ends when all are done. With one specimen
+// this is step_finish's arithmetic, sum for sum.
+template <int KIND>
+__device__ __forceinline__ void step_finish_ext(const Dev& d, const Consts& c, double sfb, double sft,
+                                                uint32_t nbroken, uint32_t moved, uint32_t second) {
+    DevScalars* sc = d.sc;
+    const uint32_t FULL = 0xffffffffu;
+    __shared__ double s_b[4], s_t[4], s_b2[4], s_t2[4];
+    __shared__ uint32_t s_n[4], s_m[4];
+    __shared__ bool s_last;
+    double b1 = second ? sfb : 0.0, t1 = second ? sft : 0.0;
+    if (second) { sfb = 0.0; sft = 0.0; }
+    for (int o = 16; o; o >>= 1) {
+        sfb += __shfl_xor_sync(FULL, sfb, o);
+        sft += __shfl_xor_sync(FULL, sft, o);
+        b1 += __shfl_xor_sync(FULL, b1, o);
+        t1 += __shfl_xor_sync(FULL, t1, o);
+    }
+    const uint32_t wn = __reduce_add_sync(FULL, nbroken), wm = __reduce_or_sync(FULL, moved);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { s_b[w] = sfb; s_t[w] = sft; s_b2[w] = b1; s_t2[w] = t1; s_n[w] = wn; s_m[w] = wm; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        d.partial[blockIdx.x] = make_double2((s_b[0] + s_b[1]) + (s_b[2] + s_b[3]), (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]));
+        d.partial2[blockIdx.x] =
+            make_double2((s_b2[0] + s_b2[1]) + (s_b2[2] + s_b2[3]), (s_t2[0] + s_t2[1]) + (s_t2[2] + s_t2[3]));
+        const uint32_t nb = s_n[0] + s_n[1] + s_n[2] + s_n[3];
+        if (nb) atomicAdd(&sc->broken, (unsigned long long)nb);
+        if (s_m[0] | s_m[1] | s_m[2] | s_m[3]) atomicOr(&sc->moved, 1u);
+        __threadfence();
+        const uint32_t ticket = atomicAdd(&sc->block_counter, 1u);
+        s_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    bool all_done = true;
+    for (uint32_t s = 0; s < d.nspec; ++s) {
+        DevScalars* S = d.spec + s;
+        const SpecGeom& G = d.geom[s];
+        if (S->done) continue;                               // uniform across the CTA
+        double pb = 0.0, pt = 0.0;
+        for (uint32_t b = G.b0 + threadIdx.x; b <= G.b1; b += blockDim.x) {
+            const double2 v = (d.blk_spec == nullptr || d.blk_spec[b] == s) ? __ldcg(&d.partial[b])
+                                                                             : __ldcg(&d.partial2[b]);
+            pb += v.x; pt += v.y;
+        }
+        for (int o = 16; o; o >>= 1) {
+            pb += __shfl_xor_sync(FULL, pb, o);
+            pt += __shfl_xor_sync(FULL, pt, o);
+        }
+        __syncthreads();
+        if (l == 0) { s_b[w] = pb; s_t[w] = pt; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const double sfb_all = (s_b[0] + s_b[1]) + (s_b[2] + s_b[3]);
+            const double sft_all = (s_t[0] + s_t[1]) + (s_t[2] + s_t[3]);
+            const double a1 = (double)S->_1d_Area;
+            if (S->curve_n < c.curve_cap) {
+                double* rec = d.curve + 3 * ((size_t)s * c.curve_cap + S->curve_n);
+                rec[0] = (S->size_d[2] - S->sz0) / S->sz0;
+                rec[1] = sfb_all * a1;
+                rec[2] = sft_all * a1;
+            }
+            S->curve_n += 1;
+            S->Stress = 0.5 * (fabs(sfb_all) + fabs(sft_all)) * a1;
+            if (!S->Loading && S->Stress > S->MinStress) S->Loading = 1;
+            if (S->FractureStress < S->Stress) {
+                S->FractureStress = S->Stress;
+                S->FractureStrain = (S->sz0 - S->size_d[2]) / S->sz0;
+            }
+            if (S->Loading && S->Stress < S->ZeroStress) S->Fracture = 1;
+            const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+            S->V = (S->Stress < 1e-9) ? 10.0 * S->VLoad : S->VLoad;
+            S->size_d[ax] += S->V * c.dt_d;
+            S->Top += S->V * c.dt_d;
+            S->TopR = S->Top - 2.0 * c.p_r_d;
+            S->size[ax] = (float)S->size_d[ax];
+            S->sized2[ax] = (float)(0.5 * S->size_d[ax]);
+            S->center_d[ax] += S->V * c.dt_d;
+            S->center[ax] = (float)S->center_d[ax];
+            S->Hd2 = S->sized2[ax];
+            S->Strain = (S->size_d[ax] - S->Size0) / S->Size0;
+            S->steps += 1;                                    // the specimen's own step count
+            const bool running = (S->Strain < S->MaxStrain) && !S->Fracture;
+            S->done = running ? 0u : 1u;
+        }
+        __syncthreads();
+        if (!S->done) all_done = false;
+    }
+    if (threadIdx.x != 0) return;
+    sc->block_counter = 0;
+    if (d.nspec > 1) sc->steps += 1;                          // (with one specimen sc == spec)
+    sc->done = all_done ? 1u : 0u;
+    const uint32_t mv = sc->moved;
+    sc->moved = 0;
+    sc->rebuild = mv;
+    if (c.use_graph) {
+        cudaGraphSetConditional(c.h_rebuild, mv ? 1u : 0u);
+        cudaGraphSetConditional(c.h_loop, (!all_done && sc->steps < sc->target) ? 1u : 0u);
+    }
+}
+
 #define FIRE_SUMS 9     // F.v + M.w, |F|^2, |v|^2, |M|^2, |w|^2, sum |f_n|, pair count, platen sums (2)
 
 template <int KIND>
@@ -799,12 +921,33 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
     const float4* __restrict__ Wv = d.ang[cur];
     const uint32_t N = c.N;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < N;
+    // specimen of this particle: the CTA's first one, or the next (each specimen has at
+    // least 128 particles, so a CTA touches at most two)
+    const uint32_t sA = d.blk_spec ? (uint32_t)d.blk_spec[blockIdx.x] : 0u;
+    const uint32_t sI = (i < N && i >= d.geom[sA].p1) ? sA + 1u : sA;
+    const SpecGeom& G = d.geom[sI];
+    const DevScalars* S = d.spec + sI;
+    // a finished specimen of a batch is frozen: its state is carried to the next buffer
+    const bool frozen = MODE == 0 && i < N && S->done != 0;
+    const bool valid = i < N && !frozen;
     const uint32_t FULL = 0xffffffffu;
-    const double Top = sc->Top, Bottom = sc->Bottom, TopR = sc->TopR, BottomR = sc->BottomR;
-    const float vt = MODE == 0 ? (float)sc->V : 0.f, RR = sc->RR;
+    const double Top = S->Top, Bottom = S->Bottom, TopR = S->TopR, BottomR = S->BottomR;
+    const float vt = MODE == 0 ? (float)S->V : 0.f, RR = S->RR;
     rf_float3 cc;
-    cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
+    cc.x = S->center[0]; cc.y = S->center[1]; cc.z = S->center[2];
+    if (frozen) {
+        d.posd[nxt][i] = P[i];
+        d.vel[nxt][i] = Vv[i];
+        d.ang[nxt][i] = Wv[i];
+        const float* oi = d.cO[cur] + (size_t)i * c.K * 3;
+        float* oo = d.cO[nxt] + (size_t)i * c.K * 3;
+        uint32_t m = d.cmask[i];
+        while (m) {
+            const uint32_t k = __ffs(m) - 1;
+            m &= m - 1;
+            oo[3 * k] = oi[3 * k]; oo[3 * k + 1] = oi[3 * k + 1]; oo[3 * k + 2] = oi[3 * k + 2];
+        }
+    }
     ExtParams ep = c.ep;
     if (MODE == 1) {
         // FIRE minimises the conservative part of the model: its own velocity mixing
@@ -930,7 +1073,7 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
             const uint32_t free = ~live & (c.K >= 32 ? 0xffffffffu : ((1u << c.K) - 1u));
             if (!free) { raise_status(&sc->err, RF_ERR_ROW_OVERFLOW); continue; }
             uint32_t k;
-            if (i == 0 && (free & 1u) && (free & ~1u)) k = __ffs(free & ~1u) - 1;
+            if (i == G.p0 && (free & 1u) && (free & ~1u)) k = __ffs(free & ~1u) - 1;   // kdxfree==0 quirk
             else k = __ffs(free) - 1;
             const uint32_t j = (uint32_t)(best & 0xffffffffull);
             d.ids[(size_t)i * c.K + k] = j;
@@ -969,9 +1112,9 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         float Vx = vi.x, Vy = vi.y, Vz = vi.z;
         if (KIND == RF_TEST_BRAZIL)
             brazil_particle_ext(Rx, Ry, Rz, Vx, Vy, Vz, Fx, Fy, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt,
-                                (double)c.zcut, xi.w - c.p_r_d, sfb, sft);
+                                (double)G.zcut, xi.w - c.p_r_d, sfb, sft);
         else
-            uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)c.zcut,
+            uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)G.zcut,
                                   xi.w - c.p_r_d, sfb, sft);
         if (MODE == 1) {
             // FIRE: keep the clamped state for the update kernel; reduce the FIRE sums
@@ -996,10 +1139,10 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         Vx += Fx * dtm; Vy += Fy * dtm; Vz += Fz * dtm;
         Rx += (double)(Vx * ep.dt); Ry += (double)(Vy * ep.dt); Rz += (double)(Vz * ep.dt);
         const float Wx = wi.x + Mx * dtI, Wy = wi.y + My * dtI, Wz = wi.z + Mz * dtI;
-        const double dx = Rx - c.box_c.x, dy = Ry - c.box_c.y, dz = Rz - c.box_c.z;
-        if ((dx - c.box_h.x > 0) || (dx + c.box_h.x < 0) || (dy - c.box_h.y > 0) || (dy + c.box_h.y < 0) ||
-            (dz - c.box_h.z > 0) || (dz + c.box_h.z < 0)) {
-            Rx = c.hp.x; Ry = c.hp.y; Rz = c.hp.z;
+        const double dx = Rx - G.box_c.x, dy = Ry - G.box_c.y, dz = Rz - G.box_c.z;
+        if ((dx - G.box_h.x > 0) || (dx + G.box_h.x < 0) || (dy - G.box_h.y > 0) || (dy + G.box_h.y < 0) ||
+            (dz - G.box_h.z > 0) || (dz + G.box_h.z < 0)) {
+            Rx = G.hp.x; Ry = G.hp.y; Rz = G.hp.z;
             Vx = 0.f; Vy = 0.f; Vz = 0.f;
         }
         d.posd[nxt][i] = make_double4(Rx, Ry, Rz, xi.w);
@@ -1011,7 +1154,7 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         }
     }
     if (MODE == 0) {
-        step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
+        step_finish_ext<KIND>(d, c, sfb, sft, nbroken, moved, sI - sA);
     } else {
         const uint32_t nb = __reduce_add_sync(FULL, nbroken);
         if ((threadIdx.x & 31) == 0 && nb) atomicAdd(&sc->broken, (unsigned long long)nb);
@@ -1484,13 +1627,24 @@ __device__ __forceinline__ double pair_uniform(uint64_t seed, uint32_t a, uint32
     const uint64_t h = mix64(mix64(seed ^ (0x51ED270B27F3A4C1ull * (stream + 1))) + (hi << 32 | lo));
     return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);       // in (0, 1)
 }
+// Bond rule and strength distribution of one specimen of a batch.
+struct BondSpec {
+    double gap_frac, wm, sig, tau;
+    uint64_t seed;
+    uint32_t p0, p1;            // its particles
+};
 __global__ void k_bond_ext(const double4* __restrict__ P, const uint_fast32_t* __restrict__ IL,
                            uint8_t* __restrict__ type, float* __restrict__ iL, double* __restrict__ L0x,
-                           float2* __restrict__ strx, uint32_t N, uint32_t K, double gap_frac, double wm,
-                           double sig, double tau, uint64_t seed) {
+                           float2* __restrict__ strx, uint32_t N, uint32_t K, const BondSpec* __restrict__ bs,
+                           uint32_t nspec) {
     const uint_fast32_t E = empty_id<uint_fast32_t>();
-    const double inv_m = 1.0 / wm;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        uint32_t sp = 0;
+        while (sp + 1 < nspec && i >= bs[sp].p1) ++sp;
+        const double gap_frac = bs[sp].gap_frac, sig = bs[sp].sig, tau = bs[sp].tau;
+        const double inv_m = 1.0 / bs[sp].wm;
+        const uint64_t seed = bs[sp].seed;
+        const uint32_t pbase = bs[sp].p0;       // strengths keyed on specimen-local ids
         const double4 xi = P[i];
         for (uint32_t k = 0; k < K; ++k) {
             const size_t r = (size_t)i * K + k;
@@ -1504,7 +1658,8 @@ __global__ void k_bond_ext(const double4* __restrict__ P, const uint_fast32_t* _
             type[r] = 1;
             iL[r] = (float)(1.0 / L);
             L0x[r] = L;
-            const double us = pair_uniform(seed, i, (uint32_t)j, 0), ut = pair_uniform(seed, i, (uint32_t)j, 1);
+            const uint32_t li = i - pbase, lj = (uint32_t)j - pbase;
+            const double us = pair_uniform(seed, li, lj, 0), ut = pair_uniform(seed, li, lj, 1);
             strx[r] = make_float2((float)(sig * pow(-log(us), inv_m)), (float)(tau * pow(-log(ut), inv_m)));
         }
     }
@@ -1592,6 +1747,10 @@ struct rf_engine {
     float* staging;
     uint64_t bonds_initial;
     uint32_t* maxq_dev;
+    // batch of specimens
+    std::vector<rf_task> spec_tasks;   // per specimen, shifted, with the batch's cell grid
+    std::vector<uint32_t> spec_p0, spec_n;
+    std::vector<double> spec_xoff;
     // FIRE relaxation graph (built on the first load increment)
     Consts cf;
     cudaGraph_t fgraph;
@@ -1800,8 +1959,35 @@ extern "C" size_t md_CellDistributionScratchBytes(uint_fast32_t N, uint_fast32_t
 
 namespace {
 
+// Host description of a batch: per-specimen tasks (shifted, with the batch's grid), bond
+// parameters and particle ranges.
+struct BatchIn {
+    std::vector<rf_task> tasks;
+    std::vector<rf_ext_params> xs;
+    std::vector<uint32_t> p0, n;
+    std::vector<double> xoff;
+};
+
+void fill_scalars(DevScalars& h, const rf_task& t) {
+    std::memset(&h, 0, sizeof(h));
+    const rf_compression& K_ = t.Compress;
+    h.V = K_.V; h.VLoad = K_.VLoad; h.Top = K_.Top; h.Bottom = K_.Bottom; h.TopR = K_.TopR; h.BottomR = K_.BottomR;
+    h.FractureStress = K_.FractureStress; h.FractureStrain = K_.FractureStrain; h.MinStress = K_.MinStress;
+    h.ZeroStress = K_.ZeroStress; h.Stress = K_.Stress; h.Strain = K_.Strain; h.MaxStrain = K_.MaxStrain;
+    h.Size0 = K_.Size0;
+    h.size_d[0] = K_.size_d.x; h.size_d[1] = K_.size_d.y; h.size_d[2] = K_.size_d.z;
+    h.center_d[0] = K_.center_d.x; h.center_d[1] = K_.center_d.y; h.center_d[2] = K_.center_d.z;
+    h.sz0 = t.sz0 != 0.0 ? t.sz0 : (double)K_.size.z;
+    h.center[0] = K_.center.x; h.center[1] = K_.center.y; h.center[2] = K_.center.z;
+    h.size[0] = K_.size.x; h.size[1] = K_.size.y; h.size[2] = K_.size.z;
+    h.sized2[0] = K_.sized2.x; h.sized2[1] = K_.sized2.y; h.sized2[2] = K_.sized2.z;
+    h.RR = K_.RR; h._1d_Area = K_._1d_Area; h.Hd2 = K_.Hd2;
+    h.Loading = K_.Loading; h.Fracture = K_.Fracture;
+    h.done = (K_.Strain < K_.MaxStrain && !K_.Fracture) ? 0u : 1u;
+}
+
 rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h_Rd, const double* h_rad,
-                             const rf_ext_params* x, rf_engine** out) {
+                             const rf_ext_params* x, rf_engine** out, const BatchIn* bin = nullptr) {
     const bool ext = x != nullptr;
     if (!t || !out || t->N == 0 || t->K == 0 || (ext ? (!h_Rd || !h_rad) : !h_R)) {
         set_error("rf_engine_create: bad arguments");
@@ -1876,7 +2062,8 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     if (cells >= 0x7FFFFFFFull) { set_error("rf_engine_create: candidate grid too large"); return fail(RF_ERR_INVALID); }
     c.cg_cells = (uint32_t)cells;
     e->cg_nb = (uint32_t)((cells + 1 + 4095) / 4096);
-    c.curve_cap = 1u << 20;
+    const uint32_t nspec = bin ? (uint32_t)bin->tasks.size() : 1u;
+    c.curve_cap = nspec == 1 ? (1u << 20) : std::max(4096u, (1u << 20) / nspec);   // records per specimen
     e->nblocks = (N + 127) / 128;
 
     Dev& d = e->d;
@@ -1894,13 +2081,58 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
         (st = dalloc(e, &d.cg_start, cells + 1)) || (st = dalloc(e, &d.cg_fill, cells + 1)) ||
         (st = dalloc(e, &d.cg_bsum, e->cg_nb)) || (st = dalloc(e, &d.cg_sorted, N)) ||
-        (st = dalloc(e, &d.partial, e->nblocks)) || (st = dalloc(e, &d.curve, 3 * (size_t)c.curve_cap)) ||
+        (st = dalloc(e, &d.partial, e->nblocks)) || (st = dalloc(e, &d.partial2, e->nblocks)) ||
+        (st = dalloc(e, &d.curve, 3 * (size_t)c.curve_cap * nspec)) ||
         (st = dalloc(e, &d.sc, 1)) || (st = dalloc(e, &e->counters_dev, 4)))
         return fail(st);
     cudaStream_t s = e->stream;
     for (int b = 0; b < 2; ++b) {
         if (cudaMemsetAsync(d.vel[b], 0, N * sizeof(float4), s) || cudaMemsetAsync(d.ang[b], 0, N * sizeof(float4), s))
             return fail(cuda_status(cudaGetLastError(), "memset"));
+    }
+    // specimens: geometry, CTA -> specimen map, per-specimen scalars
+    d.nspec = nspec;
+    {
+        std::vector<SpecGeom> hg(nspec);
+        for (uint32_t q = 0; q < nspec; ++q) {
+            const rf_task& ts = bin ? bin->tasks[q] : *t;
+            SpecGeom& G = hg[q];
+            G.zcut = (t->kind == RF_TEST_BRAZIL) ? (float)((double)ts.S.center.y + (double)ts.S.spacesized2.y)
+                                                 : (float)((double)ts.S.center.z + (double)ts.S.spacesized2.z);
+            G.box_c = ts.S.center; G.box_h = ts.S.spacesized2; G.hp = ts.S.hidenpoint;
+            G.p0 = bin ? bin->p0[q] : 0u;
+            G.p1 = bin ? bin->p0[q] + bin->n[q] : N;
+            G.b0 = G.p0 / 128; G.b1 = (G.p1 - 1) / 128;
+        }
+        SpecGeom* dg = nullptr;
+        if ((st = dalloc(e, &dg, nspec))) return fail(st);
+        if (cudaMemcpyAsync(dg, hg.data(), nspec * sizeof(SpecGeom), cudaMemcpyHostToDevice, s)) return fail(RF_ERR_CUDA);
+        d.geom = dg;
+        d.blk_spec = nullptr;
+        if (nspec > 1) {
+            std::vector<uint16_t> hb(e->nblocks);
+            uint32_t q = 0;
+            for (uint32_t b = 0; b < e->nblocks; ++b) {
+                while (q + 1 < nspec && hg[q].p1 <= b * 128u) ++q;
+                hb[b] = (uint16_t)q;
+            }
+            uint16_t* db = nullptr;
+            if ((st = dalloc(e, &db, e->nblocks))) return fail(st);
+            if (cudaMemcpyAsync(db, hb.data(), e->nblocks * sizeof(uint16_t), cudaMemcpyHostToDevice, s))
+                return fail(RF_ERR_CUDA);
+            d.blk_spec = db;
+            if ((st = dalloc(e, &d.spec, nspec))) return fail(st);
+            std::vector<DevScalars> hs(nspec);
+            for (uint32_t k = 0; k < nspec; ++k) fill_scalars(hs[k], bin->tasks[k]);
+            if (cudaMemcpyAsync(d.spec, hs.data(), nspec * sizeof(DevScalars), cudaMemcpyHostToDevice, s))
+                return fail(RF_ERR_CUDA);
+            e->spec_tasks = bin->tasks;
+            e->spec_p0 = bin->p0;
+            e->spec_n = bin->n;
+            e->spec_xoff = bin->xoff;
+        } else {
+            d.spec = d.sc;
+        }
     }
     // the scalar block is read (step parity) by the row import below: start it at zero
     if (cudaMemsetAsync(d.member, 0, N * sizeof(unsigned long long), s) || cudaMemsetAsync(d.cand_n, 0, N * 4, s) ||
@@ -1960,9 +2192,21 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         if (!st2 && !ext) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
                                                               Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
         if (!st2 && ext) {
-            k_bond_ext<<<(N + 127) / 128, 128, 0, s>>>(d.posd[0], dIL, dT, dIL_f, dL0, dStr, N, K, x->gap_frac,
-                                                       x->weibull_m, x->sigma_c, x->tau_c, x->seed);
-            ce = cudaGetLastError();
+            std::vector<BondSpec> hbs(nspec);
+            for (uint32_t q = 0; q < nspec; ++q) {
+                const rf_ext_params& xq = bin ? bin->xs[q] : *x;
+                hbs[q] = BondSpec{xq.gap_frac, xq.weibull_m, xq.sigma_c, xq.tau_c, xq.seed, bin ? bin->p0[q] : 0u,
+                                  bin ? bin->p0[q] + bin->n[q] : N};
+            }
+            BondSpec* dbs = nullptr;
+            ce = cudaMalloc(&dbs, nspec * sizeof(BondSpec));
+            if (!ce) ce = cudaMemcpyAsync(dbs, hbs.data(), nspec * sizeof(BondSpec), cudaMemcpyHostToDevice, s);
+            if (!ce) {
+                k_bond_ext<<<(N + 127) / 128, 128, 0, s>>>(d.posd[0], dIL, dT, dIL_f, dL0, dStr, N, K, dbs, nspec);
+                ce = cudaGetLastError();
+            }
+            if (!ce) ce = cudaStreamSynchronize(s);
+            cudaFree(dbs);
             if (ce) st2 = cuda_status(ce, "k_bond_ext");
         }
         if (!st2) st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
@@ -1995,23 +2239,17 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         st = init_dev;
     }
 
-    // scalar state
+    // scalar state (with one specimen the global block is also the specimen's)
     DevScalars h;
-    std::memset(&h, 0, sizeof(h));
-    const rf_compression& K_ = t->Compress;
-    h.V = K_.V; h.VLoad = K_.VLoad; h.Top = K_.Top; h.Bottom = K_.Bottom; h.TopR = K_.TopR; h.BottomR = K_.BottomR;
-    h.FractureStress = K_.FractureStress; h.FractureStrain = K_.FractureStrain; h.MinStress = K_.MinStress;
-    h.ZeroStress = K_.ZeroStress; h.Stress = K_.Stress; h.Strain = K_.Strain; h.MaxStrain = K_.MaxStrain;
-    h.Size0 = K_.Size0;
-    h.size_d[0] = K_.size_d.x; h.size_d[1] = K_.size_d.y; h.size_d[2] = K_.size_d.z;
-    h.center_d[0] = K_.center_d.x; h.center_d[1] = K_.center_d.y; h.center_d[2] = K_.center_d.z;
-    h.sz0 = t->sz0 != 0.0 ? t->sz0 : (double)K_.size.z;
-    h.center[0] = K_.center.x; h.center[1] = K_.center.y; h.center[2] = K_.center.z;
-    h.size[0] = K_.size.x; h.size[1] = K_.size.y; h.size[2] = K_.size.z;
-    h.sized2[0] = K_.sized2.x; h.sized2[1] = K_.sized2.y; h.sized2[2] = K_.sized2.z;
-    h.RR = K_.RR; h._1d_Area = K_._1d_Area; h.Hd2 = K_.Hd2;
-    h.Loading = K_.Loading; h.Fracture = K_.Fracture;
-    h.done = (K_.Strain < K_.MaxStrain && !K_.Fracture) ? 0u : 1u;
+    fill_scalars(h, *t);
+    if (nspec > 1) {
+        h.done = 0;
+        for (uint32_t q = 0; q < nspec; ++q) {
+            const rf_compression& Kq = bin->tasks[q].Compress;
+            if (Kq.Strain < Kq.MaxStrain && !Kq.Fracture) break;
+            if (q + 1 == nspec) h.done = 1;
+        }
+    }
     h.rebuild = 1;
     h.err = (uint32_t)st;
     if (cudaMemcpyAsync(d.sc, &h, sizeof(h), cudaMemcpyHostToDevice, s) || cudaStreamSynchronize(s))
@@ -2043,6 +2281,88 @@ rf_status rf_engine_create_ext(const rf_task* t, const rf_ext_params* x, const d
                                rf_engine** out) {
     if (!x) { set_error("rf_engine_create_ext: null parameters"); return RF_ERR_INVALID; }
     return engine_create_impl(t, nullptr, h_R, h_radius, x, out);
+}
+
+rf_status rf_engine_create_batch(const rf_task* tasks, const rf_ext_params* xs, const double* const* h_R,
+                                 const double* const* h_radius, int nspec, rf_engine** out) {
+    if (!tasks || !xs || !h_R || !h_radius || !out || nspec < 1 || nspec > 65535) {
+        set_error("rf_engine_create_batch: bad arguments");
+        return RF_ERR_INVALID;
+    }
+    const rf_task& t0 = tasks[0];
+    uint64_t total = 0;
+    for (int q = 0; q < nspec; ++q) {
+        const rf_task& tq = tasks[q];
+        if (!h_R[q] || !h_radius[q] || tq.N < 128 || tq.kind != t0.kind || tq.K != t0.K || tq.C.a != t0.C.a ||
+            tq.aacut != t0.aacut || tq.Po.dt != t0.Po.dt || tq.Po.p_r != t0.Po.p_r ||
+            tq.Po.aa_farcut != t0.Po.aa_farcut || tq.Po.hm_E != t0.Po.hm_E || tq.Po.hm_G != t0.Po.hm_G ||
+            tq.Po.p_A != t0.Po.p_A || tq.Po.p_mu != t0.Po.p_mu || tq.Po.p_mur != t0.Po.p_mur ||
+            tq.Po.p_m != t0.Po.p_m || xs[q].kn != xs[0].kn || xs[q].ks != xs[0].ks ||
+            xs[q].bond_lambda != xs[0].bond_lambda) {
+            set_error("rf_engine_create_batch: specimen %d must have >= 128 particles and the batch's test kind, "
+                      "slots, grid cell, material, time step and bond stiffness", q);
+            return RF_ERR_INVALID;
+        }
+        total += tq.N;
+    }
+    if (total >= 0xFFFFFFFFull) { set_error("rf_engine_create_batch: too many particles"); return RF_ERR_INVALID; }
+    // lay the specimens out along x, each shifted by a whole number of cells so that its
+    // cell-relative geometry (and so its insertion order) is what it would be alone,
+    // with two cells between neighbouring boxes (no cross-specimen links)
+    const double a = (double)t0.C.a;
+    BatchIn bin;
+    bin.tasks.resize(nspec); bin.xs.assign(xs, xs + nspec); bin.p0.resize(nspec); bin.n.resize(nspec);
+    bin.xoff.resize(nspec);
+    double cursor = 0.0, Bx = 0.0, By = 0.0, Bz = 0.0, lo_y = 1e300, lo_z = 1e300, hi_y = -1e300, hi_z = -1e300;
+    uint32_t p = 0;
+    for (int q = 0; q < nspec; ++q) {
+        const rf_sample& S = tasks[q].S;
+        const double lo = (double)S.center.x - (double)S.spacesized2.x, hi = (double)S.center.x + (double)S.spacesized2.x;
+        const double off = q == 0 ? 0.0 : std::ceil((cursor - lo) / a) * a;
+        bin.xoff[q] = off;
+        cursor = hi + off + 2.0 * a;
+        rf_task tq = tasks[q];
+        tq.S.center.x = (float)((double)S.center.x + off);
+        tq.S.A.x = (float)((double)S.A.x + off); tq.S.B.x = (float)((double)S.B.x + off);
+        tq.S.hidenpoint.x = (float)((double)S.hidenpoint.x + off);
+        tq.S.center_real.x += off; tq.S.A_real.x += off; tq.S.B_real.x += off;
+        tq.Compress.center_d.x += off;
+        tq.Compress.center.x = (float)tq.Compress.center_d.x;
+        bin.tasks[q] = tq;
+        bin.p0[q] = p; bin.n[q] = (uint32_t)tq.N;
+        p += (uint32_t)tq.N;
+        Bx = std::max(Bx, (double)tq.S.B.x); By = std::max(By, (double)S.B.y); Bz = std::max(Bz, (double)S.B.z);
+        lo_y = std::min(lo_y, (double)S.center.y - (double)S.spacesized2.y);
+        hi_y = std::max(hi_y, (double)S.center.y + (double)S.spacesized2.y);
+        lo_z = std::min(lo_z, (double)S.center.z - (double)S.spacesized2.z);
+        hi_z = std::max(hi_z, (double)S.center.z + (double)S.spacesized2.z);
+    }
+    // the batch's cell grid covers every box (cell_data::CalculateParameters on the union corner)
+    rf_cells C = t0.C;
+    C.Nr.x = (unsigned)(std::floor((float)(Bx * (double)C._1d_a)) + 1.0f);
+    C.Nr.y = (unsigned)(std::floor((float)(By * (double)C._1d_a)) + 1.0f);
+    C.Nr.z = (unsigned)(std::floor((float)(Bz * (double)C._1d_a)) + 3.0f);
+    C.N = (uint64_t)C.Nr.x * C.Nr.y * C.Nr.z;
+    for (int q = 0; q < nspec; ++q) bin.tasks[q].C = C;
+    rf_task tc = bin.tasks[0];
+    tc.N = total;
+    tc.C = C;
+    const double lo_x = (double)bin.tasks[0].S.center.x - (double)bin.tasks[0].S.spacesized2.x;
+    const double hi_x = (double)bin.tasks[nspec - 1].S.center.x + (double)bin.tasks[nspec - 1].S.spacesized2.x;
+    tc.S.center = rf_float3{(float)(0.5 * (lo_x + hi_x)), (float)(0.5 * (lo_y + hi_y)), (float)(0.5 * (lo_z + hi_z))};
+    tc.S.spacesized2 = rf_float3{(float)(0.5 * (hi_x - lo_x)), (float)(0.5 * (hi_y - lo_y)), (float)(0.5 * (hi_z - lo_z))};
+    tc.bloks = total / 1024 + 1;
+    std::vector<double> R(3 * total), rad(total);
+    for (int q = 0; q < nspec; ++q) {
+        const uint64_t n = tasks[q].N, p0 = bin.p0[q];
+        for (uint64_t i = 0; i < n; ++i) {
+            R[p0 + i] = h_R[q][i] + bin.xoff[q];
+            R[total + p0 + i] = h_R[q][n + i];
+            R[2 * total + p0 + i] = h_R[q][2 * n + i];
+            rad[p0 + i] = h_radius[q][i];
+        }
+    }
+    return engine_create_impl(&tc, nullptr, R.data(), rad.data(), &xs[0], out, &bin);
 }
 
 rf_status rf_engine_positions_f64(rf_engine* e, double* R) {
@@ -2109,6 +2429,7 @@ rf_status load_increment(rf_engine* e, const rf_relax_params* p, const float* wa
                          rf_relax_result* r) {
     if (!e || !p) { set_error("rf_engine_load_increment: bad arguments"); return RF_ERR_INVALID; }
     if (!e->c.ext) { set_error("rf_engine_load_increment: quasi-static relaxation needs the extended model"); return RF_ERR_STATE; }
+    if (e->d.nspec > 1) { set_error("rf_engine_load_increment: quasi-static relaxation runs one specimen per engine"); return RF_ERR_STATE; }
     if (!(p->dt0 > 0) || !(p->dt_max >= p->dt0) || !(p->dt_min > 0) || !(p->dt_min <= p->dt0) || !(p->tol > 0) ||
         p->max_iter == 0 || !(p->alpha0 >= 0 && p->alpha0 < 1) || !(p->f_inc >= 1) || !(p->f_dec > 0 && p->f_dec < 1)) {
         set_error("rf_engine_load_increment: bad FIRE parameters");
@@ -2167,7 +2488,7 @@ rf_status rf_engine_load_increment_pred(rf_engine* e, const rf_relax_params* p, 
 
 rf_status rf_engine_warm_features(rf_engine* e, double strain_inc, void* feat) {
     if (!e || !feat || !(strain_inc > 0)) { set_error("rf_engine_warm_features: bad arguments"); return RF_ERR_INVALID; }
-    if (!e->c.ext) { set_error("rf_engine_warm_features: needs the extended model"); return RF_ERR_STATE; }
+    if (!e->c.ext || e->d.nspec > 1) { set_error("rf_engine_warm_features: needs a one-specimen extended-model engine"); return RF_ERR_STATE; }
     if (rf_status st = fire_setup(e)) return st;
     const uint32_t N = e->c.N, rows = (N + 127) / 128 * 128;
     cudaStream_t s = e->stream;
@@ -2262,13 +2583,14 @@ rf_status rf_engine_step_host(rf_engine* e, const float* h_R_in, uint64_t nsteps
     return RF_OK;
 }
 
-rf_status rf_engine_sync(rf_engine* e, rf_task* t_out, rf_run_result* r_out) {
-    if (!e) { set_error("rf_engine_sync: null engine"); return RF_ERR_INVALID; }
-    DevScalars h;
-    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+rf_status rf_engine_sync_spec(rf_engine* e, int spec, rf_task* t_out, rf_run_result* r_out) {
+    if (!e || spec < 0 || (uint32_t)spec >= e->d.nspec) { set_error("rf_engine_sync_spec: bad arguments"); return RF_ERR_INVALID; }
+    DevScalars h, g;
+    RF_CUDA(cudaMemcpyAsync(&h, e->d.spec + spec, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+    RF_CUDA(cudaMemcpyAsync(&g, e->d.sc, sizeof(g), cudaMemcpyDeviceToHost, e->stream));
     RF_CUDA(cudaStreamSynchronize(e->stream));
     if (t_out) {
-        *t_out = e->task;
+        *t_out = e->d.nspec > 1 ? e->spec_tasks[spec] : e->task;
         rf_compression& K = t_out->Compress;
         K.V = h.V; K.Top = h.Top; K.Bottom = h.Bottom; K.TopR = h.TopR; K.BottomR = h.BottomR;
         K.FractureStress = h.FractureStress; K.FractureStrain = h.FractureStrain; K.Stress = h.Stress;
@@ -2280,12 +2602,23 @@ rf_status rf_engine_sync(rf_engine* e, rf_task* t_out, rf_run_result* r_out) {
         K.center = rf_float3{h.center[0], h.center[1], h.center[2]};
     }
     if (r_out) {
-        r_out->steps = h.steps;
+        r_out->steps = h.steps;                  // the specimen's own steps (all steps for one specimen)
         r_out->FractureStress = h.FractureStress; r_out->FractureStrain = h.FractureStrain;
         r_out->Stress = h.Stress; r_out->Strain = h.Strain; r_out->Fracture = h.Fracture;
-        r_out->broken_bonds = h.broken;
+        r_out->broken_bonds = g.broken;          // of the whole engine
         r_out->bonds_initial = e->bonds_initial;
-        r_out->error = (rf_status)h.err;
+        r_out->error = (rf_status)g.err;
+    }
+    return RF_OK;
+}
+
+rf_status rf_engine_sync(rf_engine* e, rf_task* t_out, rf_run_result* r_out) {
+    if (!e) { set_error("rf_engine_sync: null engine"); return RF_ERR_INVALID; }
+    if (rf_status st = rf_engine_sync_spec(e, 0, t_out, r_out)) return st;
+    if (r_out && e->d.nspec > 1) {
+        DevScalars g;
+        RF_CUDA(cudaMemcpy(&g, e->d.sc, sizeof(g), cudaMemcpyDeviceToHost));
+        r_out->steps = g.steps;
     }
     return RF_OK;
 }
@@ -2400,17 +2733,35 @@ rf_status rf_engine_import(rf_engine* e, const float* R, const float* V, const f
     return RF_OK;
 }
 
-rf_status rf_engine_curve(rf_engine* e, double* curve, uint64_t cap, uint64_t* n) {
-    if (!e) { set_error("rf_engine_curve: null engine"); return RF_ERR_INVALID; }
+rf_status rf_engine_curve_spec(rf_engine* e, int spec, double* curve, uint64_t cap, uint64_t* n) {
+    if (!e || spec < 0 || (uint32_t)spec >= e->d.nspec) { set_error("rf_engine_curve: bad arguments"); return RF_ERR_INVALID; }
     DevScalars h;
     RF_CUDA(cudaStreamSynchronize(e->stream));
-    RF_CUDA(cudaMemcpy(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost));
+    RF_CUDA(cudaMemcpy(&h, e->d.spec + spec, sizeof(h), cudaMemcpyDeviceToHost));
     uint64_t m = h.curve_n < e->c.curve_cap ? h.curve_n : e->c.curve_cap;
     if (n) *n = h.curve_n;
     if (curve && cap) {
         if (m > cap) m = cap;
-        RF_CUDA(cudaMemcpy(curve, e->d.curve, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+        RF_CUDA(cudaMemcpy(curve, e->d.curve + 3 * (size_t)spec * e->c.curve_cap, 3 * m * sizeof(double),
+                           cudaMemcpyDeviceToHost));
     }
+    return RF_OK;
+}
+
+rf_status rf_engine_curve(rf_engine* e, double* curve, uint64_t cap, uint64_t* n) {
+    return rf_engine_curve_spec(e, 0, curve, cap, n);
+}
+
+int rf_engine_batch_size(rf_engine* e) { return e ? (int)e->d.nspec : 0; }
+
+rf_status rf_engine_spec_info(rf_engine* e, int spec, uint64_t* first, uint64_t* count, double* x_offset,
+                              rf_task* task) {
+    if (!e || spec < 0 || (uint32_t)spec >= e->d.nspec) { set_error("rf_engine_spec_info: bad arguments"); return RF_ERR_INVALID; }
+    const bool b = e->d.nspec > 1;
+    if (first) *first = b ? e->spec_p0[spec] : 0;
+    if (count) *count = b ? e->spec_n[spec] : e->c.N;
+    if (x_offset) *x_offset = b ? e->spec_xoff[spec] : 0.0;
+    if (task) *task = b ? e->spec_tasks[spec] : e->task;
     return RF_OK;
 }
 

@@ -167,6 +167,11 @@ _proto = {
     "rf_engine_uses_graph": (i32, [P]),
     "rf_engine_create_ext": (i32, [C.POINTER(Task), C.POINTER(ExtParams), P, P, C.POINTER(P)]),
     "rf_engine_positions_f64": (i32, [P, P]),
+    "rf_engine_create_batch": (i32, [C.POINTER(Task), C.POINTER(ExtParams), P, P, i32, C.POINTER(P)]),
+    "rf_engine_batch_size": (i32, [P]),
+    "rf_engine_spec_info": (i32, [P, i32, P, P, P, C.POINTER(Task)]),
+    "rf_engine_sync_spec": (i32, [P, i32, C.POINTER(Task), C.POINTER(RunResult)]),
+    "rf_engine_curve_spec": (i32, [P, i32, P, u64, P]),
     "rf_relax_default_params": (i32, [C.POINTER(RelaxParams), C.POINTER(Task)]),
     "rf_engine_load_increment": (i32, [P, C.POINTER(RelaxParams), P, C.POINTER(RelaxResult)]),
     "rf_engine_increment_fields": (i32, [P, P, P, P]),
@@ -541,3 +546,44 @@ class MLP:
             check(lib.rf_mlp_grad(self.h, l, gT.ctypes.data, gb.ctypes.data), "rf_mlp_grad")
             out.append((gT, gb))
         return out
+
+
+class BatchEngine(Engine):
+    """Several extended-model specimens advanced by one step kernel (rf_engine_create_batch)."""
+
+    def __init__(self, tasks, params, Rs, radii):
+        n = len(tasks)
+        self.tasks = (Task * n)(*tasks)
+        self.params = (ExtParams * n)(*params)
+        self._R = [np.ascontiguousarray(R, np.float64) for R in Rs]
+        self._rad = [np.ascontiguousarray(r, np.float64) for r in radii]
+        pR = (C.c_void_p * n)(*[R.ctypes.data for R in self._R])
+        pr = (C.c_void_p * n)(*[r.ctypes.data for r in self._rad])
+        h = P()
+        check(lib.rf_engine_create_batch(self.tasks, self.params, pR, pr, n, C.byref(h)), "rf_engine_create_batch")
+        self.h = h
+        self.ext = True
+        self.nspec = n
+        self.N = int(sum(t.N for t in tasks))
+        self.K = int(tasks[0].K)
+        self.task = tasks[0]
+
+    def spec_info(self, s):
+        first, count, off = C.c_uint64(0), C.c_uint64(0), C.c_double(0)
+        t = Task()
+        check(lib.rf_engine_spec_info(self.h, s, C.byref(first), C.byref(count), C.byref(off), C.byref(t)),
+              "rf_engine_spec_info")
+        return int(first.value), int(count.value), off.value, t
+
+    def sync_spec(self, s):
+        t, r = Task(), RunResult()
+        check(lib.rf_engine_sync_spec(self.h, s, C.byref(t), C.byref(r)), "rf_engine_sync_spec")
+        return t, r
+
+    def curve_spec(self, s):
+        n = C.c_uint64(0)
+        check(lib.rf_engine_curve_spec(self.h, s, None, 0, C.byref(n)), "rf_engine_curve_spec")
+        m = min(n.value, 1 << 20)
+        buf = np.zeros(3 * max(m, 1), np.float64)
+        check(lib.rf_engine_curve_spec(self.h, s, buf.ctypes.data, m, C.byref(n)), "rf_engine_curve_spec")
+        return buf[:3 * m].reshape(m, 3)

@@ -1,0 +1,78 @@
+"""Several extended-model specimens in one engine: each specimen of the batch must
+evolve exactly as the oracle's run of that specimen alone (on the batch's cell grid,
+shifted as the batch places it), and a specimen that finishes early is frozen while
+the others go on."""
+import numpy as np
+import pytest
+
+import extspec
+import mdcall as mc
+import oracle
+import rfdem
+
+pytestmark = pytest.mark.gpu
+
+
+def _specimens(short=None):
+    """Three lattice specimens; specimen `short` is pulled (platen moving outwards) so that
+    its strain reaches MaxStrain within a few tens of steps (under compression the
+    reference's Strain < MaxStrain test never ends a run)."""
+    out = []
+    for q, (d, h) in enumerate([(6.0, 10.0), (6.0, 8.0), (7.0, 10.0)]):
+        R0, rad = extspec.lattice_ext(rfdem.RF_TEST_UNIAXIAL, d, h, seed=0xB2000000 + 100 + q)
+        kw = dict(v_load=2e-4, max_strain=2e-4) if q == short else {}
+        t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, 0.5, min_stress=1e3, **kw)
+        x = extspec.stiff_params(seed=0xB2000000 + 200 + q, weibull_m=3.0 + 3.0 * q)
+        out.append((t, R, rad, x))
+    return out
+
+
+def _check_against_oracle(e, specs, steps_each):
+    Rall = e.positions_f64()
+    st = e.export()
+    Ntot = e.N
+    E = np.iinfo(np.uint64).max
+    for q, (t, R, rad, x) in enumerate(specs):
+        first, n, off, tq = e.spec_info(q)
+        assert n == int(t.N)
+        Rq = R.reshape(3, n).copy()
+        Rq[0] += off
+        o = oracle.run_ext(tq, x, Rq.reshape(-1), rad, steps_each[q])
+        assert o["steps"] == steps_each[q] and o["status"] == 0
+        Re = Rall.reshape(3, Ntot)[:, first:first + n].reshape(-1)
+        assert np.array_equal(Re, o["R"]), (q, np.abs(Re - o["R"]).max())
+        K = int(t.K)
+        IL = st["IL"].reshape(Ntot, K)[first:first + n].astype(np.uint64)
+        IL = np.where(IL == np.uint64(rfdem.EMPTY), E, IL - np.uint64(first))
+        assert np.array_equal(IL.reshape(-1), o["IL"]), q
+        assert np.array_equal(st["ILtype"].reshape(Ntot, K)[first:first + n].reshape(-1), o["ILtype"]), q
+        _, r = e.sync_spec(q)
+        assert r.steps == steps_each[q]
+
+
+def test_batch_matches_single_runs(cuda):
+    specs = _specimens()
+    e = rfdem.BatchEngine([s[0] for s in specs], [s[3] for s in specs], [s[1] for s in specs], [s[2] for s in specs])
+    assert rfdem.lib.rf_engine_batch_size(e.h) == 3
+    steps = 250
+    e.step(steps)
+    _check_against_oracle(e, specs, [steps] * 3)
+    e.close()
+
+
+def test_batch_specimen_finishing_early_is_frozen(cuda):
+    specs = _specimens(short=1)
+    # the specimen's own stop step, from the oracle
+    t1, R1, rad1, x1 = specs[1]
+    e = rfdem.BatchEngine([s[0] for s in specs], [s[3] for s in specs], [s[1] for s in specs], [s[2] for s in specs])
+    _, _, off, tq = e.spec_info(1)
+    Rq = R1.reshape(3, -1).copy()
+    Rq[0] += off
+    o = oracle.run_ext(tq, x1, Rq.reshape(-1), rad1, 10 ** 6)
+    stop = o["steps"]
+    assert 0 < stop < 200
+    e.step(200)
+    _check_against_oracle(e, specs, [200, stop, 200])
+    c1 = e.curve_spec(1)
+    assert c1.shape[0] == stop
+    e.close()

@@ -14,6 +14,8 @@ value : particle-steps/s of the fused engine, state resident in HBM, CUDA events
 e2e   : the same metric through the public API with host buffers: rf_engine_create_ext
         from pinned host positions and radii (bond construction included), the steps,
         and the FP64 positions read back.
+batch : 64 Brazilian discs of 5k-80k particles advanced by one step kernel
+        (rf_engine_create_batch) vs one engine per specimen, particle-steps/s of both.
 fire  : quasi-static load increments (strain 2.5e-5) of the same specimen relaxed by
         FIRE to a residual of 1e-6 x the mean normal pair force: plain FIRE vs FIRE
         warm-started by the MLP trained on plain-FIRE pairs of the same run; wall time
@@ -325,6 +327,66 @@ def run_fire(rfdem, torch, t, R, rad, x, seed):
             "warm_start_includes": "feature build + MLP forward (tcgen05 BF16) per load step"}
 
 
+BATCH_SPECIMENS, BATCH_STEPS = 64, 1000
+
+
+def run_batch(rfdem, torch, seed):
+    """configs[2]-style batch: BATCH_SPECIMENS Brazilian discs (thickness = D/2) with
+    particle counts log-uniform in [5k, 80k], radii U[0.8, 1.2] x 0.25 mm, Weibull
+    modulus U[3, 10] per specimen (own seed each), platens at 0.05 m/s, dt 1e-8 s; all
+    advanced by one step kernel per step (rf_engine_create_batch) vs the same specimens
+    one engine each, run one after the other. Particle-steps/s of both."""
+    import ctypes as C
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(5000), np.log(80000), BATCH_SPECIMENS)).astype(int)
+    ms = rng.uniform(3.0, 10.0, BATCH_SPECIMENS)
+    tasks, params, Rs, rads = [], [], [], []
+    t0 = time.perf_counter()
+    for q in range(BATCH_SPECIMENS):
+        R0, rad, D, H, mo = rfdem.pack_cylinder(int(counts[q]), R0_MM, aspect=0.5, phi=PHI, seed=seed + q)
+        t, R = rfdem.make_test_ext(rfdem.RF_TEST_BRAZIL, R0, rad, R0_MM, dt=0.01, v_load=-5e-5, max_strain=1.0)
+        x = rfdem.ext_params_si(weibull_m=float(ms[q]), seed=seed + 1000 + q)
+        tasks.append(t); params.append(x); Rs.append(R); rads.append(rad)
+    t_pack = time.perf_counter() - t0
+    ntot = int(sum(int(t.N) for t in tasks))
+    be = rfdem.BatchEngine(tasks, params, Rs, rads)
+    s = torch.cuda.ExternalStream(be.stream())
+    be.step(BATCH_STEPS)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(s)
+    for _ in range(3):
+        be.step(BATCH_STEPS)
+    b.record(s)
+    b.synchronize()
+    ms_batch = a.elapsed_time(b)
+    steps_done = [be.sync_spec(q)[1].steps for q in range(BATCH_SPECIMENS)]
+    be.close()
+    done_batch = sum(int(tasks[q].N) * (steps_done[q] - BATCH_STEPS) for q in range(BATCH_SPECIMENS))
+    ms_seq = 0.0
+    done_seq = 0
+    for q in range(BATCH_SPECIMENS):
+        e = rfdem.Engine(rfdem.Task.from_buffer_copy(tasks[q]), Rs[q], ext=params[q], radius=rads[q])
+        sq = torch.cuda.ExternalStream(e.stream())
+        e.step(100)
+        torch.cuda.synchronize()
+        a.record(sq)
+        e.step(BATCH_STEPS)
+        b.record(sq)
+        b.synchronize()
+        ms_seq += a.elapsed_time(b)
+        done_seq += int(tasks[q].N) * (e.counters()["steps"] - 100)
+        e.close()
+    v_b = done_batch / (ms_batch * 1e-3)
+    v_s = done_seq / (ms_seq * 1e-3)
+    return {"workload": "%d Brazilian discs, %d particles in all (%d to %d each, log-uniform), own seeds and "
+                        "Weibull moduli U[3,10]" % (BATCH_SPECIMENS, ntot, int(counts.min()), int(counts.max())),
+            "batched_particle_steps_per_s": v_b, "one_engine_each_particle_steps_per_s": v_s,
+            "speedup_batched": v_b / v_s, "batched_ms_per_step": ms_batch / (3 * BATCH_STEPS),
+            "packing_s": t_pack, "specimens_finished_early": int(sum(1 for q in range(BATCH_SPECIMENS)
+                                                                     if steps_done[q] < 4 * BATCH_STEPS))}
+
+
 def run_engine(args):
     import torch
     rank, ws, dist = dist_init()
@@ -411,6 +473,10 @@ def run_engine(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_port_sample(t, x, R, rad)
 
+    batch = None
+    if rank == 0 and ws == 1 and not args.no_batch:
+        batch = run_batch(rfdem, torch, 0xB2000000 + 4000)
+
     fire = None
     if rank == 0 and ws == 1 and not args.no_fire:
         fire = run_fire(rfdem, torch, t, R, rad, x, 0xB2000000 + 3000)
@@ -437,6 +503,7 @@ def run_engine(args):
            "rebuilds": rebuilds,
            "clocks": r["clocks"],
            "fire": fire,
+           "batch": batch,
            "reference_model": refmodel}
     print(json.dumps(out))
     if dist is not None:
@@ -473,6 +540,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the driver-call leg (profiling runs)")
     ap.add_argument("--no-fire", action="store_true", help="skip the quasi-static FIRE comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-specimen comparison")
     ap.add_argument("--explicit-steps", type=int, default=STEPS_PER_BENCH_STEP,
                     help="explicit steps per bench step (profiling runs use fewer)")
     ap.add_argument("--no-reference-model", action="store_true", help="skip the reference-model line")

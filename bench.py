@@ -247,6 +247,7 @@ def run_explicit(rfdem, torch, t, R, rad, x, args, dist, stream_of):
     N = int(t.N)
     e = rfdem.Engine(t, R, ext=x, radius=rad)
     stream = torch.cuda.ExternalStream(e.stream())
+    tuned = e.autotune(200)            # trial steps on a snapshot, state restored
     for _ in range(args.warmup):
         e.step(S)
     torch.cuda.synchronize()
@@ -274,7 +275,7 @@ def run_explicit(rfdem, torch, t, R, rad, x, args, dist, stream_of):
         raise SystemExit("bench: the specimen finished early (%d of %d steps)" % (done_steps, S * args.steps))
     graph = e.uses_graph()
     e.close()
-    return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, error=res.error)
+    return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, error=res.error, tuned=tuned)
 
 
 FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 1, 2, 4
@@ -489,7 +490,9 @@ def run_engine(args):
                       "explicit_steps_per_bench_step": S, "slots_K": K,
                       "bonds_per_particle": round(bbar, 3), "contacts_per_particle": round(cbar, 3),
                       "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 16 + N * 300 + c1["bonds"] * 129) / 1e6),
-                      "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": r["graph"]},
+                      "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": r["graph"],
+                      "autotune": {"ctas_per_sm": r["tuned"][0],
+                                   "ms_per_200_steps_for_6_5_4": [round(v, 3) for v in r["tuned"][1]]}},
            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * N,
                    "d2h_bytes_per_step": 24 * N,
                    "path": "rf_engine_create_ext (host positions + radii, bond build) + %d explicit steps + "

@@ -470,6 +470,15 @@ rf_status rf_engine_curve(rf_engine* e, double* curve, uint64_t cap, uint64_t* n
    [3] live contact slots, [4] occupied slots; all as of the last sync. */
 rf_status rf_engine_counters(rf_engine* e, uint64_t* out, int n);
 
+/* Autotuner (extended model): times `steps` explicit steps with each compiled variant of
+   the step kernel (register caps for 6, 5 and 4 resident 128-thread CTAs per SM) on a
+   snapshot of the engine's state, restores the state, and keeps the fastest variant
+   for the step graph. All variants compute identical results. *choice: CTAs per SM of
+   the pick; ms_out[3] (may be NULL): time of each variant for 6, 5, 4. The reference
+   model's step has a single variant (choice 6, no timing). Needs a second copy of the
+   engine's device memory while it runs. */
+rf_status rf_engine_autotune(rf_engine* e, int steps, int* choice, float* ms_out);
+
 /* Kernel launches the engine issues per explicit step when no rebuild runs. */
 int rf_engine_launches_per_step(void);
 /* The stream the engine launches on (cudaStream_t), for callers that time or order work. */

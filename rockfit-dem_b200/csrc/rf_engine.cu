@@ -40,6 +40,10 @@
 #define RF_STEP_MIN_BLOCKS 6      // resident 128-thread CTAs per SM the step kernel is compiled for
 #endif
 
+#ifndef RF_GRAPH_UNROLL
+#define RF_GRAPH_UNROLL 8         // explicit steps per iteration of the graph's WHILE loop
+#endif
+
 namespace rf {
 
 // Scalar state of the run, device resident (compression_data + result bookkeeping).
@@ -75,7 +79,7 @@ struct Consts {
     float cg_inv_h;
     float cg_ox, cg_oy, cg_oz;
     uint32_t cg_nx, cg_ny, cg_nz, cg_cells;
-    float rc2, disp2;
+    float rc2, disp2, hard2;   // rebuild trigger and the displacement the candidate lists cover
     unsigned long long curve_cap;
     cudaGraphConditionalHandle h_loop, h_rebuild;
     int use_graph;
@@ -480,7 +484,7 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
     // which runs after every block has passed this point and advances the step
     // counter towards the target, sets it again, so the device loop always ends.
     if (c.use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c.h_loop, 0u);
-    if (sc->done) return;
+    if (sc->done || sc->steps >= sc->target) return;
     const uint32_t cur = (uint32_t)(sc->steps & 1ull), nxt = cur ^ 1u;
     const float4* __restrict__ P = d.pos[cur];
     const float4* __restrict__ Vv = d.vel[cur];
@@ -683,7 +687,10 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
         d.ang[nxt][i] = make_float4(Wx, Wy, Wz, 0.f);
         const float4 pr = d.pos_ref[i];
         const float ex = Rx - pr.x, ey = Ry - pr.y, ez = Rz - pr.z;
-        moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+        const float e2 = ex * ex + ey * ey + ez * ez;
+        moved = (e2 > c.disp2) ? 1u : 0u;
+        // lists may have missed a neighbour (a particle moved to the hidden point has none)
+        if (e2 > c.hard2 && !(Rx == c.hp.x && Ry == c.hp.y && Rz == c.hp.z)) raise_status(&d.sc->err, RF_ERR_CAPACITY);
     }
 
     step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
@@ -909,11 +916,13 @@ __device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c,
 // of one FIRE iteration: the same forces with the FIRE time step, platens at rest; net
 // force and moment are stored for k_fire_update and FP64 sums of the FIRE power, the
 // squared norms and the mean normal pair force are reduced for the FIRE decision.
-template <int KIND, int MODE>
-__global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Consts c) {
+// MINB: resident 128-thread CTAs per SM the kernel is compiled for (the register cap);
+// rf_engine_autotune picks among the compiled variants by timing them.
+template <int KIND, int MODE, int MINB = RF_STEP_MIN_BLOCKS>
+__global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     DevScalars* sc = d.sc;
     if (c.use_graph && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c.h_loop, 0u);
-    if (MODE == 0 && sc->done) return;
+    if (MODE == 0 && (sc->done || sc->steps >= sc->target)) return;
     if (MODE == 1 && sc->fstop) return;
     const uint32_t cur = (uint32_t)(sc->steps & 1ull), nxt = cur ^ 1u;
     const double4* __restrict__ P = d.posd[cur];
@@ -1150,7 +1159,11 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step_ext(Dev d, Con
         d.ang[nxt][i] = make_float4(Wx, Wy, Wz, 0.f);
         const float4 pr = d.pos_ref[i];
         const float ex = (float)Rx - pr.x, ey = (float)Ry - pr.y, ez = (float)Rz - pr.z;
-        moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+        const float e2 = ex * ex + ey * ey + ez * ez;
+        moved = (e2 > c.disp2) ? 1u : 0u;
+        // lists may have missed a neighbour (a particle moved to the hidden point has none)
+        if (e2 > c.hard2 && !(Rx == (double)G.hp.x && Ry == (double)G.hp.y && Rz == (double)G.hp.z))
+            raise_status(&d.sc->err, RF_ERR_CAPACITY);
         }
     }
     if (MODE == 0) {
@@ -1283,7 +1296,9 @@ __global__ void k_fire_update(Dev d, Consts c) {
         d.ang[cur][i] = w;
         const float4 pr = d.pos_ref[i];
         const float ex = (float)x.x - pr.x, ey = (float)x.y - pr.y, ez = (float)x.z - pr.z;
-        moved = (ex * ex + ey * ey + ez * ez > c.disp2) ? 1u : 0u;
+        const float e2 = ex * ex + ey * ey + ez * ez;
+        moved = (e2 > c.disp2) ? 1u : 0u;
+        if (e2 > c.hard2) raise_status(&d.sc->err, RF_ERR_CAPACITY);   // lists may have missed a neighbour
     }
     __shared__ bool s_last;
     __shared__ uint32_t s_m;
@@ -1743,6 +1758,8 @@ struct rf_engine {
     uint32_t cg_nb;
     bool graph_ok;
     std::vector<void*> allocs;
+    std::vector<size_t> alloc_bytes;
+    int step_minb = RF_STEP_MIN_BLOCKS;    // register-cap variant of the extended step (autotuned)
     unsigned long long* counters_dev;
     float* staging;
     uint64_t bonds_initial;
@@ -1764,15 +1781,25 @@ template <class T> rf_status dalloc(rf_engine* e, T** p, size_t n) {
     void* q = nullptr;
     RF_CUDA(cudaMalloc(&q, (n ? n : 1) * sizeof(T)));
     e->allocs.push_back(q);
+    e->alloc_bytes.push_back((n ? n : 1) * sizeof(T));
     *p = (T*)q;
     return RF_OK;
 }
 
 #define TRY(x) do { rf_status s__ = (x); if (s__ != RF_OK) return s__; } while (0)
 
+// Explicit extended-model step kernels compiled for 4, 5 or 6 CTAs per SM.
+void* ext_step_variant(bool brazil, int minb) {
+    switch (minb) {
+        case 4: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 4> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 4>;
+        case 5: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 5> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 5>;
+        default: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 6> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 6>;
+    }
+}
+
 void* step_kernel(const rf_engine* e) {
     const bool br = e->task.kind == RF_TEST_BRAZIL;
-    if (e->c.ext) return br ? (void*)k_step_ext<RF_TEST_BRAZIL, 0> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0>;
+    if (e->c.ext) return ext_step_variant(br, e->step_minb);
     return br ? (void*)k_step<RF_TEST_BRAZIL> : (void*)k_step<RF_TEST_UNIAXIAL>;
 }
 
@@ -1804,15 +1831,13 @@ rf_status build_graph(rf_engine* e) {
     cudaGraphNode_t wnode;
     RF_CUDA(cudaGraphAddNode(&wnode, g, &pro, 1, &wp));
     cudaGraph_t body = wp.conditional.phGraph_out[0];
-    // IF(rebuild) inside the loop body
-    cudaGraphNodeParams ip = {};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = e->c.h_rebuild;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    cudaGraphNode_t inode;
-    RF_CUDA(cudaGraphAddNode(&inode, body, nullptr, 0, &ip));
-    cudaGraph_t rb = ip.conditional.phGraph_out[0];
+    // The loop body is IF(rebuild) {rebuild kernels} followed by RF_GRAPH_UNROLL steps: the
+    // WHILE condition and the rebuild condition are evaluated once per RF_GRAPH_UNROLL
+    // steps (conditional nodes cost more than the kernels between them). The rebuild
+    // trigger is set at 0.3 of the skin so that the particles' motion over those steps
+    // stays within the 0.5 skin the candidate lists are complete for; a step that finds
+    // a particle beyond 0.5 skin reports RF_ERR_CAPACITY. A step whose step count has
+    // reached the target returns at once, so the target is kept exactly.
     const unsigned gN = (e->c.N + 255) / 256;
     const unsigned gC = (e->c.cg_cells + 1 + 255) / 256;
     struct { void* fn; unsigned grid, block; } seq[] = {
@@ -1821,17 +1846,29 @@ rf_status build_graph(rf_engine* e) {
         {(void*)k_rb_scan_apply, e->cg_nb, 1024}, {(void*)k_rb_scatter, gN, 256},
         {(void*)k_rb_cand, (e->c.N + 127) / 128, 128},
     };
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = e->c.h_rebuild;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    RF_CUDA(cudaGraphAddNode(&inode, body, nullptr, 0, &ip));
+    cudaGraph_t rb = ip.conditional.phGraph_out[0];
     cudaGraphNode_t prev = nullptr;
-    for (auto& s : seq) {
+    for (auto& q : seq) {
         cudaGraphNode_t n;
-        kp = kparams(s.fn, s.grid, s.block);
+        kp = kparams(q.fn, q.grid, q.block);
         RF_CUDA(cudaGraphAddKernelNode(&n, rb, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
         prev = n;
     }
-    cudaGraphNode_t step;
     void* fn = step_kernel(e);
-    kp = kparams(fn, e->nblocks, 128);
-    RF_CUDA(cudaGraphAddKernelNode(&step, body, &inode, 1, &kp));
+    cudaGraphNode_t last = inode;
+    for (int u = 0; u < RF_GRAPH_UNROLL; ++u) {
+        cudaGraphNode_t step;
+        kp = kparams(fn, e->nblocks, 128);
+        RF_CUDA(cudaGraphAddKernelNode(&step, body, &last, 1, &kp));
+        last = step;
+    }
     RF_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
     return RF_OK;
 }
@@ -2049,7 +2086,8 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     const double skin = 0.1 * acut;
     const double rc = acut + skin;
     c.rc2 = (float)(rc * rc);
-    c.disp2 = (float)((0.45 * skin) * (0.45 * skin));
+    c.disp2 = (float)((0.3 * skin) * (0.3 * skin));   // checked every RF_GRAPH_UNROLL steps
+    c.hard2 = (float)((0.5 * skin) * (0.5 * skin));
     const double hcell = rc * 1.0001;
     c.cg_inv_h = (float)(1.0 / hcell);
     c.cg_ox = (float)(t->S.center.x - t->S.spacesized2.x - hcell);
@@ -2533,6 +2571,86 @@ rf_status rf_engine_increment_fields(rf_engine* e, double* x0, double* dx, doubl
         if (dx) { dx[3 * i] = b[i].x - a[i].x; dx[3 * i + 1] = b[i].y - a[i].y; dx[3 * i + 2] = b[i].z - a[i].z; }
         if (rot) { rot[3 * i] = c[i].x; rot[3 * i + 1] = c[i].y; rot[3 * i + 2] = c[i].z; }
     }
+    return RF_OK;
+}
+
+rf_status rf_engine_autotune(rf_engine* e, int steps, int* choice, float* ms_out) {
+    if (!e || steps <= 0) { set_error("rf_engine_autotune: bad arguments"); return RF_ERR_INVALID; }
+    if (!e->c.ext) {
+        if (choice) *choice = RF_STEP_MIN_BLOCKS;
+        return RF_OK;                                      // the reference-model step has one variant
+    }
+    cudaStream_t s = e->stream;
+    RF_CUDA(cudaStreamSynchronize(s));
+    // snapshot the whole device state: the trials advance it and are undone afterwards
+    std::vector<void*> backup(e->allocs.size(), nullptr);
+    auto release = [&]() { for (void* p : backup) if (p) cudaFree(p); };
+    for (size_t q = 0; q < e->allocs.size(); ++q) {
+        if (cudaMalloc(&backup[q], e->alloc_bytes[q]) != cudaSuccess) { release(); return cuda_status(cudaGetLastError(), "rf_engine_autotune"); }
+        if (cudaMemcpyAsync(backup[q], e->allocs[q], e->alloc_bytes[q], cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+            release();
+            return cuda_status(cudaGetLastError(), "rf_engine_autotune");
+        }
+    }
+    auto restore = [&]() -> cudaError_t {
+        for (size_t q = 0; q < e->allocs.size(); ++q) {
+            cudaError_t ce = cudaMemcpyAsync(e->allocs[q], backup[q], e->alloc_bytes[q], cudaMemcpyDeviceToDevice, s);
+            if (ce) return ce;
+        }
+        return cudaStreamSynchronize(s);
+    };
+    const int variants[3] = {6, 5, 4};
+    float best = 1e30f;
+    int pick = e->step_minb;
+    float times[3] = {0, 0, 0};
+    Dev d = e->d;
+    Consts c = e->c;
+    c.use_graph = 0;
+    void* args[] = {&d, &c};
+    cudaEvent_t a0, a1;
+    cudaEventCreate(&a0); cudaEventCreate(&a1);
+    cudaError_t ce = cudaSuccess;
+    for (int v = 0; v < 3 && !ce; ++v) {
+        void* fn = ext_step_variant(e->task.kind == RF_TEST_BRAZIL, variants[v]);
+        for (int rep = 0; rep < 2 && !ce; ++rep) {             // first pass warms up
+            ce = restore();
+            // candidate lists from the current positions (the engine's first step would build them)
+            const unsigned gN = (c.N + 255) / 256, gC = (c.cg_cells + 1 + 255) / 256;
+            k_force_rebuild<<<1, 1, 0, s>>>(d.sc);
+            k_rb_zero<<<gC, 256, 0, s>>>(d, c);
+            k_rb_bin<<<gN, 256, 0, s>>>(d, c);
+            k_rb_scan_sums<<<e->cg_nb, 1024, 0, s>>>(d, c);
+            k_rb_scan_totals<<<1, 32, 0, s>>>(d, c);
+            k_rb_scan_apply<<<e->cg_nb, 1024, 0, s>>>(d, c);
+            k_rb_scatter<<<gN, 256, 0, s>>>(d, c);
+            k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
+            k_set_target<<<1, 1, 0, s>>>(d.sc, (unsigned long long)steps);
+            cudaEventRecord(a0, s);
+            for (int q = 0; q < steps && !ce; ++q) ce = cudaLaunchKernel(fn, dim3(e->nblocks), dim3(128), args, 0, s);
+            cudaEventRecord(a1, s);
+            if (!ce) ce = cudaEventSynchronize(a1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a0, a1);
+            times[v] = ms;
+        }
+        if (!ce && times[v] < best) { best = times[v]; pick = variants[v]; }
+    }
+    if (!ce) ce = restore();
+    cudaEventDestroy(a0); cudaEventDestroy(a1);
+    release();
+    if (ce) return cuda_status(ce, "rf_engine_autotune");
+    if (pick != e->step_minb) {
+        e->step_minb = pick;
+        if (e->graph_ok) {                                     // rebuild the step graph with the choice
+            if (e->exec) cudaGraphExecDestroy(e->exec);
+            if (e->graph) cudaGraphDestroy(e->graph);
+            e->exec = nullptr; e->graph = nullptr; e->graph_ok = false;
+            if (build_graph(e) == RF_OK) e->graph_ok = true;
+            else { cudaGetLastError(); e->c.use_graph = 0; }
+        }
+    }
+    if (choice) *choice = pick;
+    if (ms_out) for (int v = 0; v < 3; ++v) ms_out[v] = times[v];
     return RF_OK;
 }
 

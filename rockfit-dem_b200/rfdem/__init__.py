@@ -167,6 +167,7 @@ _proto = {
     "rf_engine_uses_graph": (i32, [P]),
     "rf_engine_create_ext": (i32, [C.POINTER(Task), C.POINTER(ExtParams), P, P, C.POINTER(P)]),
     "rf_engine_positions_f64": (i32, [P, P]),
+    "rf_engine_autotune": (i32, [P, i32, C.POINTER(i32), P]),
     "rf_engine_create_batch": (i32, [C.POINTER(Task), C.POINTER(ExtParams), P, P, i32, C.POINTER(P)]),
     "rf_engine_batch_size": (i32, [P]),
     "rf_engine_spec_info": (i32, [P, i32, P, P, P, C.POINTER(Task)]),
@@ -411,6 +412,14 @@ class Engine:
         check(lib.rf_engine_load_increment_pred(self.h, C.byref(params), ptr(pred), ldp, C.byref(r)),
               "rf_engine_load_increment_pred")
         return r
+
+    def autotune(self, steps=200):
+        """Pick the fastest compiled step-kernel variant (state restored afterwards);
+        returns (CTAs per SM of the pick, [ms for 6, 5, 4])."""
+        ch = C.c_int(0)
+        ms = np.zeros(3, np.float32)
+        check(lib.rf_engine_autotune(self.h, steps, C.byref(ch), ms.ctypes.data), "rf_engine_autotune")
+        return ch.value, ms.tolist()
 
     def positions_f64(self):
         R = np.zeros(3 * self.N, np.float64)

@@ -89,3 +89,20 @@ def test_ext_packed_specimen_vs_oracle_and_fp64(cuda):
     err = float(np.max(np.abs(o["R"] - g["R"])))
     print("packed N=%d bonds=%d max |R_f32force - R_fp64| = %.3e mm" % (N, int(o["ILtype"].sum()), err))
     assert err < 1e-6 * (H + D)
+
+
+def test_autotune_leaves_results_unchanged(cuda):
+    """The autotuner's trial steps are undone: an autotuned engine steps exactly like an
+    untuned one, whichever variant it picked."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
+    a = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    b = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    pick, ms = b.autotune(50)
+    assert pick in (4, 5, 6) and all(m > 0 for m in ms)
+    a.step(150)
+    b.step(150)
+    assert np.array_equal(a.positions_f64(), b.positions_f64())
+    sa, sb = a.export(), b.export()
+    assert np.array_equal(sa["IL"], sb["IL"]) and np.array_equal(sa["V"], sb["V"])
+    assert a.counters()["steps"] == b.counters()["steps"] == 150
+    a.close(); b.close()

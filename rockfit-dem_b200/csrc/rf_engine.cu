@@ -57,6 +57,10 @@ struct DevScalars {
     int32_t Loading, Fracture;
     unsigned long long steps, target, rebuilds, curve_n, broken;
     uint32_t done, err, rebuild, moved, block_counter, pad;
+    // largest displacement since the last candidate build of the positions a step reads
+    // (FP32 bits of its square, accumulated by the step writing them), for skipping scans
+    uint32_t d2max_next;
+    float dmax;
     // FIRE relaxation of a quasi-static load increment (extended model)
     double fdt, falpha, fdt0, fdtmax, fdtmin, finc, fdec, falpha0, fshrink, ftol;
     double fresidual, fmean, fpower, fcv, fcf, fcm;
@@ -80,6 +84,7 @@ struct Consts {
     float cg_ox, cg_oy, cg_oz;
     uint32_t cg_nx, cg_ny, cg_nz, cg_cells;
     float rc2, disp2, hard2;   // rebuild trigger and the displacement the candidate lists cover
+    float acut_f;              // sqrt(aacut)
     unsigned long long curve_cap;
     cudaGraphConditionalHandle h_loop, h_rebuild;
     int use_graph;
@@ -132,6 +137,7 @@ struct Dev {
     uint32_t* cand_n;   // [N]
     unsigned long long* member;   // [N]
     float4* pos_ref;    // [N]
+    float* cmargin;     // [N] smallest (distance - a_farcut) of the non-member candidates at the build
     uint32_t* cg_key;   // [N]
     uint32_t* cg_count; // [cells+1]
     uint32_t* cg_start; // [cells+1]
@@ -310,8 +316,21 @@ __global__ void k_rb_cand(Dev d, Consts c) {
                 if (d.cand[(size_t)q * c.N + i] == j) { mem |= 1ull << q; break; }
         }
         d.member[i] = mem;
+        // margin of the nearest non-member candidate: until the displacements since this
+        // build add up to it, no candidate can come within a_farcut
+        float mg = 3.0e38f;
+        for (uint32_t q = 0; q < n; ++q) {
+            if ((mem >> q) & 1ull) continue;
+            const float4 xj = posf(d, c, cur, d.cand[(size_t)q * c.N + i]);
+            const float ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
+            mg = fminf(mg, sqrtf(ddx * ddx + ddy * ddy + ddz * ddz) - c.acut_f);
+        }
+        d.cmargin[i] = mg;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&d.sc->rebuilds, 1ull);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&d.sc->rebuilds, 1ull);
+        d.sc->dmax = 0.f;                     // positions == build positions
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -341,6 +360,7 @@ __device__ __forceinline__ void delete_slot(const Dev& d, const Consts& c, uint3
     const uint32_t N = c.N;
     const size_t s = (size_t)i * c.K + k;
     d.ids[s] = EMPTY32;                       // its overlap reads as zero once the cmask bit is clear
+    d.cmargin[i] = 0.f;                       // the deleted partner may come back: scan until the next build
     retire_record(d, c, i, k, nbq, bmask);
     const uint32_t bit = 1u << k;
     live &= ~bit; bond &= ~bit; cm &= ~bit;
@@ -361,6 +381,24 @@ __device__ __forceinline__ void delete_far(const Dev& d, const Consts& c, const 
         const float rr = dist2_rn(xi, f4to3(__ldg(&P[j])));
         if (rr > c.aa_farcut || (double)rr < 1e-10) delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
     }
+}
+
+// True when the candidate scan of the add pass cannot find anything: every non-member
+// candidate was at least cmargin beyond a_farcut at the last build, and since then this
+// particle moved by |x - x_build| and none by more than dmax (the largest displacement
+// of the positions this step reads). 10 % and 1e-4 a_farcut of slack cover the float
+// rounding of the margins and displacements.
+__device__ __forceinline__ bool scan_not_needed(const Dev& d, const Consts& c, uint32_t i, float x, float y, float z) {
+    const float4 pr = d.pos_ref[i];
+    const float ex = x - pr.x, ey = y - pr.y, ez = z - pr.z;
+    const float di = sqrtf(ex * ex + ey * ey + ez * ez);
+    return di + d.sc->dmax < 0.9f * d.cmargin[i] - 1e-4f * c.acut_f;
+}
+
+// Largest squared displacement (since the last build) of the positions a step writes.
+__device__ __forceinline__ void note_displacement(const Dev& d, float e2) {
+    const uint32_t w = __reduce_max_sync(0xffffffffu, __float_as_uint(e2));
+    if ((threadIdx.x & 31) == 0 && w) atomicMax(&d.sc->d2max_next, w);
 }
 
 // The delete pass of the last step, applied before the state is read out: the step
@@ -466,6 +504,8 @@ __device__ __forceinline__ void step_finish(const Dev& d, const Consts& c, doubl
     sc->Hd2 = sc->sized2[ax];
     sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
     sc->steps += 1;
+    sc->dmax = sqrtf(__uint_as_float(sc->d2max_next));
+    sc->d2max_next = 0;
     const bool running = (sc->Strain < sc->MaxStrain) && !sc->Fracture;
     sc->done = running ? 0u : 1u;
     const uint32_t mv = sc->moved;
@@ -597,8 +637,10 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
     }
 
     // ---- add: InteractionListReConstructBPM (md_interaction_list_reconstructbpm.cu:13-46,80-139)
+    // (skipped when no candidate can have come within a_farcut since the build: the scan
+    // would add nothing)
     bool replay = false;
-    if (valid) {
+    if (valid && !scan_not_needed(d, c, i, xi.x, xi.y, xi.z)) {
         unsigned long long tried = mem;
         bool have_cells = false;
         Octant oc;
@@ -655,6 +697,7 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
     }
     cm = cm_out;
 
+    float e2max = 0.f;
     double sfb = 0.0, sft = 0.0;
     uint32_t moved = 0;
     if (valid) {
@@ -690,9 +733,11 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
         const float e2 = ex * ex + ey * ey + ez * ez;
         moved = (e2 > c.disp2) ? 1u : 0u;
         // lists may have missed a neighbour (a particle moved to the hidden point has none)
-        if (e2 > c.hard2 && !(Rx == c.hp.x && Ry == c.hp.y && Rz == c.hp.z)) raise_status(&d.sc->err, RF_ERR_CAPACITY);
+        const bool hidden = Rx == c.hp.x && Ry == c.hp.y && Rz == c.hp.z;
+        if (e2 > c.hard2 && !hidden) raise_status(&d.sc->err, RF_ERR_CAPACITY);
+        if (!hidden) e2max = e2;
     }
-
+    note_displacement(d, e2max);
     step_finish<KIND>(d, c, sfb, sft, nbroken, moved);
 }
 
@@ -897,6 +942,8 @@ __device__ __forceinline__ void step_finish_ext(const Dev& d, const Consts& c, d
     if (threadIdx.x != 0) return;
     sc->block_counter = 0;
     if (d.nspec > 1) sc->steps += 1;                          // (with one specimen sc == spec)
+    sc->dmax = sqrtf(__uint_as_float(sc->d2max_next));
+    sc->d2max_next = 0;
     sc->done = all_done ? 1u : 0u;
     const uint32_t mv = sc->moved;
     sc->moved = 0;
@@ -1057,7 +1104,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     contact_pass(true);
 
     bool replay = false;
-    if (valid) {
+    if (valid && !(MODE == 0 && scan_not_needed(d, c, i, (float)xi.x, (float)xi.y, (float)xi.z))) {
         unsigned long long tried = mem;
         bool have_cells = false;
         Octant oc;
@@ -1102,6 +1149,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     kt += ktc;
     kr += krc;
 
+    float e2max = 0.f;
     double sfb = 0.0, sft = 0.0;
     uint32_t moved = 0;
     double acc[FIRE_SUMS];
@@ -1162,11 +1210,13 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         const float e2 = ex * ex + ey * ey + ez * ez;
         moved = (e2 > c.disp2) ? 1u : 0u;
         // lists may have missed a neighbour (a particle moved to the hidden point has none)
-        if (e2 > c.hard2 && !(Rx == (double)G.hp.x && Ry == (double)G.hp.y && Rz == (double)G.hp.z))
-            raise_status(&d.sc->err, RF_ERR_CAPACITY);
+        const bool hidden = Rx == (double)G.hp.x && Ry == (double)G.hp.y && Rz == (double)G.hp.z;
+        if (e2 > c.hard2 && !hidden) raise_status(&d.sc->err, RF_ERR_CAPACITY);
+        if (!hidden) e2max = e2;
         }
     }
     if (MODE == 0) {
+        note_displacement(d, e2max);
         step_finish_ext<KIND>(d, c, sfb, sft, nbroken, moved, sI - sA);
     } else {
         const uint32_t nb = __reduce_add_sync(FULL, nbroken);
@@ -1315,6 +1365,8 @@ __global__ void k_fire_update(Dev d, Consts c) {
     if (!s_last || threadIdx.x != 0) return;
     __threadfence();
     sc->block_counter = 0;
+    sc->dmax = 3.0e38f;          // FIRE moves particles outside the step kernel: no scan skipping
+    sc->d2max_next = 0;          // until the next build or explicit step measures it again
     const uint32_t mv = sc->moved;
     sc->moved = 0;
     sc->rebuild = mv;
@@ -2088,6 +2140,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     c.rc2 = (float)(rc * rc);
     c.disp2 = (float)((0.3 * skin) * (0.3 * skin));   // checked every RF_GRAPH_UNROLL steps
     c.hard2 = (float)((0.5 * skin) * (0.5 * skin));
+    c.acut_f = (float)acut;
     const double hcell = rc * 1.0001;
     c.cg_inv_h = (float)(1.0 / hcell);
     c.cg_ox = (float)(t->S.center.x - t->S.spacesized2.x - hcell);
@@ -2116,7 +2169,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         (st = dalloc(e, &d.live, N)) || (st = dalloc(e, &d.bond, N)) || (st = dalloc(e, &d.cmask, N)) ||
         (st = dalloc(e, &d.nbq, N)) || (st = dalloc(e, &d.bmask, N)) || (st = dalloc(e, &e->maxq_dev, 1)) ||
         (st = dalloc(e, &d.cand, (size_t)c.KC * N)) || (st = dalloc(e, &d.cand_n, N)) || (st = dalloc(e, &d.member, N)) ||
-        (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
+        (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cmargin, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
         (st = dalloc(e, &d.cg_start, cells + 1)) || (st = dalloc(e, &d.cg_fill, cells + 1)) ||
         (st = dalloc(e, &d.cg_bsum, e->cg_nb)) || (st = dalloc(e, &d.cg_sorted, N)) ||
         (st = dalloc(e, &d.partial, e->nblocks)) || (st = dalloc(e, &d.partial2, e->nblocks)) ||
@@ -2174,6 +2227,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     }
     // the scalar block is read (step parity) by the row import below: start it at zero
     if (cudaMemsetAsync(d.member, 0, N * sizeof(unsigned long long), s) || cudaMemsetAsync(d.cand_n, 0, N * 4, s) ||
+        cudaMemsetAsync(d.cmargin, 0, N * sizeof(float), s) ||
         cudaMemsetAsync(d.sc, 0, sizeof(DevScalars), s))
         return fail(RF_ERR_CUDA);
 

@@ -62,6 +62,7 @@ def _declare(L):
         "rfo_fdotv_f": (f64, [P, P, u64]),
         "rfo_qs_ext_f": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
         "rfo_qs_ext_d": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
+        "rfo_warm_probe_ext_d": (None, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, u64, P]),
         "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
         "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
     }
@@ -145,6 +146,20 @@ def qs_ext(task, x, R0, radius, params, n_inc, fp64=False, trace_cap=0):
     status = fn(C.byref(task), C.byref(x), p(R), p(rad), C.byref(params), n_inc, p(it), p(cv), p(rs), p(st),
                 p(tr) if trace_cap else None, trace_cap)
     return dict(R=R, iters=it, converged=cv, residual=rs, stress=st, trace=tr[:trace_cap], status=status)
+
+
+def warm_probe(task, x, R0, radius, params, n_pre, warm_iters):
+    """FP64 extended oracle: after n_pre plain FIRE increments, relax the next increment
+    plainly and, from the same state, warm-started with that plain answer (displacements
+    and rotations) for at most warm_iters iterations. Returns a dict of iterations,
+    residuals, platen stresses and the largest bond-state differences between the two."""
+    L = load()
+    out = np.zeros(15, np.float64)
+    L.rfo_warm_probe_ext_d(C.byref(task), C.byref(x), p(np.ascontiguousarray(R0, np.float64)),
+                           p(np.ascontiguousarray(radius, np.float64)), C.byref(params), n_pre, warm_iters, p(out))
+    keys = ["it_plain", "res_plain", "res_warm", "stress_plain", "stress_warm", "dOijt", "maxOijt", "dMijn", "maxMijn",
+            "dMijt", "maxMijt", "dRij", "dx", "it_warm", "conv_warm"]
+    return dict(zip(keys, out.tolist()))
 
 
 def ref_gpu():

@@ -1271,9 +1271,13 @@ struct RunExt {
     // [delete, add, forces with the FIRE dt and without damping or rolling resistance,
     // platen clamp at rest, FIRE decision on FP64 sums, mixing and semi-implicit Euler].
     // trace (may be null) receives the residual of every iteration.
+    std::vector<double> X0, ROT;      // start positions and accumulated rotation of the last increment
+
     uint64_t fire_increment(const rf_relax_params& p, int* converged, double* residual, double* trace,
-                            uint64_t trace_cap) {
+                            uint64_t trace_cap, const double* warm = nullptr) {
         rf_compression& Kc = t->Compress;
+        X0 = R;
+        ROT.assign(3 * N, 0.0);
         const int ax = t->kind == RF_TEST_BRAZIL ? 1 : 2;
         const double delta = p.strain_inc * Kc.Size0;
         double* sz = ax == 1 ? &Kc.size_d.y : &Kc.size_d.z;
@@ -1288,11 +1292,24 @@ struct RunExt {
         std::fill(V.begin(), V.end(), (TF)0);
         std::fill(W.begin(), W.end(), (TF)0);
         // the platen pushes the particles it passed: clamp them now, so the first force
-        // pass (and its convergence test) sees the loaded configuration
+        // pass (and its convergence test) sees the loaded configuration; a warm start
+        // (the engine's rf_engine_load_increment with a prediction) jumps the positions
+        // and carries the motion into the first pass as velocities over dt0
+        const TF idt0 = (TF)(float)(1.0 / p.dt0);
         for (uint64_t i = 0; i < N; ++i) {
             TF f0 = 0, f1 = 0, f2 = 0, v0 = 0, v1 = 0, v2 = 0;
+            if (warm) {
+                const double* q = warm + 6 * i;
+                TF u[6];
+                for (int a = 0; a < 6; ++a) u[a] = (TF)(float)q[a];
+                R[i] += (double)u[0]; R[i + N] += (double)u[1]; R[i + 2 * N] += (double)u[2];
+                v0 = u[0] * idt0; v1 = u[1] * idt0; v2 = u[2] * idt0;
+                W[i] = u[3] * idt0; W[i + N] = u[4] * idt0; W[i + 2 * N] = u[5] * idt0;
+                ROT[3 * i] = u[3]; ROT[3 * i + 1] = u[4]; ROT[3 * i + 2] = u[5];
+            }
             double sb = 0, st = 0;
             platen(i, f0, f1, f2, R[i], R[i + N], R[i + 2 * N], v0, v1, v2, (TF)0, sb, st);
+            V[i] = v0; V[i + N] = v1; V[i + 2 * N] = v2;
         }
         const TF dt_keep = dt, pA_keep = p_A, mur_keep = mur;
         p_A = 0; mur = 0;
@@ -1362,6 +1379,7 @@ struct RunExt {
                     v[a] += F[a] * dtm;
                     w[a] += M[a] * dtI;
                     R[i + a * N] += (double)v[a] * (double)dtf;
+                    ROT[3 * i + a] += (double)w[a] * (double)dtf;
                     V[i + a * N] = v[a];
                     W[i + a * N] = w[a];
                 }
@@ -1418,7 +1436,58 @@ static int qs_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const doubl
 }
 }  // namespace rfo
 
+namespace rfo {
+// Exact warm start on the CPU: n_pre plain increments, then the next increment once plain
+// (reference) and once from the same state warm-started with the plain answer; returns
+// the warm start's residual after `warm_iters` iterations the largest differences of the
+// bond state from the plain relaxed state, and the warm run's iterations and convergence flag.
+template <class TF>
+static void warm_probe(rf_task* t, const rf_ext_params* xp, const double* R0, const double* rad,
+                       const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out) {
+    RunExt<TF> a;
+    a.t = t;
+    a.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed};
+    a.init(R0, rad);
+    int c; double res;
+    for (uint64_t k = 0; k < n_pre; ++k) a.fire_increment(*p, &c, &res, nullptr, 0);
+    RunExt<TF> b = a;
+    rf_task tb = *t;
+    b.t = &tb;
+    const uint64_t it_plain = a.fire_increment(*p, &c, &res, nullptr, 0);
+    std::vector<double> warm(6 * a.N);
+    for (uint64_t i = 0; i < a.N; ++i)
+        for (int k = 0; k < 3; ++k) {
+            warm[6 * i + k] = a.R[i + k * a.N] - a.X0[i + k * a.N];
+            warm[6 * i + 3 + k] = a.ROT[3 * i + k];
+        }
+    rf_relax_params q = *p;
+    q.max_iter = warm_iters;
+    int cb; double rb;
+    const uint64_t it_warm = b.fire_increment(q, &cb, &rb, nullptr, 0, warm.data());
+    double dO = 0, dN = 0, dT = 0, dR = 0, sO = 0, sN = 0, sT = 0, dx = 0;
+    for (uint64_t k = 0; k < a.N * a.K; ++k) {
+        if (a.type[k] != 1 || b.type[k] != 1) continue;
+        auto diff = [](const V3<TF>& u, const V3<TF>& v) {
+            return std::max(std::fabs((double)u.x - v.x), std::max(std::fabs((double)u.y - v.y), std::fabs((double)u.z - v.z)));
+        };
+        auto mag = [](const V3<TF>& u) { return std::max(std::fabs((double)u.x), std::max(std::fabs((double)u.y), std::fabs((double)u.z))); };
+        dO = std::max(dO, diff(a.Oijt[k], b.Oijt[k])); sO = std::max(sO, mag(a.Oijt[k]));
+        dN = std::max(dN, diff(a.Mijn[k], b.Mijn[k])); sN = std::max(sN, mag(a.Mijn[k]));
+        dT = std::max(dT, diff(a.Mijt[k], b.Mijt[k])); sT = std::max(sT, mag(a.Mijt[k]));
+        dR = std::max(dR, diff(a.Rij[k], b.Rij[k]));
+    }
+    for (uint64_t q2 = 0; q2 < 3 * a.N; ++q2) dx = std::max(dx, std::fabs(a.R[q2] - b.R[q2]));
+    out[0] = (double)it_plain; out[1] = res; out[2] = rb; out[3] = t->Compress.Stress; out[4] = tb.Compress.Stress;
+    out[5] = dO; out[6] = sO; out[7] = dN; out[8] = sN; out[9] = dT; out[10] = sT; out[11] = dR; out[12] = dx;
+    out[13] = (double)it_warm; out[14] = (double)cb;
+}
+}  // namespace rfo
+
 extern "C" {
+void rfo_warm_probe_ext_d(rf_task* t, const rf_ext_params* x, const double* R0, const double* rad,
+                          const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out) {
+    rfo::warm_probe<double>(t, x, R0, rad, p, n_pre, warm_iters, out);
+}
 int rfo_qs_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, const rf_relax_params* p,
                  uint64_t n_inc, uint64_t* iters, int* conv, double* res, double* stress, double* trace,
                  uint64_t trace_cap) {

@@ -61,3 +61,27 @@ def test_ext_directed_bonds_pair_up():
     ty = f["ILtype"].reshape(N, K)
     pairs = {(i, int(IL[i, k])) for i in range(N) for k in range(K) if ty[i, k]}
     assert pairs and all((j, i) in pairs for (i, j) in pairs)
+
+
+def test_exact_warm_start_is_path_dependent():
+    """Warm-starting a FIRE increment with its own relaxed answer (displacements and
+    rotations over dt0) does not start at equilibrium: the bond shear forces and moments
+    are integrated along the motion, and one large jump integrates a different path than
+    the relaxation did. The residual after the first pass sits far above the tolerance,
+    the bond state differs from the relaxed one by a small relative amount, and the warm
+    run still converges to the same platen stress in a fraction of the iterations."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
+    p = rfdem.RelaxParams()
+    rfdem.lib.rf_relax_default_params(C.byref(p), C.byref(t))
+    p.max_iter, p.strain_inc = 40000, 1e-4
+    one = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 1)
+    assert one["res_plain"] <= p.tol
+    assert one["res_warm"] > 10 * p.tol
+    assert one["dRij"] < 1e-9 * float(np.max(R) - np.min(R))        # positions land on the relaxed ones
+    assert 0 < one["dMijt"] < 1e-3 * one["maxMijt"]
+    assert 0 < one["dMijn"] < 1e-3 * one["maxMijn"]
+    full = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000)
+    assert full["stress_plain"] > 1e-5                              # the platen carries load
+    assert full["conv_warm"] == 1 and full["res_warm"] <= p.tol
+    assert full["it_warm"] * 2 < full["it_plain"]
+    assert abs(full["stress_warm"] - full["stress_plain"]) <= 1e-4 * abs(full["stress_plain"])

@@ -348,6 +348,9 @@ typedef struct rf_ext_params {
     double weibull_m;         /* Weibull modulus of both strengths */
     double sigma_c, tau_c;    /* Weibull scales of the tensile and shear strength */
     uint64_t seed;            /* strength stream; a pair draws from (seed, min(i,j), max(i,j)) */
+    double post_peak_drop;    /* 0: stop as the reference does (stress below ZeroStress after
+                                 loading); d in (0,1): also stop once the stress, after loading,
+                                 is below (1 - d) times its peak so far (post-peak load drop) */
 } rf_ext_params;
 
 /* Create an extended-model engine: h_R double[3N] planar (mm), h_radius double[N].

@@ -848,6 +848,7 @@ template <class T> static inline T rcp(T x) { return (T)1 / x; }
 struct ExtPar {
     double kn, ks, lambda, gap, wm, sig, tau;
     uint64_t seed;
+    double drop;      // post-peak stop: fracture once the stress is below (1 - drop) x peak (0: off)
 };
 
 static inline uint64_t mix64(uint64_t z) {
@@ -1262,6 +1263,8 @@ struct RunExt {
             V[i] = Vx; V[i + N] = Vy; V[i + 2 * N] = Vz;
         }
         sum_forces(t, sfb, sft, sz0, curve, cap, nsaved);
+        const double keep = x.drop > 0.0 ? 1.0 - x.drop : 0.0;
+        if (Kc.Loading && Kc.Stress < keep * Kc.FractureStress) Kc.Fracture = 1;
         compress(t, Kc.Stress);
         ++steps;
     }
@@ -1396,7 +1399,8 @@ static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const
                         uint64_t* nsaved, int* status, uint64_t* broken) {
     RunExt<TF> r;
     r.t = t;
-    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed};
+    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
+                 xp->post_peak_drop};
     r.init(R_io, rad);
     uint64_t ns = 0;
     while (r.running() && r.steps < max_steps) r.step(curve, cap, &ns);   // max_steps 0: bonds only
@@ -1422,7 +1426,8 @@ static int qs_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const doubl
                   uint64_t trace_cap) {
     RunExt<TF> r;
     r.t = t;
-    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed};
+    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
+                 xp->post_peak_drop};
     r.init(R_io, rad);
     for (uint64_t k = 0; k < n_inc; ++k) {
         int c = 0;
@@ -1446,7 +1451,8 @@ static void warm_probe(rf_task* t, const rf_ext_params* xp, const double* R0, co
                        const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out) {
     RunExt<TF> a;
     a.t = t;
-    a.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed};
+    a.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
+                 xp->post_peak_drop};
     a.init(R0, rad);
     int c; double res;
     for (uint64_t k = 0; k < n_pre; ++k) a.fire_increment(*p, &c, &res, nullptr, 0);

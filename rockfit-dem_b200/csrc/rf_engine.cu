@@ -52,6 +52,7 @@ struct DevScalars {
         Strain, MaxStrain, Size0;
     double size_d[3], center_d[3];
     double sz0;
+    double keep_frac;       // post-peak stop: fracture once Stress < keep_frac * peak (0: off)
     float center[3], size[3], sized2[3];
     float RR, _1d_Area, Hd2;
     int32_t Loading, Fracture;
@@ -921,6 +922,7 @@ __device__ __forceinline__ void step_finish_ext(const Dev& d, const Consts& c, d
                 S->FractureStrain = (S->sz0 - S->size_d[2]) / S->sz0;
             }
             if (S->Loading && S->Stress < S->ZeroStress) S->Fracture = 1;
+            if (S->Loading && S->Stress < S->keep_frac * S->FractureStress) S->Fracture = 1;
             const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
             S->V = (S->Stress < 1e-9) ? 10.0 * S->VLoad : S->VLoad;
             S->size_d[ax] += S->V * c.dt_d;
@@ -1037,26 +1039,30 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     {
         const uint32_t wb = __reduce_or_sync(FULL, bmask);
         const uint32_t qend = 32u - __clz(wb);
+        // every load of a record is issued before the partner's gathers and the far-link
+        // test, so a record waits for two dependent latencies (id -> partner state), not three
         for (uint32_t q = 0; q < qend; ++q) {
             if (!((bmask >> q) & 1u)) continue;
             const size_t s = (size_t)q * N + i;
             const uint32_t j = __ldg(&d.bj[s]);
+            const float4 s0 = d.bst[s], s1 = d.bst[s + QN], s2 = d.bst[s + 2 * QN];
+            const float2 str = __ldg(&d.bstr[s]);
+            const double L0 = __ldg(&d.bL0[s]);
             const double4 xj = ldg_d4(&P[j]);
+            const float4 vj = __ldg(&Vv[j]), wj = __ldg(&Wv[j]);
             const double3 rd = dsub(xj, xi);
             const double rr = dlen2(rd);
             if (rr > c.aa_farcut_d || rr < 1e-10) {
                 delete_slot(d, c, i, d.bk[s], j, ncand, nbq, live, bond, cm, bmask, mem);
                 continue;
             }
-            const float4 s0 = d.bst[s], s1 = d.bst[s + QN], s2 = d.bst[s + 2 * QN];
-            const float2 str = __ldg(&d.bstr[s]);
             BondExt b;
             b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ri, (float)xj.w);
-            b.sc = str.x; b.tc = str.y; b.L0 = __ldg(&d.bL0[s]);
+            b.sc = str.x; b.tc = str.y; b.L0 = L0;
             const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
             f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
             f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
-            const bool broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(__ldg(&Vv[j])), wi, f4to3(__ldg(&Wv[j])),
+            const bool broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(vj), wi, f4to3(wj),
                                              rij, oijt, mijn, mijt, fsb, msb, fnabs, kt, kr);
             ++npair;
             d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
@@ -2057,6 +2063,10 @@ struct BatchIn {
     std::vector<double> xoff;
 };
 
+// post-peak stop rule of an extended-model specimen: the stress fraction of the peak below
+// which it counts as fractured (0: the reference's ZeroStress rule alone)
+double keep_fraction(const rf_ext_params& x) { return x.post_peak_drop > 0.0 ? 1.0 - x.post_peak_drop : 0.0; }
+
 void fill_scalars(DevScalars& h, const rf_task& t) {
     std::memset(&h, 0, sizeof(h));
     const rf_compression& K_ = t.Compress;
@@ -2086,7 +2096,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     if (ext) {
         for (uint64_t i = 0; i < t->N; ++i) { rmax = std::max(rmax, h_rad[i]); rmin = std::min(rmin, h_rad[i]); }
         if (!(rmin > 0.0) || !(x->kn > 0.0) || !(x->ks >= 0.0) || !(x->bond_lambda > 0.0) || !(x->weibull_m > 0.0) ||
-            !(x->sigma_c > 0.0) || !(x->tau_c > 0.0)) {
+            !(x->sigma_c > 0.0) || !(x->tau_c > 0.0) || !(x->post_peak_drop >= 0.0 && x->post_peak_drop < 1.0)) {
             set_error("rf_engine_create_ext: radii and bond parameters must be positive");
             return RF_ERR_INVALID;
         }
@@ -2214,7 +2224,10 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             d.blk_spec = db;
             if ((st = dalloc(e, &d.spec, nspec))) return fail(st);
             std::vector<DevScalars> hs(nspec);
-            for (uint32_t k = 0; k < nspec; ++k) fill_scalars(hs[k], bin->tasks[k]);
+            for (uint32_t k = 0; k < nspec; ++k) {
+                fill_scalars(hs[k], bin->tasks[k]);
+                hs[k].keep_frac = keep_fraction(bin->xs[k]);
+            }
             if (cudaMemcpyAsync(d.spec, hs.data(), nspec * sizeof(DevScalars), cudaMemcpyHostToDevice, s))
                 return fail(RF_ERR_CUDA);
             e->spec_tasks = bin->tasks;
@@ -2334,6 +2347,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     // scalar state (with one specimen the global block is also the specimen's)
     DevScalars h;
     fill_scalars(h, *t);
+    if (ext) h.keep_frac = keep_fraction(*x);
     if (nspec > 1) {
         h.done = 0;
         for (uint32_t q = 0; q < nspec; ++q) {
@@ -2390,9 +2404,9 @@ rf_status rf_engine_create_batch(const rf_task* tasks, const rf_ext_params* xs, 
             tq.Po.aa_farcut != t0.Po.aa_farcut || tq.Po.hm_E != t0.Po.hm_E || tq.Po.hm_G != t0.Po.hm_G ||
             tq.Po.p_A != t0.Po.p_A || tq.Po.p_mu != t0.Po.p_mu || tq.Po.p_mur != t0.Po.p_mur ||
             tq.Po.p_m != t0.Po.p_m || xs[q].kn != xs[0].kn || xs[q].ks != xs[0].ks ||
-            xs[q].bond_lambda != xs[0].bond_lambda) {
+            xs[q].bond_lambda != xs[0].bond_lambda || !(xs[q].post_peak_drop >= 0.0 && xs[q].post_peak_drop < 1.0)) {
             set_error("rf_engine_create_batch: specimen %d must have >= 128 particles and the batch's test kind, "
-                      "slots, grid cell, material, time step and bond stiffness", q);
+                      "slots, grid cell, material, time step and bond stiffness, and a post-peak drop in [0, 1)", q);
             return RF_ERR_INVALID;
         }
         total += tq.N;

@@ -85,3 +85,29 @@ def test_exact_warm_start_is_path_dependent():
     assert full["conv_warm"] == 1 and full["res_warm"] <= p.tol
     assert full["it_warm"] * 2 < full["it_plain"]
     assert abs(full["stress_warm"] - full["stress_plain"]) <= 1e-4 * abs(full["stress_plain"])
+
+
+def test_post_peak_drop_stop_rule():
+    """post_peak_drop = d stops a run at the first step, once loading has begun, whose
+    stress is below (1 - d) times the peak so far; up to there the run is the plain one."""
+    po = rfdem.granite_potential()
+    R0, rad = extspec.lattice_ext(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, seed=0xB2000000 + 100)
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, 0.5, v_load=-2e-4, min_stress=4e-4)
+    x = extspec.stiff_params(sigma_c=po.m_Ec * 0.1, tau_c=po.m_Gc * 0.1)
+    x.post_peak_drop = 0.5
+    o = oracle.run_ext(mc.clone(t), x, R, rad, 10 ** 5)
+    S = o["steps"]
+    assert o["status"] == 0 and 100 < S < 5000
+    c = o["curve"]
+    s = 0.5 * (np.abs(c[:, 1]) + np.abs(c[:, 2]))
+    assert s.shape[0] == S
+    loading = np.flatnonzero(s > t.Compress.MinStress)
+    assert loading.size and loading[0] < S - 1
+    peak = np.maximum.accumulate(s)
+    assert s[-1] < 0.5 * peak[-1]
+    assert np.all(s[loading[0]:S - 1] >= 0.5 * peak[loading[0]:S - 1])
+    x.post_peak_drop = 0.0
+    p = oracle.run_ext(mc.clone(t), x, R, rad, S)
+    assert p["steps"] == S and np.array_equal(p["R"], o["R"])
+    q = oracle.run_ext(mc.clone(t), x, R, rad, S + 50)
+    assert q["steps"] == S + 50                        # without the rule the run goes on

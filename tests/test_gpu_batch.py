@@ -76,3 +76,43 @@ def test_batch_specimen_finishing_early_is_frozen(cuda):
     c1 = e.curve_spec(1)
     assert c1.shape[0] == stop
     e.close()
+
+
+def _drop_specimens():
+    """Three weak lattice specimens (strengths a tenth of the granite's) under slow
+    compression that reach a peak and lose half of it within a few thousand steps."""
+    po = rfdem.granite_potential()
+    out = []
+    for q, (d, h) in enumerate([(6.0, 10.0), (6.0, 8.0), (7.0, 10.0)]):
+        R0, rad = extspec.lattice_ext(rfdem.RF_TEST_UNIAXIAL, d, h, seed=0xB2000000 + 100 + q)
+        t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, 0.5, v_load=-2e-4, min_stress=4e-4)
+        x = extspec.stiff_params(seed=0xB2000000 + 200 + q, weibull_m=3.0 + 3.0 * q, sigma_c=po.m_Ec * 0.1,
+                                 tau_c=po.m_Gc * 0.1)
+        x.post_peak_drop = 0.5
+        out.append((t, R, rad, x))
+    return out
+
+
+def test_batch_post_peak_drop_stop(cuda):
+    """Each specimen runs to a post-peak load drop of 50 % and stops at the step the
+    oracle stops at, with the oracle's positions and rows."""
+    specs = _drop_specimens()
+    e = rfdem.BatchEngine([s[0] for s in specs], [s[3] for s in specs], [s[1] for s in specs], [s[2] for s in specs])
+    stops = []
+    for q, (t, R, rad, x) in enumerate(specs):
+        _, _, off, tq = e.spec_info(q)
+        Rq = R.reshape(3, -1).copy()
+        Rq[0] += off
+        o = oracle.run_ext(tq, x, Rq.reshape(-1), rad, 10 ** 5)
+        assert o["status"] == 0
+        stops.append(o["steps"])
+    assert len(set(stops)) == 3 and max(stops) < 5000
+    e.step(10 ** 5)                                   # ends when every specimen has stopped
+    _check_against_oracle(e, specs, stops)
+    for q in range(3):
+        tq, r = e.sync_spec(q)
+        assert r.Fracture == 1
+        c = e.curve_spec(q)
+        s = 0.5 * (np.abs(c[:, 1]) + np.abs(c[:, 2]))
+        assert s[-1] < 0.5 * s.max()
+    e.close()

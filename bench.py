@@ -223,8 +223,18 @@ def run_reference(args):
     print(json.dumps(out))
 
 
-def ext_specimen(rfdem, N, seed):
-    R0, rad, D, H, mo = rfdem.pack_cylinder(N, R0_MM, aspect=2.0, phi=PHI, seed=seed)
+def workload_name(args):
+    if args.particles == N_PARTICLES and args.radii == "uniform" and (args.rmin, args.rmax) == (0.8, 1.2):
+        return WORKLOAD
+    dist = "U[%g,%g]" % (args.rmin, args.rmax) if args.radii == "uniform" else \
+        "log-uniform [%g,%g]" % (args.rmin, args.rmax)
+    return ("explicit BPM uniaxial compression, %d-particle polydisperse cylinder (radii %s x 0.25 mm, aspect 2), "
+            "Weibull bond strengths, FP64 positions / FP32 forces, dt 1e-8 s, 0.1/s" % (args.particles, dist))
+
+
+def ext_specimen(rfdem, N, seed, dist="uniform", rmin=0.8, rmax=1.2):
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, R0_MM, rmin=rmin, rmax=rmax, aspect=2.0, phi=PHI, seed=seed,
+                                            dist=dist)
     v = -0.1 * H * 1e-6                        # strain rate 0.1/s in mm per microsecond
     t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, R0_MM, dt=0.01, v_load=v, max_strain=1.0)
     return t, R, rad, D, H
@@ -274,6 +284,8 @@ def run_explicit(rfdem, torch, t, R, rad, x, args, dist, stream_of):
     if done_steps != S * args.steps:
         raise SystemExit("bench: the specimen finished early (%d of %d steps)" % (done_steps, S * args.steps))
     graph = e.uses_graph()
+    if res.error:
+        raise SystemExit("bench: engine error %d (%s)" % (res.error, rfdem.STATUS.get(res.error, "?")))
     e.close()
     return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, error=res.error, tuned=tuned)
 
@@ -328,10 +340,41 @@ def run_fire(rfdem, torch, t, R, rad, x, seed):
             "warm_start_includes": "feature build + MLP forward (tcgen05 BF16) per load step"}
 
 
-BATCH_SPECIMENS, BATCH_STEPS = 64, 1000
+BATCH_SPECIMENS, BATCH_STEPS, BATCH_FULL_CAP = 64, 1000, 600000
 
 
-def run_batch(rfdem, torch, seed):
+def run_batch_to_failure(rfdem, torch, tasks, params, Rs, rads, counts, t_pack, cap=BATCH_FULL_CAP):
+    """The batch run to completion: every specimen to its 50 % post-peak load drop (or
+    the step cap), one step kernel for all; device time of the whole run and each
+    specimen's stop step, peak stress and broken bonds."""
+    be = rfdem.BatchEngine(tasks, params, Rs, rads)
+    s = torch.cuda.ExternalStream(be.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    chunk, done_steps, ms = 20000, 0, 0.0
+    while done_steps < cap:
+        a.record(s)
+        be.step(chunk)
+        b.record(s)
+        b.synchronize()
+        ms += a.elapsed_time(b)
+        done_steps += chunk
+        res = [be.sync_spec(q)[1] for q in range(len(tasks))]
+        if all(r.Fracture or r.steps < done_steps for r in res):
+            break
+    res = [be.sync_spec(q)[1] for q in range(len(tasks))]
+    be.close()
+    ps = sum(int(tasks[q].N) * int(res[q].steps) for q in range(len(tasks)))
+    return {"workload": "%d Brazilian discs run to a 50 %% post-peak load drop, %d particles in all (%d to %d each, "
+                        "log-uniform), own seeds and Weibull moduli U[3,10], platens 0.05 m/s, dt 1e-8 s"
+                        % (len(tasks), int(sum(int(t.N) for t in tasks)), int(counts.min()), int(counts.max())),
+            "device_s": ms * 1e-3, "specimen_particle_steps_per_s": ps / (ms * 1e-3),
+            "stopped_post_peak": int(sum(1 for r in res if r.Fracture)), "step_cap": cap,
+            "stop_steps": [int(r.steps) for r in res],
+            "peak_stress_MPa": [round(r.FractureStress * 1e3, 3) for r in res],
+            "broken_bonds": [int(r.broken_bonds) for r in res], "packing_s": t_pack}
+
+
+def run_batch(rfdem, torch, seed, full=False):
     """configs[2]-style batch: BATCH_SPECIMENS Brazilian discs (thickness = D/2) with
     particle counts log-uniform in [5k, 80k], radii U[0.8, 1.2] x 0.25 mm, Weibull
     modulus U[3, 10] per specimen (own seed each), platens at 0.05 m/s, dt 1e-8 s; all
@@ -347,9 +390,12 @@ def run_batch(rfdem, torch, seed):
         R0, rad, D, H, mo = rfdem.pack_cylinder(int(counts[q]), R0_MM, aspect=0.5, phi=PHI, seed=seed + q)
         t, R = rfdem.make_test_ext(rfdem.RF_TEST_BRAZIL, R0, rad, R0_MM, dt=0.01, v_load=-5e-5, max_strain=1.0)
         x = rfdem.ext_params_si(weibull_m=float(ms[q]), seed=seed + 1000 + q)
+        x.post_peak_drop = 0.5                    # each specimen stops after a 50 % post-peak load drop
         tasks.append(t); params.append(x); Rs.append(R); rads.append(rad)
     t_pack = time.perf_counter() - t0
     ntot = int(sum(int(t.N) for t in tasks))
+    if full:
+        return run_batch_to_failure(rfdem, torch, tasks, params, Rs, rads, counts, t_pack)
     be = rfdem.BatchEngine(tasks, params, Rs, rads)
     s = torch.cuda.ExternalStream(be.stream())
     be.step(BATCH_STEPS)
@@ -393,7 +439,7 @@ def run_engine(args):
     rank, ws, dist = dist_init()
     import rfdem
     S = STEPS_PER_BENCH_STEP
-    t, R, rad, Dm, Hm = ext_specimen(rfdem, N_PARTICLES, rank_seed(rank))
+    t, R, rad, Dm, Hm = ext_specimen(rfdem, args.particles, rank_seed(rank), args.radii, args.rmin, args.rmax)
     x = rfdem.ext_params_si()
     N = int(t.N)
     K = int(t.K)
@@ -476,7 +522,7 @@ def run_engine(args):
 
     batch = None
     if rank == 0 and ws == 1 and not args.no_batch:
-        batch = run_batch(rfdem, torch, 0xB2000000 + 4000)
+        batch = run_batch(rfdem, torch, 0xB2000000 + 4000, full=args.batch_full)
 
     fire = None
     if rank == 0 and ws == 1 and not args.no_fire:
@@ -486,7 +532,7 @@ def run_engine(args):
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 forces, f64 positions", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "particles": N, "specimen_mm": [round(Dm, 2), round(Hm, 2)],
+           "config": {"workload": workload_name(args), "particles": N, "specimen_mm": [round(Dm, 2), round(Hm, 2)],
                       "explicit_steps_per_bench_step": S, "slots_K": K,
                       "bonds_per_particle": round(bbar, 3), "contacts_per_particle": round(cbar, 3),
                       "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 16 + N * 300 + c1["bonds"] * 129) / 1e6),
@@ -547,7 +593,17 @@ def main():
     ap.add_argument("--explicit-steps", type=int, default=STEPS_PER_BENCH_STEP,
                     help="explicit steps per bench step (profiling runs use fewer)")
     ap.add_argument("--no-reference-model", action="store_true", help="skip the reference-model line")
+    ap.add_argument("--particles", type=int, default=N_PARTICLES, help="particles of the benchmark specimen")
+    ap.add_argument("--radii", default="uniform", choices=["uniform", "log-uniform"])
+    ap.add_argument("--rmin", type=float, default=None, help="smallest radius / 0.25 mm (0.8; 0.5 log-uniform)")
+    ap.add_argument("--rmax", type=float, default=None, help="largest radius / 0.25 mm (1.2; 1.5 log-uniform)")
+    ap.add_argument("--batch-full", action="store_true",
+                    help="run the 64-disc batch to every specimen's post-peak drop instead of the timed window")
     args = ap.parse_args()
+    if args.rmin is None:
+        args.rmin = 0.8 if args.radii == "uniform" else 0.5
+    if args.rmax is None:
+        args.rmax = 1.2 if args.radii == "uniform" else 1.5
     if args.warmup < 3:
         args.warmup = 3
     STEPS_PER_BENCH_STEP = max(1, args.explicit_steps)

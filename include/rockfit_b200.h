@@ -523,6 +523,15 @@ rf_status rf_specimen_lattice_disc(uint64_t seed, double p_r, double gap_frac, d
 rf_status rf_pack_cylinder(uint64_t seed, uint64_t N, double r0, double rmin, double rmax, double aspect,
                            double phi, const double center[3], double* R, double* radius,
                            double* diameter, double* height, double* max_overlap);
+/* Radius distributions of rf_pack_cylinder_dist. */
+typedef enum rf_radius_dist {
+    RF_RADII_UNIFORM = 0,       /* r0 * U[rmin, rmax] (rf_pack_cylinder) */
+    RF_RADII_LOG_UNIFORM = 1    /* r0 * rmin * (rmax / rmin)^U[0, 1] */
+} rf_radius_dist;
+/* rf_pack_cylinder with a choice of radius distribution. */
+rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0, double rmin, double rmax, int dist,
+                                double aspect, double phi, const double center[3], double* R, double* radius,
+                                double* diameter, double* height, double* max_overlap);
 
 /* ------------------------------------------------------------------------ */
 /* BF16 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory) and the */

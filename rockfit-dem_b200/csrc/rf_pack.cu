@@ -241,8 +241,15 @@ using namespace rf::pack;
 extern "C" rf_status rf_pack_cylinder(uint64_t seed, uint64_t N, double r0, double rmin, double rmax, double aspect,
                                       double phi, const double center[3], double* R, double* radius,
                                       double* diameter, double* height, double* max_overlap) {
+    return rf_pack_cylinder_dist(seed, N, r0, rmin, rmax, RF_RADII_UNIFORM, aspect, phi, center, R, radius, diameter,
+                                 height, max_overlap);
+}
+
+extern "C" rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0, double rmin, double rmax, int dist,
+                                           double aspect, double phi, const double center[3], double* R,
+                                           double* radius, double* diameter, double* height, double* max_overlap) {
     if (N < 2 || !(r0 > 0) || !(rmin > 0) || !(rmax >= rmin) || !(aspect > 0) || !(phi > 0.05 && phi < 0.7) || !R ||
-        !radius || !center) {
+        !radius || !center || (dist != RF_RADII_UNIFORM && dist != RF_RADII_LOG_UNIFORM)) {
         set_error("rf_pack_cylinder: bad arguments");
         return RF_ERR_INVALID;
     }
@@ -250,7 +257,8 @@ extern "C" rf_status rf_pack_cylinder(uint64_t seed, uint64_t N, double r0, doub
     std::vector<double4> hx(N);
     double vol = 0.0;
     for (uint64_t i = 0; i < N; ++i) {
-        const double r = rmin + (rmax - rmin) * unif(seed, 4 * i + 3);
+        const double u = unif(seed, 4 * i + 3);
+        const double r = dist == RF_RADII_LOG_UNIFORM ? rmin * std::pow(rmax / rmin, u) : rmin + (rmax - rmin) * u;
         hx[i].w = r;
         vol += 4.0 / 3.0 * M_PI * r * r * r;
     }

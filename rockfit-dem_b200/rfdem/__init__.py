@@ -178,6 +178,7 @@ _proto = {
     "rf_engine_load_increment": (i32, [P, C.POINTER(RelaxParams), P, C.POINTER(RelaxResult)]),
     "rf_engine_increment_fields": (i32, [P, P, P, P]),
     "rf_pack_cylinder": (i32, [u64, u64, f64, f64, f64, f64, f64, P, P, P, P, P, P]),
+    "rf_pack_cylinder_dist": (i32, [u64, u64, f64, f64, f64, i32, f64, f64, P, P, P, P, P, P]),
     "rf_gemm_bf16": (i32, [P, i32, P, i32, i32, i32, i32, i32, P, P, i32, P, i32, P, i32, P, i32, i32, f32, i32, P]),
     "rf_gemm_status": (i32, [P]),
     "rf_mlp_create": (i32, [u64, C.POINTER(P)]),
@@ -290,15 +291,22 @@ def make_test(kind, diameter, height, seed=0xB2000000, potential=None, K=32, gap
 
 
 # --- extended model: packed polydisperse specimens ------------------------------
-def pack_cylinder(N, r0, rmin=0.8, rmax=1.2, aspect=2.0, phi=0.6, seed=0xB2000000, center=(0.0, 0.0, 0.0)):
-    """Seeded FIRE packing on the GPU (rf_pack_cylinder). Returns (R float64[3N] planar,
-    radius float64[N], diameter, height, max relative overlap); sizes in mm."""
+RF_RADII_UNIFORM, RF_RADII_LOG_UNIFORM = 0, 1
+
+
+def pack_cylinder(N, r0, rmin=0.8, rmax=1.2, aspect=2.0, phi=0.6, seed=0xB2000000, center=(0.0, 0.0, 0.0),
+                  dist="uniform"):
+    """Seeded FIRE packing on the GPU (rf_pack_cylinder_dist); radii r0 * U[rmin, rmax]
+    (dist "uniform") or log-uniform on [rmin, rmax] * r0 ("log-uniform"). Returns
+    (R float64[3N] planar, radius float64[N], diameter, height, max relative overlap);
+    sizes in mm."""
+    kinds = {"uniform": RF_RADII_UNIFORM, "log-uniform": RF_RADII_LOG_UNIFORM}
     R = np.zeros(3 * N, np.float64)
     rad = np.zeros(N, np.float64)
     D, H, mo = C.c_double(0), C.c_double(0), C.c_double(0)
     c = (C.c_double * 3)(*center)
-    check(lib.rf_pack_cylinder(seed, N, r0, rmin, rmax, aspect, phi, c, R.ctypes.data, rad.ctypes.data,
-                               C.byref(D), C.byref(H), C.byref(mo)), "rf_pack_cylinder")
+    check(lib.rf_pack_cylinder_dist(seed, N, r0, rmin, rmax, kinds[dist], aspect, phi, c, R.ctypes.data,
+                                    rad.ctypes.data, C.byref(D), C.byref(H), C.byref(mo)), "rf_pack_cylinder_dist")
     return R, rad, D.value, H.value, mo.value
 
 
@@ -328,7 +336,9 @@ def make_test_ext(kind, R0, radius, r0, K=32, potential=None, margin=None, v_loa
     po.p_r = r0
     po.b_r = 0.330015 * r0
     po.b_d = 2.0 * r0 + 0.0593169 * r0 * 2.0
-    po.a_farcut = 2.9 * r0
+    # the reference's list and delete cutoff, widened just past the largest contact
+    # distance 2 r_max where that reaches it (radius ratios above 2.4)
+    po.a_farcut = max(2.9 * r0, 2.02 * float(np.max(radius)))
     N = radius.size
     P3 = R0.reshape(3, N).copy()
     # the platens act on the particle surfaces (centre +- (radius - r0)): box the specimen

@@ -106,3 +106,29 @@ def test_autotune_leaves_results_unchanged(cuda):
     assert np.array_equal(sa["IL"], sb["IL"]) and np.array_equal(sa["V"], sb["V"])
     assert a.counters()["steps"] == b.counters()["steps"] == 150
     a.close(); b.close()
+
+
+def test_ext_log_uniform_radius_ratio_3_vs_oracle(cuda):
+    """Radii log-uniform in [0.5, 1.5] r0 (radius ratio 3): the packer keeps the range and
+    the overlap bound, the list cutoff widens to just past 2 r_max, and the engine's step
+    equals the float oracle's bit for bit."""
+    N, r0 = 3000, 0.25
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, r0, rmin=0.5, rmax=1.5, aspect=2.0, phi=0.55,
+                                            seed=0xB2000000 + 5001, dist="log-uniform")
+    assert mo < 2e-4
+    assert np.all(rad >= 0.5 * r0 - 1e-12) and np.all(rad <= 1.5 * r0 + 1e-12)
+    # log-uniform: log(r) is uniform, so its mean sits at the middle of the log range
+    lr = np.log(rad / r0)
+    assert abs(lr.mean() - 0.5 * (np.log(0.5) + np.log(1.5))) < 0.03
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, r0, min_stress=1e3)
+    assert abs(t.Po.a_farcut - 2.02 * rad.max()) < 1e-12
+    x = rfdem.ext_params_si()
+    steps = 300
+    o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
+    res, st = run_engine_ext(t, x, R, rad, steps)
+    assert res.steps == steps and res.error == 0 and o["status"] == 0
+    assert np.array_equal(st["R64"], o["R"])
+    assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
+    assert np.array_equal(st["ILtype"], o["ILtype"])
+    rows = (st["IL"].reshape(N, -1) != rfdem.EMPTY).sum(axis=1)
+    print("radius ratio 3: slots per row mean %.1f max %d of %d" % (rows.mean(), rows.max(), int(t.K)))

@@ -441,6 +441,7 @@ def run_engine(args):
     S = STEPS_PER_BENCH_STEP
     t, R, rad, Dm, Hm = ext_specimen(rfdem, args.particles, rank_seed(rank), args.radii, args.rmin, args.rmax)
     x = rfdem.ext_params_si()
+    x.list_gap = args.list_gap * R0_MM
     N = int(t.N)
     K = int(t.K)
     r = run_explicit(rfdem, torch, t, R, rad, x, args, dist, None)
@@ -534,6 +535,8 @@ def run_engine(args):
            "vs_baseline": None, "dtype": "f32 forces, f64 positions", "data": "synthetic",
            "config": {"workload": workload_name(args), "particles": N, "specimen_mm": [round(Dm, 2), round(Hm, 2)],
                       "explicit_steps_per_bench_step": S, "slots_K": K,
+                      "list_rule": ("pairs within min(a_farcut, r_i + r_j + %g mm)" % x.list_gap) if x.list_gap > 0
+                      else "pairs within a_farcut (the reference's)",
                       "bonds_per_particle": round(bbar, 3), "contacts_per_particle": round(cbar, 3),
                       "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 16 + N * 300 + c1["bonds"] * 129) / 1e6),
                       "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": r["graph"],
@@ -597,6 +600,9 @@ def main():
     ap.add_argument("--radii", default="uniform", choices=["uniform", "log-uniform"])
     ap.add_argument("--rmin", type=float, default=None, help="smallest radius / 0.25 mm (0.8; 0.5 log-uniform)")
     ap.add_argument("--rmax", type=float, default=None, help="largest radius / 0.25 mm (1.2; 1.5 log-uniform)")
+    ap.add_argument("--list-gap", type=float, default=None,
+                    help="list gap / 0.25 mm: pairs listed within min(a_farcut, r_i + r_j + gap) "
+                         "(default 0.25; 0 is the reference's uniform cutoff a_farcut)")
     ap.add_argument("--batch-full", action="store_true",
                     help="run the 64-disc batch to every specimen's post-peak drop instead of the timed window")
     args = ap.parse_args()
@@ -604,6 +610,8 @@ def main():
         args.rmin = 0.8 if args.radii == "uniform" else 0.5
     if args.rmax is None:
         args.rmax = 1.2 if args.radii == "uniform" else 1.5
+    if args.list_gap is None:
+        args.list_gap = 0.25
     if args.warmup < 3:
         args.warmup = 3
     STEPS_PER_BENCH_STEP = max(1, args.explicit_steps)

@@ -351,6 +351,9 @@ typedef struct rf_ext_params {
     double post_peak_drop;    /* 0: stop as the reference does (stress below ZeroStress after
                                  loading); d in (0,1): also stop once the stress, after loading,
                                  is below (1 - d) times its peak so far (post-peak load drop) */
+    double list_gap;          /* 0: a pair is listed within a_farcut (the reference's rule); g > 0:
+                                 within min(a_farcut, r_i + r_j + g), which keeps the rows of small
+                                 particles short when the radii span a wide range */
 } rf_ext_params;
 
 /* Create an extended-model engine: h_R double[3N] planar (mm), h_radius double[N].

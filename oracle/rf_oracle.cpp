@@ -849,6 +849,7 @@ struct ExtPar {
     double kn, ks, lambda, gap, wm, sig, tau;
     uint64_t seed;
     double drop;      // post-peak stop: fracture once the stress is below (1 - drop) x peak (0: off)
+    double lgap;      // list gap: 0 lists pairs within a_farcut; g > 0 within min(a_farcut, r_i + r_j + g)
 };
 
 static inline uint64_t mix64(uint64_t z) {
@@ -875,7 +876,7 @@ struct RunExt {
     std::vector<id_t> IL, CI, CIs, pnC;
     std::vector<uint8_t> type;
     std::vector<V3<TF>> Rij, Oijt, Mijn, Mijt;
-    double sz0, aa_farcut, aacut;
+    double sz0, aa_farcut, aacut, a_farcut;
     int status;
     uint64_t steps, broken;
     TF dt, hm_E, hm_G, p_A, mu, mur, kn, ks, lambda, cmass;
@@ -886,6 +887,16 @@ struct RunExt {
     double rr(uint64_t i, uint64_t j) const {
         const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
         return dx * dx + dy * dy + dz * dz;
+    }
+    // squared list cutoffs of a pair (add and delete tests): the reference's float aacut
+    // and double aa_farcut, or with a list gap min(a_farcut, r_i + r_j + g)^2 for both
+    double cut2_add(uint64_t i, uint64_t j) const {
+        if (x.lgap > 0.0) { const double q = std::fmin(a_farcut, (rad[i] + rad[j]) + x.lgap); return q * q; }
+        return aacut;
+    }
+    double cut2_del(uint64_t i, uint64_t j) const {
+        if (x.lgap > 0.0) { const double q = std::fmin(a_farcut, (rad[i] + rad[j]) + x.lgap); return q * q; }
+        return aa_farcut;
     }
     void zero_slot(uint64_t k) {
         Rij[k] = {0, 0, 0}; Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
@@ -904,12 +915,14 @@ struct RunExt {
         const rf_potential& P = t->Po;
         dt = (TF)P.dt; hm_E = (TF)P.hm_E; hm_G = (TF)P.hm_G; p_A = (TF)P.p_A; mu = (TF)P.p_mu; mur = (TF)P.p_mur;
         kn = (TF)x.kn; ks = (TF)x.ks; lambda = (TF)x.lambda; cmass = (TF)(P.p_m / (P.p_r * P.p_r * P.p_r));
-        aa_farcut = P.aa_farcut; aacut = (double)t->aacut;
+        aa_farcut = P.aa_farcut; aacut = (double)t->aacut; a_farcut = P.a_farcut;
         to_float();
         const float inv_a = t->C._1d_a, a = t->C.a;
         int s = cell_distribution<float>(Rf.data(), N, CI.data(), CIs.data(), pnC.data(), CN, inv_a, t->C.Nr);
         if (s) status = s;
-        s = construct_list<float>(Rf.data(), N, CIs.data(), pnC.data(), IL.data(), K, a, inv_a, t->aacut, t->C.Nr, CN);
+        if (x.lgap > 0.0) s = construct_list_pairs();
+        else s = construct_list<float>(Rf.data(), N, CIs.data(), pnC.data(), IL.data(), K, a, inv_a, t->aacut,
+                                       t->C.Nr, CN);
         if (s) status = s;
         // bonds: gap below gap_frac * min radius; FP64 rest length; Weibull strengths per pair
         for (uint64_t i = 0; i < N; ++i)
@@ -927,10 +940,40 @@ struct RunExt {
                 tau[k] = x.tau * std::pow(-std::log(ut), 1.0 / x.wm);
                 if (sizeof(TF) == 4) { sig[k] = (float)sig[k]; tau[k] = (float)tau[k]; }
             }
-        // DeleteFarLinks on the float positions, as the initial build does
-        std::vector<V3<float>> z(N * K, {0, 0, 0});
-        delete_far_links<float>(Rf.data(), N, IL.data(), type.data(), z.data(), z.data(), z.data(), z.data(), K,
-                                (float)P.aa_farcut);
+        // DeleteFarLinks on the float positions, as the initial build does (with a list gap
+        // every listed pair is within its cutoff)
+        if (!(x.lgap > 0.0)) {
+            std::vector<V3<float>> z(N * K, {0, 0, 0});
+            delete_far_links<float>(Rf.data(), N, IL.data(), type.data(), z.data(), z.data(), z.data(), z.data(), K,
+                                    (float)P.aa_farcut);
+        }
+    }
+
+    // construct_list's visiting order (the reference's initial construction) with the pair
+    // cutoff min(a_farcut, r_i + r_j + g) tested on the FP64 positions
+    int construct_list_pairs() {
+        int st = ST_OK;
+        std::fill(IL.begin(), IL.end(), EMPTY);
+        const float inv_a = t->C._1d_a, a = t->C.a;
+        for (uint64_t i = 0; i < N; ++i) {
+            int64_t cells[8];
+            octant_cells<float>(Rf.data(), N, i, a, inv_a, t->C.Nr, cells);
+            uint64_t n = 0;
+            for (int c = 0; c < 8; ++c) {
+                if (cells[c] < 0 || (uint64_t)cells[c] >= CN) { st = ST_CELL_RANGE; continue; }
+                const uint64_t start = pnC[cells[c]], cnt = pnC[cells[c] + CN];
+                for (uint64_t m = 0; m < cnt; ++m) {
+                    if (start + m >= N) break;
+                    const id_t j = CIs[start + m + N];
+                    if (j >= N) continue;
+                    if (rr(i, j) < cut2_add(i, j) && j != i) {
+                        if (n < K) IL[i * K + n] = j; else st = ST_ROW_OVERFLOW;
+                        ++n;
+                    }
+                }
+            }
+        }
+        return st;
     }
 
     void delete_far() {
@@ -940,7 +983,7 @@ struct RunExt {
                 const id_t j = IL[k];
                 if (j == EMPTY || j >= N) continue;
                 const double d2 = rr(i, j);
-                if (d2 > aa_farcut || d2 < 1e-10) { IL[k] = EMPTY; type[k] = 0; zero_slot(k); }
+                if (d2 > cut2_del(i, j) || d2 < 1e-10) { IL[k] = EMPTY; type[k] = 0; zero_slot(k); }
             }
     }
 
@@ -959,7 +1002,7 @@ struct RunExt {
                     const id_t j = CIs[start + m + N];
                     if (j >= N) continue;
                     const double d2 = rr(i, j);
-                    if (!(d2 < aacut && d2 > 1e-10)) continue;
+                    if (!(d2 < cut2_add(i, j) && d2 > 1e-10)) continue;
                     bool have = false;
                     for (uint64_t q = 0; q < K; ++q) if (IL[i * K + q] == j) have = true;
                     if (have) continue;
@@ -1400,7 +1443,7 @@ static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const
     RunExt<TF> r;
     r.t = t;
     r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
-                 xp->post_peak_drop};
+                 xp->post_peak_drop, xp->list_gap};
     r.init(R_io, rad);
     uint64_t ns = 0;
     while (r.running() && r.steps < max_steps) r.step(curve, cap, &ns);   // max_steps 0: bonds only
@@ -1427,7 +1470,7 @@ static int qs_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const doubl
     RunExt<TF> r;
     r.t = t;
     r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
-                 xp->post_peak_drop};
+                 xp->post_peak_drop, xp->list_gap};
     r.init(R_io, rad);
     for (uint64_t k = 0; k < n_inc; ++k) {
         int c = 0;
@@ -1452,7 +1495,7 @@ static void warm_probe(rf_task* t, const rf_ext_params* xp, const double* R0, co
     RunExt<TF> a;
     a.t = t;
     a.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
-                 xp->post_peak_drop};
+                 xp->post_peak_drop, xp->list_gap};
     a.init(R0, rad);
     int c; double res;
     for (uint64_t k = 0; k < n_pre; ++k) a.fire_increment(*p, &c, &res, nullptr, 0);

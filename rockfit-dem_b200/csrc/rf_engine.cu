@@ -94,7 +94,10 @@ struct Consts {
     ExtParams ep;
     float kn, ks, br_lambda, cmass;     // bond stiffness per area, bond radius / min(r_i, r_j), mass = cmass r^3
     double aa_farcut_d, aacut_d;
-    double Top_shift;                   // unused (reserved)
+    // list rule: lgap_d == 0 lists pairs within a_farcut (add test on the float aacut,
+    // delete test on aa_farcut, as the reference); lgap_d > 0 within min(a_farcut, r_i + r_j + g)
+    double a_farcut_d, lgap_d;
+    float lgap_f, skin_f;
 };
 
 // Per-specimen geometry of a batch (constant during a run): the platen's cut height, the
@@ -294,7 +297,13 @@ __global__ void k_rb_cand(Dev d, Consts c) {
                             if (j == i) continue;
                             const float4 xj = posf(d, c, cur, j);
                             const float ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
-                            if (ddx * ddx + ddy * ddy + ddz * ddz < c.rc2) {
+                            const float d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                            bool near = d2 < c.rc2;
+                            if (c.lgap_f > 0.f && near) {
+                                const float q = fminf(c.acut_f, (xi.w + xj.w) + c.lgap_f) + c.skin_f;
+                                near = d2 < q * q;
+                            }
+                            if (near) {
                                 if (n < c.KC) d.cand[(size_t)n * c.N + i] = j;
                                 else raise_status(&d.sc->err, RF_ERR_CAPACITY);
                                 ++n;
@@ -318,13 +327,14 @@ __global__ void k_rb_cand(Dev d, Consts c) {
         }
         d.member[i] = mem;
         // margin of the nearest non-member candidate: until the displacements since this
-        // build add up to it, no candidate can come within a_farcut
+        // build add up to it, no candidate can come within its list cutoff
         float mg = 3.0e38f;
         for (uint32_t q = 0; q < n; ++q) {
             if ((mem >> q) & 1ull) continue;
             const float4 xj = posf(d, c, cur, d.cand[(size_t)q * c.N + i]);
             const float ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
-            mg = fminf(mg, sqrtf(ddx * ddx + ddy * ddy + ddz * ddz) - c.acut_f);
+            const float cut = c.lgap_f > 0.f ? fminf(c.acut_f, (xi.w + xj.w) + c.lgap_f) : c.acut_f;
+            mg = fminf(mg, sqrtf(ddx * ddx + ddy * ddy + ddz * ddz) - cut);
         }
         d.cmargin[i] = mg;
     }
@@ -758,6 +768,23 @@ __device__ __forceinline__ double3 dsub(const double4 a, const double4 b) {
 }
 __device__ __forceinline__ double dlen2(const double3 r) { return r.x * r.x + r.y * r.y + r.z * r.z; }
 
+// Squared list cutoffs of a pair of the extended model (radii ri, rj): the add test and
+// the delete test. With a list gap g the pair's cutoff is min(a_farcut, ri + rj + g).
+__device__ __forceinline__ double cut2_add(const Consts& c, double ri, double rj) {
+    if (c.lgap_d > 0.0) {
+        const double q = fmin(c.a_farcut_d, (ri + rj) + c.lgap_d);
+        return q * q;
+    }
+    return c.aacut_d;
+}
+__device__ __forceinline__ double cut2_del(const Consts& c, double ri, double rj) {
+    if (c.lgap_d > 0.0) {
+        const double q = fmin(c.a_farcut_d, (ri + rj) + c.lgap_d);
+        return q * q;
+    }
+    return c.aa_farcut_d;
+}
+
 __device__ __forceinline__ void delete_far_ext(const Dev& d, const Consts& c, const double4* __restrict__ P,
                                                uint32_t i, const double4 xi, uint32_t ncand, uint32_t nbq,
                                                uint32_t& live, uint32_t& bond, uint32_t& cm, uint32_t& bmask,
@@ -768,8 +795,10 @@ __device__ __forceinline__ void delete_far_ext(const Dev& d, const Consts& c, co
         const uint32_t k = __ffs(m) - 1;
         m &= m - 1;
         const uint32_t j = row[k];
-        const double rr = dlen2(dsub(ldg_d4(&P[j]), xi));
-        if (rr > c.aa_farcut_d || rr < 1e-10) delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
+        const double4 xj = ldg_d4(&P[j]);
+        const double rr = dlen2(dsub(xj, xi));
+        if (rr > cut2_del(c, xi.w, xj.w) || rr < 1e-10)
+            delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
     }
 }
 
@@ -1052,7 +1081,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             const float4 vj = __ldg(&Vv[j]), wj = __ldg(&Wv[j]);
             const double3 rd = dsub(xj, xi);
             const double rr = dlen2(rd);
-            if (rr > c.aa_farcut_d || rr < 1e-10) {
+            if (rr > cut2_del(c, xi.w, xj.w) || rr < 1e-10) {
                 delete_slot(d, c, i, d.bk[s], j, ncand, nbq, live, bond, cm, bmask, mem);
                 continue;
             }
@@ -1088,7 +1117,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             const double4 xj = ldg_d4(&P[j]);
             const double3 rd = dsub(xj, xi);
             const double rr = dlen2(rd);
-            if (with_delete && (rr > c.aa_farcut_d || rr < 1e-10)) {
+            if (with_delete && (rr > cut2_del(c, xi.w, xj.w) || rr < 1e-10)) {
                 delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
                 continue;
             }
@@ -1123,7 +1152,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                 const uint32_t j = __ldg(&d.cand[(size_t)q * N + i]);
                 const double4 xj = ldg_d4(&P[j]);
                 const double rr = dlen2(dsub(xj, xi));
-                if (!(rr < c.aacut_d && rr > 1e-10)) continue;
+                if (!(rr < cut2_add(c, xi.w, xj.w) && rr > 1e-10)) continue;
                 if (!have_cells) { oc = octant_of(xif, c.g); have_cells = true; }
                 const int rank = octant_rank(oc, ref_cell(mk3((float)xj.x, (float)xj.y, (float)xj.z), c.g));
                 if (rank < 0) continue;
@@ -1706,6 +1735,39 @@ struct BondSpec {
     uint64_t seed;
     uint32_t p0, p1;            // its particles
 };
+// Initial rows of the extended model with a list gap g: the reference's construction
+// (md_interaction_list_construct.cu:13-98: the 8 octant cells in visiting order, their
+// occupants in cell order, slots filled in order) with the pair test
+// rr < min(a_farcut, r_i + r_j + g)^2 on the FP64 positions. IL is preset to empty.
+__global__ void k_list_ext(const float* __restrict__ R, const double4* __restrict__ P, uint32_t N,
+                           const uint_fast32_t* __restrict__ CIs, const uint_fast32_t* __restrict__ pnC,
+                           uint_fast32_t* __restrict__ IL, uint32_t K, RefGrid g, double a_farcut, double gap,
+                           uint32_t* err) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        int64_t cells[8];
+        octant_cells(mk3(R[i], R[i + N], R[i + 2 * (size_t)N]), g, cells);
+        const double4 xi = P[i];
+        uint32_t n = 0;
+        for (int c = 0; c < 8; ++c) {
+            if (cells[c] < 0 || (uint64_t)cells[c] >= g.CN) { raise_status(err, RF_ERR_CELL_RANGE); continue; }
+            const uint64_t s = (uint64_t)pnC[cells[c]], cnt = (uint64_t)pnC[cells[c] + g.CN];
+            for (uint64_t m = 0; m < cnt; ++m) {
+                if (s + m >= N) break;
+                const uint_fast32_t j = CIs[s + m + N];
+                if (j >= N) continue;
+                const double4 xj = P[j];
+                const double rr = dlen2(dsub(xj, xi));
+                const double q = fmin(a_farcut, (xi.w + xj.w) + gap);
+                if (rr < q * q && j != i) {
+                    if (n < K) IL[(size_t)i * K + n] = j;
+                    else raise_status(err, RF_ERR_ROW_OVERFLOW);
+                    ++n;
+                }
+            }
+        }
+    }
+}
+
 __global__ void k_bond_ext(const double4* __restrict__ P, const uint_fast32_t* __restrict__ IL,
                            uint8_t* __restrict__ type, float* __restrict__ iL, double* __restrict__ L0x,
                            float2* __restrict__ strx, uint32_t N, uint32_t K, const BondSpec* __restrict__ bs,
@@ -2096,7 +2158,8 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     if (ext) {
         for (uint64_t i = 0; i < t->N; ++i) { rmax = std::max(rmax, h_rad[i]); rmin = std::min(rmin, h_rad[i]); }
         if (!(rmin > 0.0) || !(x->kn > 0.0) || !(x->ks >= 0.0) || !(x->bond_lambda > 0.0) || !(x->weibull_m > 0.0) ||
-            !(x->sigma_c > 0.0) || !(x->tau_c > 0.0) || !(x->post_peak_drop >= 0.0 && x->post_peak_drop < 1.0)) {
+            !(x->sigma_c > 0.0) || !(x->tau_c > 0.0) || !(x->post_peak_drop >= 0.0 && x->post_peak_drop < 1.0) ||
+            !(x->list_gap >= 0.0 && x->list_gap < 1e300)) {
             set_error("rf_engine_create_ext: radii and bond parameters must be positive");
             return RF_ERR_INVALID;
         }
@@ -2137,6 +2200,9 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         c.kn = (float)x->kn; c.ks = (float)x->ks; c.br_lambda = (float)x->bond_lambda;
         c.cmass = (float)(P.p_m / (P.p_r * P.p_r * P.p_r));     // mass = density * 4/3 pi r^3
         c.aa_farcut_d = P.aa_farcut; c.aacut_d = (double)t->aacut;
+        c.a_farcut_d = P.a_farcut;
+        c.lgap_d = x->list_gap;
+        c.lgap_f = (float)x->list_gap;
     }
     c.aacut = t->aacut; c.aa_farcut = (float)P.aa_farcut;
     c.g.a = t->C.a; c.g.inv_a = t->C._1d_a; c.g.nx = t->C.Nr.x; c.g.ny = t->C.Nr.y; c.g.nz = t->C.Nr.z; c.g.CN = t->C.N;
@@ -2151,6 +2217,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     c.disp2 = (float)((0.3 * skin) * (0.3 * skin));   // checked every RF_GRAPH_UNROLL steps
     c.hard2 = (float)((0.5 * skin) * (0.5 * skin));
     c.acut_f = (float)acut;
+    c.skin_f = (float)skin;
     const double hcell = rc * 1.0001;
     c.cg_inv_h = (float)(1.0 / hcell);
     c.cg_ox = (float)(t->S.center.x - t->S.spacesized2.x - hcell);
@@ -2289,10 +2356,25 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             rf_status a = md_CellDistribution(dR, N, dCI, dCIs, dpnC, t->C.N, t->C._1d_a, t->C.Nr, scratch, sb, s);
             if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a) init_dev = a;
         }
-        if (!st2) {
+        const bool pair_cut = ext && x->list_gap > 0.0;
+        if (!st2 && !pair_cut) {
             rf_status a = md_InteractionListConstruct(dR, N, dCIs, dpnC, dIL, K, t->C.a, t->C._1d_a, t->aacut,
                                                       t->C.Nr, t->C.N, s);
             if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a && !init_dev) init_dev = a;
+        }
+        if (!st2 && pair_cut) {
+            uint32_t w = 0;
+            ce = cudaMemsetAsync(dIL, 0xFF, NK * sizeof(uint_fast32_t), s);
+            if (!ce) ce = cudaMemsetAsync(e->maxq_dev, 0, sizeof(uint32_t), s);
+            if (!ce) {
+                k_list_ext<<<(N + 127) / 128, 128, 0, s>>>(dR, d.posd[0], N, dCIs, dpnC, dIL, K, c.g, P.a_farcut,
+                                                           x->list_gap, e->maxq_dev);
+                ce = cudaGetLastError();
+            }
+            if (!ce) ce = cudaMemcpyAsync(&w, e->maxq_dev, sizeof(w), cudaMemcpyDeviceToHost, s);
+            if (!ce) ce = cudaStreamSynchronize(s);
+            if (ce) st2 = cuda_status(ce, "k_list_ext");
+            else if (w && !init_dev) init_dev = (rf_status)w;
         }
         if (!st2 && !ext) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
                                                               Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
@@ -2314,8 +2396,10 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             cudaFree(dbs);
             if (ce) st2 = cuda_status(ce, "k_bond_ext");
         }
-        if (!st2) st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
-                                          (float)P.aa_farcut, s);
+        // (with a list gap every listed pair is within its cutoff: nothing to delete)
+        if (!st2 && !pair_cut)
+            st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
+                                    (float)P.aa_farcut, s);
         if (!st2) {
             // bond records: as many per particle as its row holds bonds (bonds are never created later)
             uint32_t qb = 0;
@@ -2404,9 +2488,10 @@ rf_status rf_engine_create_batch(const rf_task* tasks, const rf_ext_params* xs, 
             tq.Po.aa_farcut != t0.Po.aa_farcut || tq.Po.hm_E != t0.Po.hm_E || tq.Po.hm_G != t0.Po.hm_G ||
             tq.Po.p_A != t0.Po.p_A || tq.Po.p_mu != t0.Po.p_mu || tq.Po.p_mur != t0.Po.p_mur ||
             tq.Po.p_m != t0.Po.p_m || xs[q].kn != xs[0].kn || xs[q].ks != xs[0].ks ||
-            xs[q].bond_lambda != xs[0].bond_lambda || !(xs[q].post_peak_drop >= 0.0 && xs[q].post_peak_drop < 1.0)) {
+            xs[q].bond_lambda != xs[0].bond_lambda || xs[q].list_gap != xs[0].list_gap ||
+            !(xs[q].post_peak_drop >= 0.0 && xs[q].post_peak_drop < 1.0)) {
             set_error("rf_engine_create_batch: specimen %d must have >= 128 particles and the batch's test kind, "
-                      "slots, grid cell, material, time step and bond stiffness, and a post-peak drop in [0, 1)", q);
+                      "slots, grid cell, material, time step, bond stiffness and list gap, and a post-peak drop in [0, 1)", q);
             return RF_ERR_INVALID;
         }
         total += tq.N;

@@ -59,28 +59,72 @@ __global__ void k_bin(Dev d, Par c) {
     }
 }
 // single-block exclusive scan of the cell counts (cells are few: N / ~2)
-__global__ void k_scan(Dev d, Par c) {
-    __shared__ uint32_t wsum[32];
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
+// Exclusive scan of the cell counts into cell starts, in three kernels: per-chunk sums
+// (SCAN_CHUNK cells per block), a one-block scan of the chunk sums, and the chunks'
+// own scans offset by their sums.
+constexpr uint32_t SCAN_CHUNK = 4096;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* wsum, uint32_t* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) { const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += y; }
+    if (lane == 31) wsum[w] = incl;
     __syncthreads();
-    for (uint32_t base = 0; base < c.cells; base += blockDim.x) {
+    if (w == 0) {
+        const uint32_t t = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+        uint32_t ti = t;
+        for (int o = 1; o < 32; o <<= 1) { const uint32_t y = __shfl_up_sync(0xffffffffu, ti, o); if (lane >= o) ti += y; }
+        wsum[lane] = ti - t;
+        if (lane == 31) *total = ti;
+    }
+    __syncthreads();
+    const uint32_t r = wsum[w] + incl - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void k_scan_sums(Dev d, Par c) {
+    __shared__ uint32_t sh[32];
+    const size_t base = (size_t)blockIdx.x * SCAN_CHUNK;
+    uint32_t s = 0;
+    for (uint32_t t = threadIdx.x; t < SCAN_CHUNK; t += blockDim.x)
+        if (base + t < c.cells) s += d.count[base + t];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) d.bsum[blockIdx.x] = v;
+    }
+}
+
+// one block: exclusive scan of the nb chunk sums, in place
+__global__ void k_scan_chunks(Dev d, uint32_t nb) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t total;
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < nb; base += blockDim.x) {
         const uint32_t q = base + threadIdx.x;
+        const uint32_t v = q < nb ? d.bsum[q] : 0;
+        const uint32_t ex = block_excl_scan(v, wsum, &total);
+        if (q < nb) d.bsum[q] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+}
+
+__global__ void k_scan_apply(Dev d, Par c) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t total;
+    const size_t base = (size_t)blockIdx.x * SCAN_CHUNK;
+    uint32_t carry = d.bsum[blockIdx.x];
+    for (uint32_t off = 0; off < SCAN_CHUNK; off += blockDim.x) {
+        const size_t q = base + off + threadIdx.x;
         const uint32_t v = q < c.cells ? d.count[q] : 0;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        uint32_t incl = v;
-        for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += y; }
-        if (lane == 31) wsum[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            uint32_t t = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0, ti = t;
-            for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, ti, o); if (lane >= o) ti += y; }
-            wsum[lane] = ti - t;
-        }
-        __syncthreads();
-        if (q < c.cells) d.start[q] = carry + wsum[w] + incl - v;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry += wsum[w] + incl;
+        const uint32_t ex = block_excl_scan(v, wsum, &total);
+        if (q < c.cells) d.start[q] = carry + ex;
+        carry += total;
         __syncthreads();
     }
 }
@@ -301,6 +345,8 @@ extern "C" rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0,
     if (!e) e = al((void**)&d.start, (size_t)c.cells * 4);
     if (!e) e = al((void**)&d.fill, (size_t)c.cells * 4);
     if (!e) e = al((void**)&d.part, nb * sizeof(double4));
+    const uint32_t nchunks = (c.cells + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    if (!e) e = al((void**)&d.bsum, (size_t)nchunks * sizeof(uint32_t));
     if (!e) e = al((void**)&d.s, sizeof(Scal));
     cudaStream_t st = nullptr;
     if (!e) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -318,7 +364,9 @@ extern "C" rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0,
         for (int it = 0; it < BATCH; ++it) {
             k_zero<<<(c.cells + 255) / 256, 256, 0, st>>>(d, c);
             k_bin<<<nb, 256, 0, st>>>(d, c);
-            k_scan<<<1, 1024, 0, st>>>(d, c);
+            k_scan_sums<<<nchunks, 256, 0, st>>>(d, c);
+            k_scan_chunks<<<1, 1024, 0, st>>>(d, nchunks);
+            k_scan_apply<<<nchunks, 1024, 0, st>>>(d, c);
             k_scatter<<<nb, 256, 0, st>>>(d, c);
             k_cellsort<<<(c.cells + 255) / 256, 256, 0, st>>>(d, c);
             k_force<<<nb, 256, 0, st>>>(d, c);

@@ -111,3 +111,34 @@ def test_post_peak_drop_stop_rule():
     assert p["steps"] == S and np.array_equal(p["R"], o["R"])
     q = oracle.run_ext(mc.clone(t), x, R, rad, S + 50)
     assert q["steps"] == S + 50                        # without the rule the run goes on
+
+
+@pytest.mark.parametrize("gap", [0.1, 0.25])
+def test_list_gap_rows_hold_exactly_the_pairs_within_their_cutoff(gap):
+    """With a list gap g the initial rows hold exactly the pairs within
+    min(a_farcut, r_i + r_j + g) (FP64 distances); the rows are shorter than under the
+    reference's uniform a_farcut, the bonds are the same, and the float-force oracle still
+    tracks the FP64 one."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 5.0, 6.0, min_stress=1e3)
+    N, K = int(t.N), int(t.K)
+    u = oracle.run_ext(mc.clone(t), x, R, rad, 0)
+    x.list_gap = gap * 0.5
+    f = oracle.run_ext(mc.clone(t), x, R, rad, 0)
+    assert f["status"] == 0
+    E = np.iinfo(np.uint64).max
+    IL = f["IL"].reshape(N, K)
+    P = R.reshape(3, N).T
+    a_far = float(t.Po.a_farcut)
+    for i in range(N):
+        d = np.sqrt(((P - P[i]) ** 2).sum(axis=1))
+        cut = np.minimum(a_far, rad[i] + rad + x.list_gap)
+        want = set(np.flatnonzero((d ** 2 < cut ** 2) & (np.arange(N) != i)).tolist())
+        got = set(int(j) for j in IL[i] if j != E)
+        assert got == want, i
+    assert (f["IL"] != E).sum() < (u["IL"] != E).sum()
+    assert int(np.count_nonzero(f["ILtype"])) == int(np.count_nonzero(u["ILtype"]))
+    steps = 150
+    a = oracle.run_ext(mc.clone(t), x, R, rad, steps)
+    b = oracle.run_ext(mc.clone(t), x, R, rad, steps, fp64=True)
+    assert a["status"] == 0 and b["status"] == 0
+    assert np.max(np.abs(a["R"] - b["R"])) < 1e-6 * float(np.max(R) - np.min(R))

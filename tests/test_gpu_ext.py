@@ -108,10 +108,12 @@ def test_autotune_leaves_results_unchanged(cuda):
     a.close(); b.close()
 
 
-def test_ext_log_uniform_radius_ratio_3_vs_oracle(cuda):
+@pytest.mark.parametrize("gap", [0.0, 0.5], ids=["uniform-cutoff", "list-gap"])
+def test_ext_log_uniform_radius_ratio_3_vs_oracle(cuda, gap):
     """Radii log-uniform in [0.5, 1.5] r0 (radius ratio 3): the packer keeps the range and
     the overlap bound, the list cutoff widens to just past 2 r_max, and the engine's step
-    equals the float oracle's bit for bit."""
+    equals the float oracle's bit for bit, with the uniform cutoff and with a list gap
+    of 0.5 r0 (pair cutoff min(a_farcut, r_i + r_j + g))."""
     N, r0 = 3000, 0.25
     R0, rad, D, H, mo = rfdem.pack_cylinder(N, r0, rmin=0.5, rmax=1.5, aspect=2.0, phi=0.55,
                                             seed=0xB2000000 + 5001, dist="log-uniform")
@@ -123,6 +125,7 @@ def test_ext_log_uniform_radius_ratio_3_vs_oracle(cuda):
     t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, r0, min_stress=1e3)
     assert abs(t.Po.a_farcut - 2.02 * rad.max()) < 1e-12
     x = rfdem.ext_params_si()
+    x.list_gap = gap * r0
     steps = 300
     o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
     res, st = run_engine_ext(t, x, R, rad, steps)
@@ -131,4 +134,20 @@ def test_ext_log_uniform_radius_ratio_3_vs_oracle(cuda):
     assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
     assert np.array_equal(st["ILtype"], o["ILtype"])
     rows = (st["IL"].reshape(N, -1) != rfdem.EMPTY).sum(axis=1)
-    print("radius ratio 3: slots per row mean %.1f max %d of %d" % (rows.mean(), rows.max(), int(t.K)))
+    print("radius ratio 3, list gap %g r0: slots per row mean %.1f max %d of %d" % (gap, rows.mean(), rows.max(),
+                                                                                  int(t.K)))
+
+
+def test_ext_list_gap_lattice_vs_oracle(cuda):
+    """A list gap on the lattice specimen (both test kinds' code paths share it): engine ==
+    float oracle bit for bit over steps that break bonds and form contacts."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_BRAZIL, 10.0, 4.0, min_stress=1e3)
+    x.list_gap = 0.1
+    steps = 300
+    o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
+    res, st = run_engine_ext(t, x, R, rad, steps)
+    assert res.steps == o["steps"] == steps and res.error == 0 and o["status"] == 0
+    assert np.array_equal(st["R64"], o["R"])
+    assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
+    assert np.array_equal(st["ILtype"], o["ILtype"])
+    assert res.broken_bonds == o["broken"]

@@ -340,7 +340,7 @@ def run_fire(rfdem, torch, t, R, rad, x, seed):
             "warm_start_includes": "feature build + MLP forward (tcgen05 BF16) per load step"}
 
 
-BATCH_SPECIMENS, BATCH_STEPS, BATCH_FULL_CAP = 64, 1000, 600000
+BATCH_SPECIMENS, BATCH_STEPS, BATCH_FULL_CAP = 64, 1000, 300000
 
 
 def run_batch_to_failure(rfdem, torch, tasks, params, Rs, rads, counts, t_pack, cap=BATCH_FULL_CAP):

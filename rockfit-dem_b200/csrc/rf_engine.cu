@@ -1139,7 +1139,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     contact_pass(true);
 
     bool replay = false;
-    if (valid && !(MODE == 0 && scan_not_needed(d, c, i, (float)xi.x, (float)xi.y, (float)xi.z))) {
+    if (valid && !scan_not_needed(d, c, i, (float)xi.x, (float)xi.y, (float)xi.z)) {
         unsigned long long tried = mem;
         bool have_cells = false;
         Octant oc;
@@ -1351,6 +1351,7 @@ __global__ void k_fire_update(Dev d, Consts c) {
     const bool stop = sc->fstop != 0;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t moved = 0;
+    float e2max = 0.f;
     if (!stop && i < c.N) {
         double4 x = d.posd[cur][i];
         float4 v = d.vel[cur][i], w = d.ang[cur][i];
@@ -1384,7 +1385,9 @@ __global__ void k_fire_update(Dev d, Consts c) {
         const float e2 = ex * ex + ey * ey + ez * ez;
         moved = (e2 > c.disp2) ? 1u : 0u;
         if (e2 > c.hard2) raise_status(&d.sc->err, RF_ERR_CAPACITY);   // lists may have missed a neighbour
+        e2max = e2;
     }
+    note_displacement(d, e2max);           // every lane of the warp takes part
     __shared__ bool s_last;
     __shared__ uint32_t s_m;
     if (threadIdx.x == 0) s_m = 0;
@@ -1400,8 +1403,10 @@ __global__ void k_fire_update(Dev d, Consts c) {
     if (!s_last || threadIdx.x != 0) return;
     __threadfence();
     sc->block_counter = 0;
-    sc->dmax = 3.0e38f;          // FIRE moves particles outside the step kernel: no scan skipping
-    sc->d2max_next = 0;          // until the next build or explicit step measures it again
+    // largest displacement since the last candidate build of the positions the next force
+    // pass reads (this update wrote them): the force pass's add-pass scan skip uses it
+    sc->dmax = sqrtf(__uint_as_float(sc->d2max_next));
+    sc->d2max_next = 0;
     const uint32_t mv = sc->moved;
     sc->moved = 0;
     sc->rebuild = mv;
@@ -1438,6 +1443,8 @@ __global__ void k_qs_begin_scalars(Dev d, Consts c, double delta) {
         sc->fcv = 1.0; sc->fcf = 0.0; sc->fcm = 0.0;
         sc->fwarm = 1;
         sc->done = 0;
+        sc->dmax = 3.0e38f;        // the increment moves particles (platen, warm start): the first pass scans
+        sc->d2max_next = 0;
         sc->rebuild = 1;          // positions jumped (platen clamp, warm start): rebuild the candidates
     }
 }

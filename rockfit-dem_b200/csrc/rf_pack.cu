@@ -224,11 +224,28 @@ __global__ void k_force(Dev d, Par c) {
     }
 }
 
-// FIRE step decision (one thread): power, time step, mixing factor.
+// FIRE step decision (one block): sums of the block partials in a fixed order (thread t
+// adds partials t, t + blockDim, ...; then a fixed tree), then power, time step and
+// mixing factor on thread 0.
 __global__ void k_fire_decide(Dev d, Par c, int nblocks) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double sh[4][32];
     double fv = 0, ff = 0, vv = 0, mo = 0;
-    for (int b = 0; b < nblocks; ++b) { const double4 p = d.part[b]; fv += p.x; ff += p.y; vv += p.z; mo = fmax(mo, p.w); }
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        const double4 p = d.part[b];
+        fv += p.x; ff += p.y; vv += p.z; mo = fmax(mo, p.w);
+    }
+    for (int o = 16; o; o >>= 1) {
+        fv += __shfl_xor_sync(0xffffffffu, fv, o);
+        ff += __shfl_xor_sync(0xffffffffu, ff, o);
+        vv += __shfl_xor_sync(0xffffffffu, vv, o);
+        mo = fmax(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { sh[0][w] = fv; sh[1][w] = ff; sh[2][w] = vv; sh[3][w] = mo; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    fv = 0; ff = 0; vv = 0; mo = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { fv += sh[0][q]; ff += sh[1][q]; vv += sh[2][q]; mo = fmax(mo, sh[3][q]); }
     Scal* s = d.s;
     s->fdotv = fv; s->ff = ff; s->vv = vv; s->maxov = mo;
     if (fv > 0) {
@@ -370,7 +387,7 @@ extern "C" rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0,
             k_scatter<<<nb, 256, 0, st>>>(d, c);
             k_cellsort<<<(c.cells + 255) / 256, 256, 0, st>>>(d, c);
             k_force<<<nb, 256, 0, st>>>(d, c);
-            k_fire_decide<<<1, 32, 0, st>>>(d, c, nb);
+            k_fire_decide<<<1, 1024, 0, st>>>(d, c, nb);
             k_fire_update<<<nb, 256, 0, st>>>(d, c);
         }
         e = cudaStreamEndCapture(st, &graph);

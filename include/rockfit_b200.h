@@ -521,7 +521,9 @@ rf_status rf_specimen_lattice_disc(uint64_t seed, double p_r, double gap_frac, d
  * container wall) while the radii grow in stages to their targets, until the largest
  * overlap is below 2e-4 of the smaller radius. Outputs: R double[3N] planar (centred at
  * center, mm), radius double[N] (mm), the container's diameter and height (mm), and the
- * final largest relative overlap. aspect 0.5 gives a Brazilian disc (axis z).
+ * final largest relative overlap. aspect 0.5 gives a Brazilian disc (axis z). Particles
+ * are numbered in spatial order (cells of 6 r0, x fastest, then y, then z), which keeps
+ * neighbours close in memory.
  */
 rf_status rf_pack_cylinder(uint64_t seed, uint64_t N, double r0, double rmin, double rmax, double aspect,
                            double phi, const double center[3], double* R, double* radius,

@@ -5,6 +5,7 @@
 // (histogram, scan, scatter). Each FIRE iteration is two fused kernels (forces with the
 // power and norm partials; then the per-particle FIRE update), the scalar FIRE state
 // lives on the device and batches of iterations are captured in a CUDA graph.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -421,11 +422,29 @@ extern "C" rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0,
     if (st) cudaStreamDestroy(st);
     for (void* p : allocs) cudaFree(p);
     if (e) return cuda_status(e, "rf_pack_cylinder");
-    for (uint64_t i = 0; i < N; ++i) {
-        R[i] = center[0] + r0 * hx[i].x;
-        R[i + N] = center[1] + r0 * hx[i].y;
-        R[i + 2 * N] = center[2] + r0 * hx[i].z;
-        radius[i] = r0 * hx[i].w;
+    // number the particles in spatial order (cells of 6 r0, x fastest, then y, then z;
+    // packing order within a cell), so that a particle's neighbours sit close to it in
+    // memory and the step kernels' neighbour gathers hit the caches
+    std::vector<uint64_t> key(N), order(N);
+    {
+        const double h = 6.0;
+        const double x0 = -Rc, y0 = -Rc, z0 = -Hh;
+        const uint64_t nx = (uint64_t)std::ceil(2.0 * Rc / h) + 2, ny = nx;
+        for (uint64_t i = 0; i < N; ++i) {
+            const double fx = std::floor((hx[i].x - x0) / h), fy = std::floor((hx[i].y - y0) / h),
+                         fz = std::floor((hx[i].z - z0) / h);
+            const uint64_t cx = fx < 0 ? 0 : (uint64_t)fx, cy = fy < 0 ? 0 : (uint64_t)fy, cz = fz < 0 ? 0 : (uint64_t)fz;
+            key[i] = cx + nx * (cy + ny * cz);
+            order[i] = i;
+        }
+        std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return key[a] < key[b]; });
+    }
+    for (uint64_t q = 0; q < N; ++q) {
+        const double4& p = hx[order[q]];
+        R[q] = center[0] + r0 * p.x;
+        R[q + N] = center[1] + r0 * p.y;
+        R[q + 2 * N] = center[2] + r0 * p.z;
+        radius[q] = r0 * p.w;
     }
     if (diameter) *diameter = r0 * D;
     if (height) *height = r0 * H;

@@ -116,3 +116,19 @@ def test_batch_post_peak_drop_stop(cuda):
         s = 0.5 * (np.abs(c[:, 1]) + np.abs(c[:, 2]))
         assert s[-1] < 0.5 * s.max()
     e.close()
+
+
+def test_sharded_run_matches_the_batch(cuda):
+    """rfdem.shard on one rank: the rank's share (all specimens) runs in one batched
+    engine, and the gathered table equals the batch's own per-specimen results."""
+    from rfdem.shard import RESULT_FIELDS, run_sharded
+    specs = _specimens(short=1)
+    tasks, params, Rs, rads = [s[0] for s in specs], [s[3] for s in specs], [s[1] for s in specs], [s[2] for s in specs]
+    table = run_sharded(tasks, params, Rs, rads, steps=200)
+    e = rfdem.BatchEngine(tasks, params, Rs, rads)
+    e.step(200)
+    for q in range(3):
+        _, r = e.sync_spec(q)
+        assert [float(getattr(r, f)) for f in RESULT_FIELDS] == table[q].tolist()
+    e.close()
+    assert table[1][0] < 200 and table[0][0] == table[2][0] == 200

@@ -539,6 +539,51 @@ rf_status rf_pack_cylinder_dist(uint64_t seed, uint64_t N, double r0, double rmi
                                 double* diameter, double* height, double* max_overlap);
 
 /* ------------------------------------------------------------------------ */
+/* State files                                                               */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * The reference's binary state dump, byte for byte: SaveAllData / LoadAllData
+ * (md_savealldata.cpp:12-91; write_sample_data :98-111, write_particle_data :127-142,
+ * write_interaction_list_data :176-199). id_bytes is the width of uint_fast32_t in the
+ * build that reads or wrote the file: 4 for the reference's own (MSVC) build, 8 for a
+ * Linux build. The sample's R0 and H0 are written as three floats each, as the
+ * reference does: (R0, H0, Vgenmax) and (H0, Vgenmax, the 4 bytes after Vgenmax, which
+ * hold the sample's PN with 4-byte ids and padding (0 here) with 8-byte ids). Arrays in
+ * the reference layout: F, V, R, M, W float[3N] planar, Q float[4N], IL, ILtype,
+ * _1d_iL [N*K], the slot vectors rf_float3[N*K]; a NULL array is written as zeros
+ * (R, IL and ILtype are required).
+ */
+rf_status rf_save_all_data(const char* path, int id_bytes, const rf_sample* S, uint64_t pn, uint64_t N, uint32_t K,
+                           float acut, const float* F, const float* V, const float* R, const float* M,
+                           const float* W, const float* Q, const uint_fast32_t* IL, const uint8_t* ILtype,
+                           const float* _1d_iL, const rf_float3* Rij, const rf_float3* Oijt, const rf_float3* Fijn,
+                           const rf_float3* Fijt, const rf_float3* Mijn, const rf_float3* Mijt,
+                           const rf_float3* Mijadd);
+/* Read a file of rf_save_all_data / SaveAllData. Call with R == NULL to learn N and K
+   (and S, pn, acut), then again with buffers of those sizes (NULL arrays other than R,
+   IL, ILtype are skipped). Like LoadAllData, S's real extents (A_real, B_real,
+   size_real, center_real) are recomputed from the loaded positions. */
+rf_status rf_load_all_data(const char* path, int id_bytes, rf_sample* S, uint64_t* pn, uint64_t* N, uint32_t* K,
+                           float* acut, float* F, float* V, float* R, float* M, float* W, float* Q,
+                           uint_fast32_t* IL, uint8_t* ILtype, float* _1d_iL, rf_float3* Rij, rf_float3* Oijt,
+                           rf_float3* Fijn, rf_float3* Fijt, rf_float3* Mijn, rf_float3* Mijt, rf_float3* Mijadd);
+/* LAMMPS data text of SaveLammpsDATASimple (md_savelammpsdata.cpp:8-74): box and atoms in
+   metres, per-atom translational / rotational / total kinetic energy in joules (zeros
+   unless with_energy), one bond line per directed bond slot. */
+rf_status rf_save_lammps_data(const char* path, const rf_task* t, uint64_t N, uint32_t K, const float* R,
+                              const float* V, const float* W, const uint_fast32_t* IL, const uint8_t* ILtype,
+                              int with_energy);
+/*
+ * Versioned checkpoint of a reference-model engine: a header ("RFB2CKPT", version 1, id
+ * width, the rf_task as rf_engine_sync returns it) followed by the rf_save_all_data
+ * payload of the engine's exported state. rf_engine_restore makes an engine from such a
+ * file whose steps continue the saved run bit for bit (the load curve restarts).
+ */
+rf_status rf_engine_checkpoint(rf_engine* e, const char* path);
+rf_status rf_engine_restore(const char* path, rf_engine** out);
+
+/* ------------------------------------------------------------------------ */
 /* BF16 tensor-core GEMM (tcgen05, FP32 accumulation in tensor memory) and the */
 /* warm-start MLP. No reference counterpart.                                  */
 /* ------------------------------------------------------------------------ */

@@ -9,6 +9,9 @@ Build recipe for the checkers:
   harness ``oracle/ref/ref_gpu_harness.cu``.
 * ``oracle/_ref/libmdref_cpu.so`` -- the reference's own CPU bond-force function
   (md_calculateforcesbpm_cpu.cpp) plus ``oracle/ref/ref_cpu_harness.cpp``.
+* ``oracle/_ref/libmdref_io.so`` -- the reference's own state writers
+  (md_savelammpsdata.cpp, md_savealldata.cpp, the latter with ``-include cstring``,
+  which its source needs on Linux) plus ``oracle/ref/ref_io_harness.cpp``.
 
 The ``_ref`` builds read the reference sources where they lie (``--ref`` or
 ``$RF_REFERENCE_DIR``, default ``/root/reference``) and are skipped when that tree
@@ -41,6 +44,7 @@ REF_GPU_SOURCES = [
     "md_results.cu",
 ]
 REF_CPU_SOURCES = ["md_calculateforcesbpm_cpu.cpp"]
+REF_IO_SOURCES = ["md_savelammpsdata.cpp", "md_savealldata.cpp"]
 
 
 def _run(cmd, cwd=None):
@@ -99,6 +103,13 @@ def build_ref(ref_dir=None, force=False, gpu=True, cpu=True):
             _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-I" + CUDA_INC] + inc + forced +
                  ["-o", out] + srcs + [harness, "-lpthread"])
         outs["cpu"] = out
+        out = os.path.join(REF_OUT, "libmdref_io.so")
+        srcs = [os.path.join(ref_dir, s) for s in REF_IO_SOURCES]
+        harness = os.path.join(HERE, "ref", "ref_io_harness.cpp")
+        if force or not _newer(out, srcs + [harness, __file__]):
+            _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-include", "cstring", "-I" + CUDA_INC] + inc +
+                 forced + ["-o", out] + srcs + [harness, "-L/usr/local/cuda/lib64", "-lcudart"])
+        outs["io"] = out
     return outs
 
 

@@ -19,7 +19,7 @@ INCLUDE = os.path.join(HERE, "..", "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CU_SOURCES = ["rf_md_kernels.cu", "rf_engine.cu", "rf_pack.cu", "rf_mlp.cu"]
-CXX_SOURCES = ["rf_host.cpp"]
+CXX_SOURCES = ["rf_host.cpp", "rf_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-ffp-contract=off", "-I" + INCLUDE]

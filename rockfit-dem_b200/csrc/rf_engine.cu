@@ -31,6 +31,7 @@
 // kernel, so one graph launch advances many steps without host round trips.
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <vector>
 #include <algorithm>
 #include <cuda_bf16.h>
@@ -2154,8 +2155,18 @@ void fill_scalars(DevScalars& h, const rf_task& t) {
     h.done = (K_.Strain < K_.MaxStrain && !K_.Fracture) ? 0u : 1u;
 }
 
+// Rows given in the reference layout (a restored checkpoint) instead of built from the
+// positions: the engine sizes its bond records for them.
+struct RowsIn {
+    const uint_fast32_t* IL;
+    const uint8_t* ILtype;
+    const float* iL;
+    const rf_float3 *Rij, *Oijt, *Mijn, *Mijt;
+};
+
 rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h_Rd, const double* h_rad,
-                             const rf_ext_params* x, rf_engine** out, const BatchIn* bin = nullptr) {
+                             const rf_ext_params* x, rf_engine** out, const BatchIn* bin = nullptr,
+                             const RowsIn* rows = nullptr) {
     const bool ext = x != nullptr;
     if (!t || !out || t->N == 0 || t->K == 0 || (ext ? (!h_Rd || !h_rad) : !h_R)) {
         set_error("rf_engine_create: bad arguments");
@@ -2364,7 +2375,17 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a) init_dev = a;
         }
         const bool pair_cut = ext && x->list_gap > 0.0;
-        if (!st2 && !pair_cut) {
+        if (!st2 && rows) {
+            ce = cudaMemcpyAsync(dIL, rows->IL, NK * sizeof(uint_fast32_t), cudaMemcpyHostToDevice, s);
+            if (!ce) ce = cudaMemcpyAsync(dT, rows->ILtype, NK, cudaMemcpyHostToDevice, s);
+            if (!ce) ce = cudaMemcpyAsync(dIL_f, rows->iL, NK * sizeof(float), cudaMemcpyHostToDevice, s);
+            const rf_float3* src[4] = {rows->Rij, rows->Oijt, rows->Mijn, rows->Mijt};
+            rf_float3* dst[4] = {Rij, Oijt, Mijn, Mijt};
+            for (int q = 0; q < 4 && !ce; ++q)
+                ce = cudaMemcpyAsync(dst[q], src[q], NK * sizeof(rf_float3), cudaMemcpyHostToDevice, s);
+            if (ce) st2 = cuda_status(ce, "engine rows");
+        }
+        if (!st2 && !pair_cut && !rows) {
             rf_status a = md_InteractionListConstruct(dR, N, dCIs, dpnC, dIL, K, t->C.a, t->C._1d_a, t->aacut,
                                                       t->C.Nr, t->C.N, s);
             if (a != RF_OK && a != RF_ERR_CELL_RANGE && a != RF_ERR_ROW_OVERFLOW) st2 = a; else if (a && !init_dev) init_dev = a;
@@ -2383,7 +2404,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             if (ce) st2 = cuda_status(ce, "k_list_ext");
             else if (w && !init_dev) init_dev = (rf_status)w;
         }
-        if (!st2 && !ext) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
+        if (!st2 && !ext && !rows) st2 = md_ConstructBoundInteractions(dR, dV, dV, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt,
                                                               Mijadd, N, K, (float)P.b_dd, (float)P.b_r, s);
         if (!st2 && ext) {
             std::vector<BondSpec> hbs(nspec);
@@ -2404,7 +2425,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             if (ce) st2 = cuda_status(ce, "k_bond_ext");
         }
         // (with a list gap every listed pair is within its cutoff: nothing to delete)
-        if (!st2 && !pair_cut)
+        if (!st2 && !pair_cut && !rows)
             st2 = md_DeleteFarLinks(dR, N, dIL, dT, dIL_f, Rij, Oijt, Fijn, Fijt, Mijn, Mijt, Mijadd, K,
                                     (float)P.aa_farcut, s);
         if (!st2) {
@@ -3023,6 +3044,105 @@ rf_status rf_engine_curve_spec(rf_engine* e, int spec, double* curve, uint64_t c
         RF_CUDA(cudaMemcpy(curve, e->d.curve + 3 * (size_t)spec * e->c.curve_cap, 3 * m * sizeof(double),
                            cudaMemcpyDeviceToHost));
     }
+    return RF_OK;
+}
+
+}  // extern "C"
+
+// Checkpoint files: header, the rf_task, the SaveAllData payload (rf_io.cpp).
+namespace rf {
+rf_status io_write_all(std::ostream& f, int id_bytes, const rf_sample* S, uint64_t pn, uint64_t N, uint32_t K,
+                       float acut, const float* F, const float* V, const float* R, const float* M, const float* W,
+                       const float* Q, const uint_fast32_t* IL, const uint8_t* ILtype, const float* _1d_iL,
+                       const rf_float3* Rij, const rf_float3* Oijt, const rf_float3* Fijn, const rf_float3* Fijt,
+                       const rf_float3* Mijn, const rf_float3* Mijt, const rf_float3* Mijadd);
+rf_status io_read_all(std::istream& f, int id_bytes, rf_sample* S, uint64_t* pn, uint64_t* N_out, uint32_t* K_out,
+                      float* acut, float* F, float* V, float* R, float* M, float* W, float* Q, uint_fast32_t* IL,
+                      uint8_t* ILtype, float* _1d_iL, rf_float3* Rij, rf_float3* Oijt, rf_float3* Fijn,
+                      rf_float3* Fijt, rf_float3* Mijn, rf_float3* Mijt, rf_float3* Mijadd);
+}  // namespace rf
+
+namespace {
+const char kCkptMagic[8] = {'R', 'F', 'B', '2', 'C', 'K', 'P', 'T'};
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, id_bytes, model, reserved;
+    uint64_t task_bytes;
+};
+}  // namespace
+
+extern "C" {
+
+rf_status rf_engine_checkpoint(rf_engine* e, const char* path) {
+    if (!e || !path) { set_error("rf_engine_checkpoint: bad arguments"); return RF_ERR_INVALID; }
+    if (e->c.ext) {
+        set_error("rf_engine_checkpoint: the reference model only (the extended model has no reference layout)");
+        return RF_ERR_STATE;
+    }
+    rf_task t;
+    rf_run_result r;
+    TRY(rf_engine_sync(e, &t, &r));
+    const uint64_t N = e->c.N, K = e->c.K, NK = N * K;
+    std::vector<float> R(3 * N), V(3 * N), W(3 * N), iL(NK);
+    std::vector<uint_fast32_t> IL(NK);
+    std::vector<uint8_t> ty(NK);
+    std::vector<rf_float3> Rij(NK), Oijt(NK), Mijn(NK), Mijt(NK);
+    TRY(rf_engine_export(e, R.data(), V.data(), W.data(), IL.data(), ty.data(), iL.data(), Rij.data(), Oijt.data(),
+                         Mijn.data(), Mijt.data()));
+    std::ofstream f(path, std::ios::out | std::ios::binary | std::ios::trunc);
+    if (!f) { set_error("rf_engine_checkpoint: cannot open %s", path); return RF_ERR_INVALID; }
+    CkptHeader h;
+    std::memcpy(h.magic, kCkptMagic, 8);
+    h.version = 1; h.id_bytes = (uint32_t)sizeof(uint_fast32_t); h.model = 0; h.reserved = 0;
+    h.task_bytes = sizeof(rf_task);
+    f.write((const char*)&h, sizeof(h));
+    f.write((const char*)&t, sizeof(t));
+    TRY(io_write_all(f, (int)sizeof(uint_fast32_t), &t.S, 0, N, (uint32_t)K, t.acut, nullptr, V.data(), R.data(),
+                     nullptr, W.data(), nullptr, IL.data(), ty.data(), iL.data(), Rij.data(), Oijt.data(), nullptr,
+                     nullptr, Mijn.data(), Mijt.data(), nullptr));
+    f.close();
+    if (!f) { set_error("rf_engine_checkpoint: write to %s failed", path); return RF_ERR_INVALID; }
+    return RF_OK;
+}
+
+rf_status rf_engine_restore(const char* path, rf_engine** out) {
+    if (!path || !out) { set_error("rf_engine_restore: bad arguments"); return RF_ERR_INVALID; }
+    *out = nullptr;
+    std::ifstream f(path, std::ios::in | std::ios::binary);
+    if (!f) { set_error("rf_engine_restore: cannot open %s", path); return RF_ERR_INVALID; }
+    CkptHeader h;
+    f.read((char*)&h, sizeof(h));
+    if (!f || std::memcmp(h.magic, kCkptMagic, 8) != 0 || h.version != 1 || h.model != 0 ||
+        h.id_bytes != sizeof(uint_fast32_t) || h.task_bytes != sizeof(rf_task)) {
+        set_error("rf_engine_restore: %s is not a version-1 checkpoint of this build", path);
+        return RF_ERR_INVALID;
+    }
+    rf_task t;
+    f.read((char*)&t, sizeof(t));
+    const std::streampos body = f.tellg();
+    uint64_t N = 0;
+    uint32_t K = 0;
+    TRY(io_read_all(f, (int)h.id_bytes, nullptr, nullptr, &N, &K, nullptr, nullptr, nullptr, nullptr, nullptr,
+                    nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                    nullptr));
+    if (N != t.N || K != t.K) { set_error("rf_engine_restore: the payload does not match the task"); return RF_ERR_INVALID; }
+    const uint64_t NK = N * K;
+    std::vector<float> R(3 * N), V(3 * N), W(3 * N), iL(NK);
+    std::vector<uint_fast32_t> IL(NK);
+    std::vector<uint8_t> ty(NK);
+    std::vector<rf_float3> Rij(NK), Oijt(NK), Mijn(NK), Mijt(NK);
+    f.clear();
+    f.seekg(body);
+    TRY(io_read_all(f, (int)h.id_bytes, nullptr, nullptr, &N, &K, nullptr, nullptr, V.data(), R.data(), nullptr,
+                    W.data(), nullptr, IL.data(), ty.data(), iL.data(), Rij.data(), Oijt.data(), nullptr, nullptr,
+                    Mijn.data(), Mijt.data(), nullptr));
+    RowsIn rows{IL.data(), ty.data(), iL.data(), Rij.data(), Oijt.data(), Mijn.data(), Mijt.data()};
+    rf_engine* e = nullptr;
+    TRY(engine_create_impl(&t, R.data(), nullptr, nullptr, nullptr, &e, nullptr, &rows));
+    const rf_status st = rf_engine_import(e, R.data(), V.data(), W.data(), IL.data(), ty.data(), iL.data(), Rij.data(),
+                                          Oijt.data(), Mijn.data(), Mijt.data());
+    if (st != RF_OK) { rf_engine_destroy(e); return st; }
+    *out = e;
     return RF_OK;
 }
 

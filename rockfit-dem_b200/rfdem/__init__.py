@@ -160,6 +160,11 @@ _proto = {
     "rf_engine_step_host": (i32, [P, P, u64, P]),
     "rf_engine_sync": (i32, [P, C.POINTER(Task), C.POINTER(RunResult)]),
     "rf_engine_export": (i32, [P] + [P] * 10),
+    "rf_save_all_data": (i32, [C.c_char_p, i32, C.POINTER(Sample), u64, u64, C.c_uint32, f32] + [P] * 16),
+    "rf_load_all_data": (i32, [C.c_char_p, i32, C.POINTER(Sample), P, P, P, P] + [P] * 16),
+    "rf_save_lammps_data": (i32, [C.c_char_p, C.POINTER(Task), u64, C.c_uint32, P, P, P, P, P, i32]),
+    "rf_engine_checkpoint": (i32, [P, C.c_char_p]),
+    "rf_engine_restore": (i32, [C.c_char_p, P]),
     "rf_engine_import": (i32, [P] + [P] * 10),
     "rf_engine_curve": (i32, [P, P, u64, P]),
     "rf_engine_counters": (i32, [P, P, i32]),
@@ -373,6 +378,22 @@ def make_test_ext(kind, R0, radius, r0, K=32, potential=None, margin=None, v_loa
 
 class Engine:
     """The fused engine on the current CUDA device."""
+
+    @classmethod
+    def restore(cls, path):
+        """An engine from a checkpoint file (rf_engine_restore) continuing the saved run."""
+        h = P()
+        check(lib.rf_engine_restore(os.fsencode(path), C.byref(h)), "rf_engine_restore")
+        e = cls.__new__(cls)
+        e.h = h
+        e.ext = False
+        t, _ = e.sync()
+        e.task, e.N, e.K = t, int(t.N), int(t.K)
+        return e
+
+    def checkpoint(self, path):
+        """Write a checkpoint file (rf_engine_checkpoint)."""
+        check(lib.rf_engine_checkpoint(self.h, os.fsencode(path)), "rf_engine_checkpoint")
 
     def __init__(self, task, R, ext=None, radius=None):
         self.task = task
@@ -607,3 +628,50 @@ class BatchEngine(Engine):
         buf = np.zeros(3 * max(m, 1), np.float64)
         check(lib.rf_engine_curve_spec(self.h, s, buf.ctypes.data, m, C.byref(n)), "rf_engine_curve_spec")
         return buf[:3 * m].reshape(m, 3)
+
+
+# --- state files ---------------------------------------------------------------
+_ALL_PARTICLE = ["F", "V", "R", "M", "W"]
+_ALL_SLOTS = ["Rij", "Oijt", "Fijn", "Fijt", "Mijn", "Mijt", "Mijadd"]
+
+
+def save_all_data(path, sample, st, N, K, acut, pn=0, id_bytes=4):
+    """The reference's SaveAllData file (rf_save_all_data) from a state dict in the
+    reference layout (keys R, V, W, IL, ILtype, iL, Rij, Oijt, Mijn, Mijt as Engine.export
+    returns them; optional F, M, Q, Fijn, Fijt, Mijadd; missing arrays are written as zeros)."""
+    def a(k, dt):
+        return None if st.get(k) is None else np.ascontiguousarray(st[k], dt)
+    arrs = [a(k, np.float32) for k in _ALL_PARTICLE] + [a("Q", np.float32), a("IL", ID_NP), a("ILtype", np.uint8),
+                                                         a("iL", np.float32)] + [a(k, np.float32) for k in _ALL_SLOTS]
+    check(lib.rf_save_all_data(os.fsencode(path), id_bytes, C.byref(sample), pn, N, K, acut,
+                               *[ptr(x) for x in arrs]), "rf_save_all_data")
+
+
+def load_all_data(path, id_bytes=4):
+    """Read a SaveAllData file: returns (Sample, pn, acut, N, K, state dict)."""
+    S, pn, N, K, ac = Sample(), C.c_uint64(0), C.c_uint64(0), C.c_uint32(0), C.c_float(0)
+    nul = [None] * 16
+    check(lib.rf_load_all_data(os.fsencode(path), id_bytes, C.byref(S), C.byref(pn), C.byref(N), C.byref(K),
+                               C.byref(ac), *nul), "rf_load_all_data")
+    n, k = int(N.value), int(K.value)
+    st = {key: np.zeros(3 * n, np.float32) for key in _ALL_PARTICLE}
+    st["Q"] = np.zeros(4 * n, np.float32)
+    st["IL"] = np.zeros(n * k, ID_NP)
+    st["ILtype"] = np.zeros(n * k, np.uint8)
+    st["iL"] = np.zeros(n * k, np.float32)
+    for key in _ALL_SLOTS:
+        st[key] = np.zeros(3 * n * k, np.float32)
+    order = _ALL_PARTICLE + ["Q", "IL", "ILtype", "iL"] + _ALL_SLOTS
+    check(lib.rf_load_all_data(os.fsencode(path), id_bytes, C.byref(S), C.byref(pn), C.byref(N), C.byref(K),
+                               C.byref(ac), *[ptr(st[key]) for key in order]), "rf_load_all_data")
+    return S, int(pn.value), ac.value, n, k, st
+
+
+def save_lammps_data(path, task, st, with_energy=True):
+    """LAMMPS data text of SaveLammpsDATASimple (rf_save_lammps_data) from a state dict."""
+    N, K = int(task.N), int(task.K)
+    arr = [np.ascontiguousarray(st[k], np.float32) for k in ("R", "V", "W")]
+    check(lib.rf_save_lammps_data(os.fsencode(path), C.byref(task), N, K, *[ptr(x) for x in arr],
+                                  ptr(np.ascontiguousarray(st["IL"], ID_NP)),
+                                  ptr(np.ascontiguousarray(st["ILtype"], np.uint8)), 1 if with_energy else 0),
+          "rf_save_lammps_data")

@@ -132,3 +132,23 @@ def test_fracture_stops_on_device(cuda):
     assert res2.steps == s0
     assert res.broken_bonds > 0
     e.close()
+
+
+def test_checkpoint_file_resume_is_bitexact(cuda, tmp_path):
+    """rf_engine_checkpoint mid-run, rf_engine_restore in a fresh engine: the restored run
+    continues the uninterrupted one bit for bit; the file's payload is the reference's
+    SaveAllData layout, which rf_load_all_data reads back."""
+    t, R = rfdem.make_test(rfdem.RF_TEST_UNIAXIAL, 9.0, 14.0, seed=21)
+    a = rfdem.Engine(mc.clone(t), R)
+    a.step(260)
+    ref = a.export()
+    b = rfdem.Engine(mc.clone(t), R)
+    b.step(130)
+    path = tmp_path / "mid.ckpt"
+    b.checkpoint(str(path))
+    mid = b.export()
+    c = rfdem.Engine.restore(str(path))
+    assert_state_equal(c.export(), mid)
+    c.step(130)
+    assert_state_equal(c.export(), ref)
+    a.close(); b.close(); c.close()

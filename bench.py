@@ -434,6 +434,31 @@ def run_batch(rfdem, torch, seed, full=False):
                                                                      if steps_done[q] < 4 * BATCH_STEPS))}
 
 
+def run_fit_step(rfdem):
+    """One step of the material fitter at the reference's specimen sizes (cylinder D 12.5 x
+    H 25 mm, disc D 25 x 10 mm, p_r 0.5 mm): its 12 simulations to fracture, all engines
+    launched before any is waited on vs one after the other; wall time of each (engine
+    creation included) and the simulations' particle-steps."""
+    from rfdem import fit
+    S = fit.Specimens()
+    out = {}
+    for mode, conc in (("concurrent", True), ("sequential", False)):
+        T = fit.FitTask(2)
+        T.calculate_start_parameters()
+        t0 = time.perf_counter()
+        steps = fit.evaluate(T, S, concurrent=conc)
+        out[mode + "_s"] = time.perf_counter() - t0
+        out["runs"] = len(steps)
+        out["steps_per_run"] = sorted(steps.values())
+        out["results_" + mode] = T.RFunction.tolist()
+    out["speedup_concurrent"] = out["sequential_s"] / out["concurrent_s"]
+    out["same_results"] = out["results_concurrent"] == out["results_sequential"]
+    del out["results_sequential"]
+    out["workload"] = ("one conjugate-gradient step of the reference's material fitter: 6 parameter sets x "
+                       "(uniaxial + Brazilian) to fracture, reference model")
+    return out
+
+
 def run_engine(args):
     import torch
     rank, ws, dist = dist_init()
@@ -525,6 +550,10 @@ def run_engine(args):
     if rank == 0 and ws == 1 and not args.no_batch:
         batch = run_batch(rfdem, torch, 0xB2000000 + 4000, full=args.batch_full)
 
+    fitstep = None
+    if rank == 0 and ws == 1 and args.fit:
+        fitstep = run_fit_step(rfdem)
+
     fire = None
     if rank == 0 and ws == 1 and not args.no_fire:
         fire = run_fire(rfdem, torch, t, R, rad, x, 0xB2000000 + 3000)
@@ -556,6 +585,7 @@ def run_engine(args):
            "clocks": r["clocks"],
            "fire": fire,
            "batch": batch,
+           "fit": fitstep,
            "reference_model": refmodel}
     print(json.dumps(out))
     if dist is not None:
@@ -603,6 +633,7 @@ def main():
     ap.add_argument("--list-gap", type=float, default=None,
                     help="list gap / 0.25 mm: pairs listed within min(a_farcut, r_i + r_j + gap) "
                          "(default 0.25; 0 is the reference's uniform cutoff a_farcut)")
+    ap.add_argument("--fit", action="store_true", help="time one material-fitter step (12 runs to fracture)")
     ap.add_argument("--batch-full", action="store_true",
                     help="run the 64-disc batch to every specimen's post-peak drop instead of the timed window")
     args = ap.parse_args()

@@ -11,7 +11,8 @@ Build recipe for the checkers:
   (md_calculateforcesbpm_cpu.cpp) plus ``oracle/ref/ref_cpu_harness.cpp``.
 * ``oracle/_ref/libmdref_io.so`` -- the reference's own state writers
   (md_savelammpsdata.cpp, md_savealldata.cpp, the latter with ``-include cstring``,
-  which its source needs on Linux) plus ``oracle/ref/ref_io_harness.cpp``.
+  which its source needs on Linux) plus ``oracle/ref/ref_io_harness.cpp``, and its
+  conjugate-gradient parameter update (mp_task.h) behind ``oracle/ref/ref_fit_harness.cpp``.
 
 The ``_ref`` builds read the reference sources where they lie (``--ref`` or
 ``$RF_REFERENCE_DIR``, default ``/root/reference``) and are skipped when that tree
@@ -105,10 +106,11 @@ def build_ref(ref_dir=None, force=False, gpu=True, cpu=True):
         outs["cpu"] = out
         out = os.path.join(REF_OUT, "libmdref_io.so")
         srcs = [os.path.join(ref_dir, s) for s in REF_IO_SOURCES]
-        harness = os.path.join(HERE, "ref", "ref_io_harness.cpp")
-        if force or not _newer(out, srcs + [harness, __file__]):
+        harness = [os.path.join(HERE, "ref", "ref_io_harness.cpp"), os.path.join(HERE, "ref", "ref_fit_harness.cpp")]
+        deps = srcs + harness + [os.path.join(ref_dir, "mp_task.h"), __file__]
+        if force or not _newer(out, deps):
             _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-include", "cstring", "-I" + CUDA_INC] + inc +
-                 forced + ["-o", out] + srcs + [harness, "-L/usr/local/cuda/lib64", "-lcudart"])
+                 forced + ["-o", out] + srcs + harness + ["-L/usr/local/cuda/lib64", "-lcudart"])
         outs["io"] = out
     return outs
 

@@ -375,7 +375,7 @@ def run_batch_to_failure(rfdem, torch, tasks, params, Rs, rads, counts, t_pack, 
 
 
 def run_batch(rfdem, torch, seed, full=False):
-    """configs[2]-style batch: BATCH_SPECIMENS Brazilian discs (thickness = D/2) with
+    """The batched-disc workload: BATCH_SPECIMENS Brazilian discs (thickness = D/2) with
     particle counts log-uniform in [5k, 80k], radii U[0.8, 1.2] x 0.25 mm, Weibull
     modulus U[3, 10] per specimen (own seed each), platens at 0.05 m/s, dt 1e-8 s; all
     advanced by one step kernel per step (rf_engine_create_batch) vs the same specimens

@@ -92,3 +92,24 @@ def test_all_data_matches_reference_and_reads_back(tmp_path):
         assert (S2.R0, S2.H0, S2.Vgenmax) == (t.S.R0, t.S.H0, t.S.Vgenmax)
         P3 = full["R"].reshape(3, N)
         assert S2.A_real.x == float(P3[0].min()) and S2.B_real.z == float(P3[2].max())
+
+
+def test_state_file_error_paths(tmp_path):
+    """Bad id widths, truncated dumps and files that are not checkpoints are refused with
+    an error status (no GPU involved: restore reads and checks the header first)."""
+    t, N, K, st = _state()
+    with pytest.raises(rfdem.RFError):
+        rfdem.save_all_data(str(tmp_path / "x.dat"), t.S, st, N, K, t.acut, id_bytes=5)
+    good = tmp_path / "good.dat"
+    rfdem.save_all_data(str(good), t.S, st, N, K, t.acut, id_bytes=4)
+    data = good.read_bytes()
+    cut = tmp_path / "cut.dat"
+    cut.write_bytes(data[: len(data) // 2])
+    with pytest.raises(rfdem.RFError):
+        rfdem.load_all_data(str(cut), id_bytes=4)
+    with pytest.raises(rfdem.RFError):
+        rfdem.load_all_data(str(good), id_bytes=8)             # wrong width: counts do not match
+    with pytest.raises(rfdem.RFError):
+        rfdem.Engine.restore(str(good))                        # a dump, not a checkpoint
+    with pytest.raises(rfdem.RFError):
+        rfdem.Engine.restore(str(tmp_path / "missing.ckpt"))

@@ -64,6 +64,7 @@ def _declare(L):
         "rfo_qs_ext_d": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
         "rfo_warm_probe_ext_d": (None, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, u64, P]),
         "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
+        "rfo_run_ext_pos_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P, i32]),
         "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
     }
     for n, (r, a) in proto.items():
@@ -110,8 +111,9 @@ def run_d(task, R0, max_steps):
     return int(steps), R, curve[:3 * min(ns.value, cap)].reshape(-1, 3), ty, status.value
 
 
-def run_ext(task, x, R0, radius, max_steps, fp64=False):
-    """Extended model run (float forces as the engine computes them, or the FP64 oracle).
+def run_ext(task, x, R0, radius, max_steps, fp64=False, positions="f64"):
+    """Extended model run (float forces as the engine computes them, or the FP64 oracle;
+    positions "hilo" / "f32": float forces with positions kept as hi/lo float pairs / floats).
     Returns dict(steps, R (double planar, after the pending delete pass), V, IL, ILtype,
     curve, status, broken)."""
     L = load()
@@ -124,9 +126,12 @@ def run_ext(task, x, R0, radius, max_steps, fp64=False):
     cap = max(int(max_steps), 1) + 1
     curve = np.zeros(3 * cap, np.float64)
     ns, status, broken = C.c_uint64(0), C.c_int(0), C.c_uint64(0)
-    fn = L.rfo_run_ext_d if fp64 else L.rfo_run_ext_f
-    steps = fn(C.byref(task), C.byref(x), p(R), p(rad), max_steps, p(V), p(IL), p(ty), p(curve), cap, C.byref(ns),
-               C.byref(status), C.byref(broken))
+    args = [C.byref(task), C.byref(x), p(R), p(rad), max_steps, p(V), p(IL), p(ty), p(curve), cap, C.byref(ns),
+            C.byref(status), C.byref(broken)]
+    if positions != "f64" and not fp64:
+        steps = L.rfo_run_ext_pos_f(*args, {"hilo": 1, "f32": 2}[positions])
+    else:
+        steps = (L.rfo_run_ext_d if fp64 else L.rfo_run_ext_f)(*args)
     return dict(steps=int(steps), R=R, V=V, IL=IL, ILtype=ty, curve=curve[:3 * min(ns.value, cap)].reshape(-1, 3),
                 status=status.value, broken=int(broken.value))
 

@@ -865,8 +865,30 @@ static inline double pair_uniform(uint64_t seed, uint64_t a, uint64_t b, uint32_
     return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
 }
 
+// Positions kept as hi/lo pairs of floats (x = hi + lo, |lo| at most half an ulp of hi)
+// instead of doubles: a double is rounded to the nearest such pair, and an increment is
+// added with float operations only (Knuth's two-sum of hi and the increment, the error
+// folded into lo, Dekker's fast two-sum to renormalise). Every pair is a double exactly.
+static inline double hilo_round(double x) {
+    const float h = (float)x;
+    const float l = (float)(x - (double)h);
+    return (double)h + (double)l;
+}
+static inline double hilo_add(double x, float d) {
+    const float h = (float)x;
+    const float l = (float)(x - (double)h);
+    const float s = h + d;
+    const float bb = s - h;
+    const float e = (h - (s - bb)) + (d - bb);
+    const float t = l + e;
+    const float hi = s + t;
+    const float lo = t - (hi - s);
+    return (double)hi + (double)lo;
+}
+
 template <class TF>
 struct RunExt {
+    int pos_mode = 0;           // positions as doubles (0), hi/lo float pairs (1, see hilo_add) or floats (2)
     rf_task* t;
     ExtPar x;
     uint64_t N, K, CN;
@@ -905,6 +927,10 @@ struct RunExt {
     void init(const double* R0, const double* r0) {
         N = t->N; K = t->K; CN = t->C.N;
         R.assign(R0, R0 + 3 * N); rad.assign(r0, r0 + N); Rf.assign(3 * N, 0.f);
+        if (pos_mode == 1)
+            for (double& v : R) v = hilo_round(v);
+        if (pos_mode == 2)
+            for (double& v : R) v = (double)(float)v;
         V.assign(3 * N, 0); W.assign(3 * N, 0);
         IL.assign(N * K, EMPTY); type.assign(N * K, 0); L0.assign(N * K, 1.0); sig.assign(N * K, 0.0);
         tau.assign(N * K, 0.0);
@@ -1294,7 +1320,15 @@ struct RunExt {
             const TF mi = cmass * ri * ri * ri;
             const TF dtm = dt / mi, dtI = dt / ((TF)0.4f * mi * ri * ri);
             Vx += Fx * dtm; Vy += Fy * dtm; Vz += Fz * dtm;
-            Rx += (double)(Vx * dt); Ry += (double)(Vy * dt); Rz += (double)(Vz * dt);
+            if (pos_mode == 1) {
+                Rx = hilo_add(Rx, (float)(Vx * dt)); Ry = hilo_add(Ry, (float)(Vy * dt));
+                Rz = hilo_add(Rz, (float)(Vz * dt));
+            } else if (pos_mode == 2) {
+                Rx = (double)((float)Rx + (float)(Vx * dt)); Ry = (double)((float)Ry + (float)(Vy * dt));
+                Rz = (double)((float)Rz + (float)(Vz * dt));
+            } else {
+                Rx += (double)(Vx * dt); Ry += (double)(Vy * dt); Rz += (double)(Vz * dt);
+            }
             W[i] += Mn[i].x * dtI; W[i + N] += Mn[i].y * dtI; W[i + 2 * N] += Mn[i].z * dtI;
             const double dx = Rx - S.center.x, dy = Ry - S.center.y, dz = Rz - S.center.z;
             if ((dx - S.spacesized2.x > 0) || (dx + S.spacesized2.x < 0) || (dy - S.spacesized2.y > 0) ||
@@ -1439,8 +1473,9 @@ struct RunExt {
 template <class TF>
 static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const double* rad, uint64_t max_steps,
                         TF* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,
-                        uint64_t* nsaved, int* status, uint64_t* broken) {
+                        uint64_t* nsaved, int* status, uint64_t* broken, int pos_mode = 0) {
     RunExt<TF> r;
+    r.pos_mode = pos_mode;
     r.t = t;
     r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
                  xp->post_peak_drop, xp->list_gap};
@@ -1554,6 +1589,14 @@ uint64_t rfo_run_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const d
                        uint64_t* nsaved, int* status, uint64_t* broken) {
     return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
                                broken);
+}
+// Float forces with positions as hi/lo float pairs (pos_mode 1) or as floats (2): the
+// precision comparison.
+uint64_t rfo_run_ext_pos_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,
+                           float* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,
+                           uint64_t* nsaved, int* status, uint64_t* broken, int pos_mode) {
+    return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
+                               broken, pos_mode);
 }
 uint64_t rfo_run_ext_d(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,
                        double* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,

@@ -142,3 +142,24 @@ def test_list_gap_rows_hold_exactly_the_pairs_within_their_cutoff(gap):
     b = oracle.run_ext(mc.clone(t), x, R, rad, steps, fp64=True)
     assert a["status"] == 0 and b["status"] == 0
     assert np.max(np.abs(a["R"] - b["R"])) < 1e-6 * float(np.max(R) - np.min(R))
+
+
+def test_position_precision_fp64_vs_hilo_vs_fp32():
+    """Float forces with positions as FP64, as hi/lo float pairs, or as plain floats,
+    each against the FP64 oracle: FP64 and hi/lo positions both track it to the float
+    forces' own error, while float positions lose the small increments (the platen
+    stress then drifts by tens of percent)."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
+    steps = 1000
+    g = oracle.run_ext(mc.clone(t), x, R, rad, steps, fp64=True)
+    err, stress = {}, {}
+    for mode in ("f64", "hilo", "f32"):
+        f = oracle.run_ext(mc.clone(t), x, R, rad, steps, positions=mode)
+        assert f["steps"] == steps and f["status"] == 0
+        err[mode] = float(np.max(np.abs(f["R"] - g["R"])))
+        stress[mode] = abs(f["curve"][-1, 1] / g["curve"][-1, 1] - 1.0)
+    ext = float(np.max(R) - np.min(R))
+    assert err["f64"] < 1e-8 * ext and err["hilo"] < 1e-8 * ext
+    assert stress["f64"] < 1e-5 and stress["hilo"] < 1e-5
+    assert err["f32"] > 1e4 * max(err["f64"], err["hilo"])
+    assert stress["f32"] > 0.05

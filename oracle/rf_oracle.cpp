@@ -865,6 +865,10 @@ static inline double pair_uniform(uint64_t seed, uint64_t a, uint64_t b, uint32_
     return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
 }
 
+// Bond state inside a quasi-static increment: integrated iteration by iteration (0) or
+// carried from the increment's start state to the current configuration (1, bond_total).
+static int g_qs_total = 1;
+
 // Positions kept as hi/lo pairs of floats (x = hi + lo, |lo| at most half an ulp of hi)
 // instead of doubles: a double is rounded to the nearest such pair, and an increment is
 // added with float operations only (Knuth's two-sum of hi and the increment, the error
@@ -898,6 +902,10 @@ struct RunExt {
     std::vector<id_t> IL, CI, CIs, pnC;
     std::vector<uint8_t> type;
     std::vector<V3<TF>> Rij, Oijt, Mijn, Mijt;
+    // bond state at the start of a quasi-static increment; during the increment's FIRE
+    // iterations (qs_total) a bond's state is computed from it and the motion since then
+    std::vector<V3<TF>> Rij0, Oijt0, Mijn0, Mijt0;
+    bool qs_total = false;
     double sz0, aa_farcut, aacut, a_farcut;
     int status;
     uint64_t steps, broken;
@@ -1135,6 +1143,92 @@ struct RunExt {
         return false;
     }
 
+    // One bond slot inside a quasi-static increment: the state is the increment's start
+    // state carried to the current configuration in one step -- start normal Rij0 to the
+    // current normal n, the particles' rotations ti, tj and displacements ui, uj since the
+    // increment began -- with bond()'s formulas, so it depends on where the particles are,
+    // not on the path the relaxation took to get there.
+    bool bond_total(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& ui, const V3<TF>& uj, const V3<TF>& ti,
+                    const V3<TF>& tj, TF br, V3<TF>& fs, V3<TF>& ms, double& fnsum, double* kt, double* kr) {
+        const TF PI = pi_t<TF>();
+        const TF rijm = (TF)rlen;
+        const TF inv_rm = rcp(rijm);
+        const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
+        const TF stretch = (TF)(rlen - L0[k]);
+        const TF A = br * br * PI;
+        const TF J = PI * br * br * br * br;
+        if (kt) {
+            *kt += (double)((kn + ks) * A);
+            *kr += (double)((TF)0.25f * kn * J + (TF)0.5f * ks * J + (TF)0.25f * ks * A * rijm * rijm);
+        }
+        TF cef = kn * stretch;
+        TF Sc = cef;
+        cef *= A;
+        fnsum += std::fabs((double)cef);
+        fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
+        const V3<TF>& R0 = Rij0[k];
+        const TF tx = R0.y * nz - R0.z * ny, ty = R0.z * nx - R0.x * nz, tz = R0.x * ny - R0.y * nx;
+        const TF wsx = tj.x + ti.x, wsy = tj.y + ti.y, wsz = tj.z + ti.z;
+        const TF cphi = (wsx * nx + wsy * ny + wsz * nz) * (TF)0.5f;
+        const TF phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
+        Rij[k] = {nx, ny, nz};
+        const TF M1x = (TF)1.0f + tz * phz + ty * phy, M1y = phz - tz - ty * phx, M1z = -phy - tz * phx + ty;
+        const TF M2x = tz - phz - tx * phy, M2y = tz * phz + (TF)1.0f + tx * phx, M2z = -tz * phy + phx - tx;
+        const TF M3x = -ty - tx * phz + phy, M3y = -ty * phz + tx - phx, M3z = ty * phy + tx * phx + (TF)1.0f;
+        const TF dwx = tj.x - ti.x, dwy = tj.y - ti.y, dwz = tj.z - ti.z;
+        {
+            TF c1 = nx * dwx + ny * dwy + nz * dwz;
+            c1 *= (TF)0.5f * ks;
+            const V3<TF> o = Mijn0[k];
+            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
+            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
+            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
+            Mijn[k] = {mx, my, mz};
+            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+        }
+        {
+            const TF c1 = nx * dwx + ny * dwy + nz * dwz;
+            const TF c2 = (TF)0.25f * kn;
+            const V3<TF> o = Mijt0[k];
+            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
+            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
+            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
+            Mijt[k] = {mx, my, mz};
+            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+        }
+        TF Mc;
+        {
+            const TF hx = (TF)0.5f * wsx, hy = (TF)0.5f * wsy, hz = (TF)0.5f * wsz;
+            const TF vx = uj.x - ui.x - hy * r.z + hz * r.y;
+            const TF vy = uj.y - ui.y - hz * r.x + hx * r.z;
+            const TF vz = uj.z - ui.z - hx * r.y + hy * r.x;
+            TF c = nx * vx + ny * vy + nz * vz;
+            const V3<TF> o = Oijt0[k];
+            const TF ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c);
+            const TF oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (vy - ny * c);
+            const TF oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (vz - nz * c);
+            c = ks;
+            Mc = c;
+            c *= A;
+            fs.x += ox * c; fs.y += oy * c; fs.z += oz * c;
+            Oijt[k] = {ox, oy, oz};
+            ms.x += (TF)0.5f * (r.y * oz - r.z * oy) * c;
+            ms.y += (TF)0.5f * (r.z * ox - r.x * oz) * c;
+            ms.z += (TF)0.5f * (r.x * oy - r.y * ox) * c;
+        }
+        const V3<TF>& O = Oijt[k];
+        const V3<TF>& Mt = Mijt[k];
+        const V3<TF>& Mn = Mijn[k];
+        Mc *= norm3(O.x, O.y, O.z);
+        Sc += norm3(Mt.x, Mt.y, Mt.z) * (TF)4.0f * br;
+        Mc += norm3(Mn.x, Mn.y, Mn.z) * (TF)2.0f * br;
+        if ((Sc > (TF)sig[k]) || (Mc > (TF)tau[k])) {
+            Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
+            return true;
+        }
+        return false;
+    }
+
     // One overlapping pair (engine contact_pair_ext).
     void contact(uint64_t k, const V3<TF>& r, TF rijm, TF delta, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
                  const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms, double& fnsum,
@@ -1219,7 +1313,17 @@ struct RunExt {
                 const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
                 const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
                 const TF br = lambda * std::min(ri, (TF)rad[j]);
-                if (bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb, fnsum, kt, kr)) { type[k] = 0; ++broken; }
+                bool broke;
+                if (qs_total) {
+                    const V3<TF> ui = {(TF)(R[i] - X0[i]), (TF)(R[i + N] - X0[i + N]), (TF)(R[i + 2 * N] - X0[i + 2 * N])};
+                    const V3<TF> uj = {(TF)(R[j] - X0[j]), (TF)(R[j + N] - X0[j + N]), (TF)(R[j + 2 * N] - X0[j + 2 * N])};
+                    const V3<TF> ti = {(TF)ROT[3 * i], (TF)ROT[3 * i + 1], (TF)ROT[3 * i + 2]};
+                    const V3<TF> tj = {(TF)ROT[3 * j], (TF)ROT[3 * j + 1], (TF)ROT[3 * j + 2]};
+                    broke = bond_total(k, r, std::sqrt(d2), ui, uj, ti, tj, br, fsb, msb, fnsum, kt, kr);
+                } else {
+                    broke = bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb, fnsum, kt, kr);
+                }
+                if (broke) { type[k] = 0; ++broken; }
                 npair += 1;
             }
             for (uint64_t q = 0; q < K; ++q) {                   // _21 order: type-0 slots by slot
@@ -1352,12 +1456,14 @@ struct RunExt {
     // platen clamp at rest, FIRE decision on FP64 sums, mixing and semi-implicit Euler].
     // trace (may be null) receives the residual of every iteration.
     std::vector<double> X0, ROT;      // start positions and accumulated rotation of the last increment
+    std::vector<V3<TF>> Flast, Mlast; // net forces and moments of the last increment's last pass
 
     uint64_t fire_increment(const rf_relax_params& p, int* converged, double* residual, double* trace,
                             uint64_t trace_cap, const double* warm = nullptr) {
         rf_compression& Kc = t->Compress;
         X0 = R;
         ROT.assign(3 * N, 0.0);
+        Rij0 = Rij; Oijt0 = Oijt; Mijn0 = Mijn; Mijt0 = Mijt;
         const int ax = t->kind == RF_TEST_BRAZIL ? 1 : 2;
         const double delta = p.strain_inc * Kc.Size0;
         double* sz = ax == 1 ? &Kc.size_d.y : &Kc.size_d.z;
@@ -1393,6 +1499,7 @@ struct RunExt {
         }
         const TF dt_keep = dt, pA_keep = p_A, mur_keep = mur;
         p_A = 0; mur = 0;
+        qs_total = g_qs_total;
         double fdt = p.dt0, alpha = p.alpha0, cv = 1, cf = 0, cm = 0;
         uint64_t npos = 0, it = 0;
         bool uphill = false;
@@ -1466,6 +1573,8 @@ struct RunExt {
             }
         }
         dt = dt_keep; p_A = pA_keep; mur = mur_keep;
+        qs_total = false;
+        Flast = Fn; Mlast = Mn;
         return it;
     }
 };
@@ -1590,6 +1699,7 @@ uint64_t rfo_run_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const d
     return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
                                broken);
 }
+void rfo_set_qs_total(int on) { rfo::g_qs_total = on; }
 // Float forces with positions as hi/lo float pairs (pos_mode 1) or as floats (2): the
 // precision comparison.
 uint64_t rfo_run_ext_pos_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,

@@ -63,28 +63,44 @@ def test_ext_directed_bonds_pair_up():
     assert pairs and all((j, i) in pairs for (i, j) in pairs)
 
 
-def test_exact_warm_start_is_path_dependent():
+def _qs_total(on):
+    L = oracle.load()
+    L.rfo_set_qs_total.argtypes = [C.c_int]
+    L.rfo_set_qs_total(on)
+
+
+def test_exact_warm_start_lands_on_the_relaxed_state():
     """Warm-starting a FIRE increment with its own relaxed answer (displacements and
-    rotations over dt0) does not start at equilibrium: the bond shear forces and moments
-    are integrated along the motion, and one large jump integrates a different path than
-    the relaxation did. The residual after the first pass sits far above the tolerance,
-    the bond state differs from the relaxed one by a small relative amount, and the warm
-    run still converges to the same platen stress in a fraction of the iterations."""
+    rotations). Inside an increment the bond state is computed from the increment's start
+    state and the motion since then (the engine's FIRE mode), so the jump lands on the
+    relaxed state: the first pass's residual is within a few times the tolerance and the
+    warm run converges in a small fraction of the iterations, to the same stress. With
+    the state integrated iteration by iteration instead (the explicit steps' rule) the
+    shear forces and moments depend on the relaxation's path: the jump starts far above
+    the tolerance and saves far less."""
     t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
     p = rfdem.RelaxParams()
     rfdem.lib.rf_relax_default_params(C.byref(p), C.byref(t))
     p.max_iter, p.strain_inc = 40000, 1e-4
-    one = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 1)
+    try:
+        out = {}
+        for total in (1, 0):
+            _qs_total(total)
+            one = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 1)
+            full = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000)
+            out[total] = (one, full)
+    finally:
+        _qs_total(1)
+    one, full = out[1]
     assert one["res_plain"] <= p.tol
-    assert one["res_warm"] > 10 * p.tol
-    assert one["dRij"] < 1e-9 * float(np.max(R) - np.min(R))        # positions land on the relaxed ones
-    assert 0 < one["dMijt"] < 1e-3 * one["maxMijt"]
-    assert 0 < one["dMijn"] < 1e-3 * one["maxMijn"]
-    full = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000)
+    assert one["res_warm"] < 20 * p.tol
     assert full["stress_plain"] > 1e-5                              # the platen carries load
-    assert full["conv_warm"] == 1 and full["res_warm"] <= p.tol
-    assert full["it_warm"] * 2 < full["it_plain"]
-    assert abs(full["stress_warm"] - full["stress_plain"]) <= 1e-4 * abs(full["stress_plain"])
+    assert full["conv_warm"] == 1 and full["it_warm"] * 10 < full["it_plain"]
+    assert abs(full["stress_warm"] - full["stress_plain"]) <= 1e-5 * abs(full["stress_plain"])
+    one0, full0 = out[0]
+    assert one0["res_warm"] > 50 * one["res_warm"]
+    assert 0 < one0["dMijt"] < 1e-3 * one0["maxMijt"]
+    assert full0["conv_warm"] == 1 and full0["it_warm"] > 3 * full["it_warm"]
 
 
 def test_post_peak_drop_stop_rule():

@@ -906,6 +906,10 @@ struct RunExt {
     // iterations (qs_total) a bond's state is computed from it and the motion since then
     std::vector<V3<TF>> Rij0, Oijt0, Mijn0, Mijt0;
     bool qs_total = false;
+    // inside a quasi-static increment's FIRE iterations a particle held by a platen does
+    // not slide along it either (the platens hold what they touch; this removes the
+    // specimen's rigid tilting and sliding, which would leave FIRE without a minimum)
+    bool in_fire = false;
     double sz0, aa_farcut, aacut, a_farcut;
     int status;
     uint64_t steps, broken;
@@ -1374,7 +1378,10 @@ struct RunExt {
                             Fz -= (TF)0.45f * fy * Vz * iv;
                         }
                     }
-                    if (Ry + off - Top > -1e-9) { Ry = Top - off; Vy = vt; Fy = 0; }
+                    if (Ry + off - Top > -1e-9) {
+                        Ry = Top - off; Vy = vt; Fy = 0;
+                        if (in_fire) { Fx = 0; Fz = 0; Vx = 0; Vz = 0; }
+                    }
                 }
                 if (Ry - off - BottomR < 1e-9) {
                     const TF fy = Fy;
@@ -1387,7 +1394,10 @@ struct RunExt {
                             Fz += (TF)0.45f * fy * Vz * iv;
                         }
                     }
-                    if (Ry - off - Bottom < 1e-9) { Ry = Bottom + off; Vy = 0; Fy = 0; }
+                    if (Ry - off - Bottom < 1e-9) {
+                        Ry = Bottom + off; Vy = 0; Fy = 0;
+                        if (in_fire) { Fx = 0; Fz = 0; Vx = 0; Vz = 0; }
+                    }
                 }
             }
         } else {
@@ -1395,11 +1405,17 @@ struct RunExt {
             if (rx * rx + ry * ry < (TF)RR && Rz < Zcut) {
                 if (Rz + off - TopR > -1e-9) {
                     if (Fz > 0) sft += (double)Fz;
-                    if (Rz + off - Top > -1e-9) { Rz = Top - off; Vz = vt; Fz = 0; }
+                    if (Rz + off - Top > -1e-9) {
+                        Rz = Top - off; Vz = vt; Fz = 0;
+                        if (in_fire) { Fx = 0; Fy = 0; Vx = 0; Vy = 0; }
+                    }
                 }
                 if (Rz - off - BottomR < 1e-9) {
                     if (Fz < 0) sfb += (double)Fz;
-                    if (Rz - off - Bottom < 1e-9) { Rz = Bottom + off; Vz = 0; Fz = 0; }
+                    if (Rz - off - Bottom < 1e-9) {
+                        Rz = Bottom + off; Vz = 0; Fz = 0;
+                        if (in_fire) { Fx = 0; Fy = 0; Vx = 0; Vy = 0; }
+                    }
                 }
             }
         }
@@ -1500,6 +1516,7 @@ struct RunExt {
         const TF dt_keep = dt, pA_keep = p_A, mur_keep = mur;
         p_A = 0; mur = 0;
         qs_total = g_qs_total;
+        in_fire = true;
         double fdt = p.dt0, alpha = p.alpha0, cv = 1, cf = 0, cm = 0;
         uint64_t npos = 0, it = 0;
         bool uphill = false;
@@ -1574,6 +1591,7 @@ struct RunExt {
         }
         dt = dt_keep; p_A = pA_keep; mur = mur_keep;
         qs_total = false;
+        in_fire = false;
         Flast = Fn; Mlast = Mn;
         return it;
     }

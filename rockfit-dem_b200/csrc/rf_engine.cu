@@ -824,27 +824,35 @@ __global__ void k_delete_pending_ext(Dev d, Consts c) {
 // centre plus (radius - p_r) towards the top platen and minus it towards the bottom
 // one, so a polydisperse specimen meets a flat platen with every particle that
 // touches it; for radius p_r this is the reference's centre rule.
-__device__ __forceinline__ void uniaxial_particle_ext(double& Rx, double& Ry, double& Rz, float& Vz, float& Fz,
-                                                      const rf_float3 c, float RR, double Zt, double Zb, double Ztr,
-                                                      double Zbr, float vt, double Zcut, double off, double& sfb,
-                                                      double& sft) {
+// hold: inside a quasi-static increment's FIRE iterations a particle held by a platen
+// does not slide along it either (removes the specimen's rigid tilting and sliding).
+__device__ __forceinline__ void uniaxial_particle_ext(double& Rx, double& Ry, double& Rz, float& Vx, float& Vy,
+                                                      float& Vz, float& Fx, float& Fy, float& Fz, const rf_float3 c,
+                                                      float RR, double Zt, double Zb, double Ztr, double Zbr, float vt,
+                                                      double Zcut, double off, double& sfb, double& sft, bool hold) {
     const float rx = (float)(Rx - c.x), ry = (float)(Ry - c.y);
     const double rz = Rz;
     if (rx * rx + ry * ry < RR && rz < Zcut) {
         if (rz + off - Ztr > -1e-9) {
             if (Fz > 0) sft += (double)Fz;
-            if (rz + off - Zt > -1e-9) { Rz = Zt - off; Vz = vt; Fz = 0.f; }
+            if (rz + off - Zt > -1e-9) {
+                Rz = Zt - off; Vz = vt; Fz = 0.f;
+                if (hold) { Fx = 0.f; Fy = 0.f; Vx = 0.f; Vy = 0.f; }
+            }
         }
         if (rz - off - Zbr < 1e-9) {
             if (Fz < 0) sfb += (double)Fz;
-            if (rz - off - Zb < 1e-9) { Rz = Zb + off; Vz = 0.f; Fz = 0.f; }
+            if (rz - off - Zb < 1e-9) {
+                Rz = Zb + off; Vz = 0.f; Fz = 0.f;
+                if (hold) { Fx = 0.f; Fy = 0.f; Vx = 0.f; Vy = 0.f; }
+            }
         }
     }
 }
 __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, double& Rz, float& Vx, float& Vy,
                                                     float& Vz, float& Fx, float& Fy, float& Fz, const rf_float3 c,
                                                     float RR, double Yt, double Yb, double Ytr, double Ybr, float vt,
-                                                    double Zcut, double off, double& sfb, double& sft) {
+                                                    double Zcut, double off, double& sfb, double& sft, bool hold) {
     const float rx = (float)(Rx - c.x), rz = (float)(Rz - c.z);
     const double ry = Ry;
     if (rx * rx + rz * rz < RR && (double)rz < Zcut) {
@@ -859,7 +867,10 @@ __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, doub
                     Fz -= 0.45f * fy * Vz * iv;
                 }
             }
-            if (ry + off - Yt > -1e-9) { Ry = Yt - off; Vy = vt; Fy = 0.f; }
+            if (ry + off - Yt > -1e-9) {
+                Ry = Yt - off; Vy = vt; Fy = 0.f;
+                if (hold) { Fx = 0.f; Fz = 0.f; Vx = 0.f; Vz = 0.f; }
+            }
         }
         if (ry - off - Ybr < 1e-9) {
             const float fy = Fy;
@@ -872,7 +883,10 @@ __device__ __forceinline__ void brazil_particle_ext(double& Rx, double& Ry, doub
                     Fz += 0.45f * fy * Vz * iv;
                 }
             }
-            if (ry - off - Yb < 1e-9) { Ry = Yb + off; Vy = 0.f; Fy = 0.f; }
+            if (ry - off - Yb < 1e-9) {
+                Ry = Yb + off; Vy = 0.f; Fy = 0.f;
+                if (hold) { Fx = 0.f; Fz = 0.f; Vx = 0.f; Vz = 0.f; }
+            }
         }
     }
 }
@@ -1221,10 +1235,10 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         float Vx = vi.x, Vy = vi.y, Vz = vi.z;
         if (KIND == RF_TEST_BRAZIL)
             brazil_particle_ext(Rx, Ry, Rz, Vx, Vy, Vz, Fx, Fy, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt,
-                                (double)G.zcut, xi.w - c.p_r_d, sfb, sft);
+                                (double)G.zcut, xi.w - c.p_r_d, sfb, sft, MODE == 1);
         else
-            uniaxial_particle_ext(Rx, Ry, Rz, Vz, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt, (double)G.zcut,
-                                  xi.w - c.p_r_d, sfb, sft);
+            uniaxial_particle_ext(Rx, Ry, Rz, Vx, Vy, Vz, Fx, Fy, Fz, cc, RR, Top, Bottom, TopR, BottomR, vt,
+                                  (double)G.zcut, xi.w - c.p_r_d, sfb, sft, MODE == 1);
         if (MODE == 1) {
             // FIRE: keep the clamped state for the update kernel; reduce the FIRE sums
             d.posd[nxt][i] = make_double4(Rx, Ry, Rz, xi.w);
@@ -1502,10 +1516,10 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int 
         double sb = 0.0, st = 0.0;
         if (KIND == RF_TEST_BRAZIL)
             brazil_particle_ext(x.x, x.y, x.z, v0, v1, v2, f0, f1, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f,
-                                (double)c.zcut, x.w - c.p_r_d, sb, st);
+                                (double)c.zcut, x.w - c.p_r_d, sb, st, false);
         else
-            uniaxial_particle_ext(x.x, x.y, x.z, v2, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f, (double)c.zcut,
-                                  x.w - c.p_r_d, sb, st);
+            uniaxial_particle_ext(x.x, x.y, x.z, v0, v1, v2, f0, f1, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f,
+                                  (double)c.zcut, x.w - c.p_r_d, sb, st, false);
         d.posd[cur][i] = x;
         d.vel[cur][i] = make_float4(v0, v1, v2, 0.f);
         d.ang[cur][i] = w;

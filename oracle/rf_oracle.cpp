@@ -865,9 +865,10 @@ static inline double pair_uniform(uint64_t seed, uint64_t a, uint64_t b, uint32_
     return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
 }
 
-// Bond state inside a quasi-static increment: integrated iteration by iteration (0) or
-// carried from the increment's start state to the current configuration (1, bond_total).
-static int g_qs_total = 1;
+// Bond state inside a quasi-static increment: integrated iteration by iteration (0, the
+// engine's FIRE mode) or carried from the increment's start state to the current
+// configuration (1, bond_total: a study of a path-independent rule, not run by the engine).
+static int g_qs_total = 0;
 
 // Positions kept as hi/lo pairs of floats (x = hi + lo, |lo| at most half an ulp of hi)
 // instead of doubles: a double is rounded to the nearest such pair, and an increment is

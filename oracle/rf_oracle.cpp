@@ -865,10 +865,10 @@ static inline double pair_uniform(uint64_t seed, uint64_t a, uint64_t b, uint32_
     return ((double)(h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
 }
 
-// Bond state inside a quasi-static increment: integrated iteration by iteration (0, the
-// engine's FIRE mode) or carried from the increment's start state to the current
-// configuration (1, bond_total: a study of a path-independent rule, not run by the engine).
-static int g_qs_total = 0;
+// Bond state inside a quasi-static increment: carried from the increment's start state to
+// the current configuration (1, bond_total: the engine's FIRE mode) or integrated iteration
+// by iteration (0, the explicit steps' rule; kept for comparison).
+static int g_qs_total = 1;
 
 // Positions kept as hi/lo pairs of floats (x = hi + lo, |lo| at most half an ulp of hi)
 // instead of doubles: a double is rounded to the nearest such pair, and an increment is
@@ -1153,7 +1153,10 @@ struct RunExt {
     // current normal n, the particles' rotations ti, tj and displacements ui, uj since the
     // increment began -- with bond()'s formulas, so it depends on where the particles are,
     // not on the path the relaxation took to get there.
-    bool bond_total(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& ui, const V3<TF>& uj, const V3<TF>& ti,
+    // du: the pair's relative motion since the increment began less the mean rotation's
+    // part, (r - r0) - ((ti + tj) / 2) x r, formed in double by the caller (in float its
+    // terms cancel and the relaxation stalls on the rounding).
+    bool bond_total(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& du, const V3<TF>& ti,
                     const V3<TF>& tj, TF br, V3<TF>& fs, V3<TF>& ms, double& fnsum, double* kt, double* kr) {
         const TF PI = pi_t<TF>();
         const TF rijm = (TF)rlen;
@@ -1203,10 +1206,7 @@ struct RunExt {
         }
         TF Mc;
         {
-            const TF hx = (TF)0.5f * wsx, hy = (TF)0.5f * wsy, hz = (TF)0.5f * wsz;
-            const TF vx = uj.x - ui.x - hy * r.z + hz * r.y;
-            const TF vy = uj.y - ui.y - hz * r.x + hx * r.z;
-            const TF vz = uj.z - ui.z - hx * r.y + hy * r.x;
+            const TF vx = du.x, vy = du.y, vz = du.z;
             TF c = nx * vx + ny * vy + nz * vz;
             const V3<TF> o = Oijt0[k];
             const TF ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c);
@@ -1320,11 +1320,17 @@ struct RunExt {
                 const TF br = lambda * std::min(ri, (TF)rad[j]);
                 bool broke;
                 if (qs_total) {
-                    const V3<TF> ui = {(TF)(R[i] - X0[i]), (TF)(R[i + N] - X0[i + N]), (TF)(R[i + 2 * N] - X0[i + 2 * N])};
-                    const V3<TF> uj = {(TF)(R[j] - X0[j]), (TF)(R[j + N] - X0[j + N]), (TF)(R[j + 2 * N] - X0[j + 2 * N])};
+                    // the pair's relative displacement since the increment began, formed in
+                    // double as (r - r0) so that it keeps its own precision (a difference of
+                    // the two particles' float displacements loses it to their size)
                     const V3<TF> ti = {(TF)ROT[3 * i], (TF)ROT[3 * i + 1], (TF)ROT[3 * i + 2]};
                     const V3<TF> tj = {(TF)ROT[3 * j], (TF)ROT[3 * j + 1], (TF)ROT[3 * j + 2]};
-                    broke = bond_total(k, r, std::sqrt(d2), ui, uj, ti, tj, br, fsb, msb, fnsum, kt, kr);
+                    const double hx = 0.5 * (ROT[3 * i] + ROT[3 * j]), hy = 0.5 * (ROT[3 * i + 1] + ROT[3 * j + 1]),
+                                 hz = 0.5 * (ROT[3 * i + 2] + ROT[3 * j + 2]);
+                    const V3<TF> du = {(TF)(dx - (X0[j] - X0[i]) - (hy * dz - hz * dy)),
+                                       (TF)(dy - (X0[j + N] - X0[i + N]) - (hz * dx - hx * dz)),
+                                       (TF)(dz - (X0[j + 2 * N] - X0[i + 2 * N]) - (hx * dy - hy * dx))};
+                    broke = bond_total(k, r, std::sqrt(d2), du, ti, tj, br, fsb, msb, fnsum, kt, kr);
                 } else {
                     broke = bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb, fnsum, kt, kr);
                 }

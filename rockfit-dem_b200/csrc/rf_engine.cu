@@ -135,6 +135,7 @@ struct Dev {
     uint8_t* bk;        // [QB][N] slot of the record (0xFF: record retired)
     float* bil;         // [QB][N] 1/L0
     float4* bst;        // [3][QB][N] (Rij.xyz Oijt.x) (Oijt.yz Mijn.xy) (Mijn.z Mijt.xyz)
+    float4* bst0;       // bst at the start of the current quasi-static increment (FIRE mode)
     uint32_t* nbq;      // [N] records of the particle
     uint32_t* bmask;    // [N] records holding an intact bond
     // Verlet candidates
@@ -1084,12 +1085,16 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         const uint32_t wb = __reduce_or_sync(FULL, bmask);
         const uint32_t qend = 32u - __clz(wb);
         // every load of a record is issued before the partner's gathers and the far-link
-        // test, so a record waits for two dependent latencies (id -> partner state), not three
+        // test, so a record waits for two dependent latencies (id -> partner state), not three.
+        // FIRE mode reads the records' increment-start state and the motion since then.
+        const float4* src = MODE == 1 ? d.bst0 : d.bst;
+        double4 xi0 = xi, ri0 = make_double4(0, 0, 0, 0);
+        if (MODE == 1 && valid) { xi0 = d.x0[i]; ri0 = d.rot[i]; }
         for (uint32_t q = 0; q < qend; ++q) {
             if (!((bmask >> q) & 1u)) continue;
             const size_t s = (size_t)q * N + i;
             const uint32_t j = __ldg(&d.bj[s]);
-            const float4 s0 = d.bst[s], s1 = d.bst[s + QN], s2 = d.bst[s + 2 * QN];
+            const float4 s0 = src[s], s1 = src[s + QN], s2 = src[s + 2 * QN];
             const float2 str = __ldg(&d.bstr[s]);
             const double L0 = __ldg(&d.bL0[s]);
             const double4 xj = ldg_d4(&P[j]);
@@ -1106,8 +1111,20 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
             f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
             f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
-            const bool broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(vj), wi, f4to3(wj), rij, oijt, mijn,
-                                             mijt, fsb, msb, fnabs, kt, kr);
+            bool broke;
+            if (MODE == 1) {
+                const double4 xj0 = ldg_d4(&d.x0[j]), rj0 = ldg_d4(&d.rot[j]);
+                const double hx = 0.5 * (ri0.x + rj0.x), hy = 0.5 * (ri0.y + rj0.y), hz = 0.5 * (ri0.z + rj0.z);
+                const f3 du = mk3((float)(rd.x - (xj0.x - xi0.x) - (hy * rd.z - hz * rd.y)),
+                                  (float)(rd.y - (xj0.y - xi0.y) - (hz * rd.x - hx * rd.z)),
+                                  (float)(rd.z - (xj0.z - xi0.z) - (hx * rd.y - hy * rd.x)));
+                broke = bond_slot_ext_total(ep, b, r, sqrt(rr), du, mk3((float)ri0.x, (float)ri0.y, (float)ri0.z),
+                                            mk3((float)rj0.x, (float)rj0.y, (float)rj0.z), rij, oijt, mijn, mijt, rij,
+                                            oijt, mijn, mijt, fsb, msb, fnabs, kt, kr);
+            } else {
+                broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(vj), wi, f4to3(wj), rij, oijt, mijn, mijt, fsb,
+                                      msb, fnabs, kt, kr);
+            }
             ++npair;
             d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
             d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
@@ -2644,7 +2661,7 @@ rf_status fire_setup(rf_engine* e) {
     rf_status st;
     if ((st = dalloc(e, &d.frc, N)) || (st = dalloc(e, &d.mom, N)) ||
         (st = dalloc(e, &d.fpart, (size_t)e->nblocks * FIRE_SUMS)) || (st = dalloc(e, &d.rot, N)) ||
-        (st = dalloc(e, &d.x0, N)))
+        (st = dalloc(e, &d.x0, N)) || (st = dalloc(e, &d.bst0, 3 * (size_t)d.QB * N)))
         return st;
     e->cf = e->c;
     if (!getenv("RF_ENGINE_NO_GRAPH")) {
@@ -2680,6 +2697,8 @@ rf_status load_increment(rf_engine* e, const rf_relax_params* p, const float* wa
     h.fdec = p->f_dec; h.fshrink = p->f_alpha; h.fndelay = p->n_delay; h.ftol = p->tol; h.fmax_iter = p->max_iter;
     RF_CUDA(cudaMemcpyAsync(d.sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
     const double delta = p->strain_inc * h.Size0;
+    // the bond records' state at the start of the increment (FIRE mode computes from it)
+    RF_CUDA(cudaMemcpyAsync(d.bst0, d.bst, 3 * (size_t)d.QB * N * sizeof(float4), cudaMemcpyDeviceToDevice, s));
     if (e->task.kind == RF_TEST_BRAZIL) {
         k_qs_begin_scalars<RF_TEST_BRAZIL><<<1, 32, 0, s>>>(d, e->cf, delta);
         k_qs_begin<RF_TEST_BRAZIL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm, ldw, scaled, delta);

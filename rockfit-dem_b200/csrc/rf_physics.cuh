@@ -437,6 +437,97 @@ __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt&
     return false;
 }
 
+// One bond record inside a quasi-static increment (FIRE mode). The state is the record's
+// state at the start of the increment (Rij0, Oijt0, Mijn0, Mijt0) carried to the current
+// configuration in one step -- the start normal to the current one, the particles'
+// rotations ti, tj since the increment began, and du, the pair's relative motion since
+// then less the mean rotation's part ((r - r0) - ((ti + tj) / 2) x r, formed in double
+// by the caller: in float its terms cancel and the relaxation stalls on the rounding) --
+// with the formulas of bond_slot_ext. The relaxed state so depends on where the particles
+// are, not on the path the relaxation took: an exact warm start lands on it at once.
+__device__ __forceinline__ bool bond_slot_ext_total(const ExtParams& p, const BondExt& b, const f3 r,
+                                                    const double rlen, const f3 du, const f3 ti, const f3 tj,
+                                                    const f3 Rij0, const f3 Oijt0, const f3 Mijn0, const f3 Mijt0,
+                                                    f3& Rij, f3& Oijt, f3& Mijn, f3& Mijt, f3& fs, f3& ms,
+                                                    float& fnabs, float& kt, float& kr) {
+    const float rijm = (float)rlen;
+    const float inv_rm = __frcp_rn(rijm);
+    const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
+    const float stretch = (float)(rlen - b.L0);
+    const float A = b.br * b.br * RF_PI_F;
+    const float J = RF_PI_F * b.br * b.br * b.br * b.br;
+    kt += (b.kn + b.ks) * A;
+    kr += 0.25f * b.kn * J + 0.5f * b.ks * J + 0.25f * b.ks * A * rijm * rijm;
+    float cef = b.kn * stretch;
+    float Sc = cef;
+    cef *= A;
+    fnabs += fabsf(cef);
+    fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
+    const float tx = Rij0.y * nz - Rij0.z * ny;
+    const float ty = Rij0.z * nx - Rij0.x * nz;
+    const float tz = Rij0.x * ny - Rij0.y * nx;
+    const float wsx = tj.x + ti.x, wsy = tj.y + ti.y, wsz = tj.z + ti.z;
+    const float cphi = (wsx * nx + wsy * ny + wsz * nz) * 0.5f;
+    const float phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
+    Rij = mk3(nx, ny, nz);
+    const float M1x = 1.0f + tz * phz + ty * phy;
+    const float M1y = phz - tz - ty * phx;
+    const float M1z = -phy - tz * phx + ty;
+    const float M2x = tz - phz - tx * phy;
+    const float M2y = tz * phz + 1.0f + tx * phx;
+    const float M2z = -tz * phy + phx - tx;
+    const float M3x = -ty - tx * phz + phy;
+    const float M3y = -ty * phz + tx - phx;
+    const float M3z = ty * phy + tx * phx + 1.0f;
+    const float dwx = tj.x - ti.x, dwy = tj.y - ti.y, dwz = tj.z - ti.z;
+    {
+        float c1 = nx * dwx + ny * dwy + nz * dwz;
+        c1 *= 0.5f * b.ks;
+        const f3 o = Mijn0;
+        const float mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
+        const float my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
+        const float mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
+        Mijn = mk3(mx, my, mz);
+        ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+    }
+    {
+        const float c1 = nx * dwx + ny * dwy + nz * dwz;
+        const float c2 = 0.25f * b.kn;
+        const f3 o = Mijt0;
+        const float mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
+        const float my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
+        const float mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
+        Mijt = mk3(mx, my, mz);
+        ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+    }
+    float Mc;
+    {
+        float c = nx * du.x + ny * du.y + nz * du.z;
+        const f3 o = Oijt0;
+        const float ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (du.x - nx * c);
+        const float oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (du.y - ny * c);
+        const float oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (du.z - nz * c);
+        c = b.ks;
+        Mc = c;
+        c *= A;
+        fs.x += ox * c; fs.y += oy * c; fs.z += oz * c;
+        Oijt = mk3(ox, oy, oz);
+        ms.x += 0.5f * (r.y * oz - r.z * oy) * c;
+        ms.y += 0.5f * (r.z * ox - r.x * oz) * c;
+        ms.z += 0.5f * (r.x * oy - r.y * ox) * c;
+    }
+    Mc *= norm3(Oijt.x, Oijt.y, Oijt.z);
+    Sc += norm3(Mijt.x, Mijt.y, Mijt.z) * 4.0f * b.br;
+    Mc += norm3(Mijn.x, Mijn.y, Mijn.z) * 2.0f * b.br;
+    if ((Sc > b.sc) || (Mc > b.tc)) {
+        Oijt = mk3(0.f, 0.f, 0.f);
+        Mijn = mk3(0.f, 0.f, 0.f);
+        Mijt = mk3(0.f, 0.f, 0.f);
+        return true;
+    }
+    return false;
+}
+
 // Overlapping pair of the extended model. delta = r_i + r_j - |r| is formed in double
 // by the caller (in float it would cancel to a few significant bits at small overlaps);
 // mi, mj are the masses.

@@ -71,13 +71,13 @@ def _qs_total(on):
 
 def test_exact_warm_start_lands_on_the_relaxed_state():
     """Warm-starting a FIRE increment with its own relaxed answer (displacements and
-    rotations), FP64 oracle. With the bond state integrated iteration by iteration (the
-    engine's FIRE mode) the shear forces and moments depend on the relaxation's path: the
-    jump starts far above the tolerance and saves only part of the iterations. With the
-    state computed from the increment's start state and the motion since then (the
-    oracle's path-independent study rule) the jump lands on the relaxed state: the first
-    pass's residual is within a few times the tolerance and the warm run converges in a
-    small fraction of the iterations, to the same stress."""
+    rotations), FP64 oracle. With the bond state computed from the increment's start
+    state and the motion since then (the engine's FIRE mode) the jump lands on the relaxed
+    state: the first pass's residual is within a few times the tolerance and the warm run
+    converges in a small fraction of the iterations, to the same stress. With the state
+    integrated iteration by iteration instead (the explicit steps' rule) the shear forces
+    and moments depend on the relaxation's path: the jump starts far above the tolerance
+    and saves only part of the iterations."""
     t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
     p = rfdem.RelaxParams()
     rfdem.lib.rf_relax_default_params(C.byref(p), C.byref(t))
@@ -90,7 +90,7 @@ def test_exact_warm_start_lands_on_the_relaxed_state():
             full = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000)
             out[total] = (one, full)
     finally:
-        _qs_total(0)
+        _qs_total(1)
     one, full = out[1]
     assert one["res_plain"] <= p.tol
     assert one["res_warm"] < 20 * p.tol

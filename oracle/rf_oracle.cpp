@@ -1511,7 +1511,22 @@ struct RunExt {
                 const double* q = warm + 6 * i;
                 TF u[6];
                 for (int a = 0; a < 6; ++a) u[a] = (TF)(float)q[a];
+                // a particle the platens held at the end of the last increment stays on its
+                // platen (the top one has moved by delta)
+                const bool brz = t->kind == RF_TEST_BRAZIL;
+                const double off = rad[i] - t->Po.p_r;
+                const double Zcut = brz ? (double)(float)((double)t->S.center.y + (double)t->S.spacesized2.y)
+                                        : (double)(float)((double)t->S.center.z + (double)t->S.spacesized2.z);
+                const double a0 = brz ? R[i + N] : R[i + 2 * N];
+                const float q0 = (float)(R[i] - Kc.center.x);
+                const float q1 = brz ? (float)(R[i + 2 * N] - Kc.center.z) : (float)(R[i + N] - Kc.center.y);
+                const bool zone = q0 * q0 + q1 * q1 < Kc.RR && (brz ? (double)(float)(R[i + 2 * N] - Kc.center.z) : a0) < Zcut;
+                const bool at_top = zone && a0 + off - (Kc.Top + delta) > -1e-9;
+                const bool at_bottom = zone && a0 - off - Kc.Bottom < 1e-9;
                 R[i] += (double)u[0]; R[i + N] += (double)u[1]; R[i + 2 * N] += (double)u[2];
+                double& ax = brz ? R[i + N] : R[i + 2 * N];
+                if (at_top) ax = Kc.Top - off;
+                else if (at_bottom) ax = Kc.Bottom + off;
                 v0 = u[0] * idt0; v1 = u[1] * idt0; v2 = u[2] * idt0;
                 W[i] = u[3] * idt0; W[i + N] = u[4] * idt0; W[i + 2 * N] = u[5] * idt0;
                 ROT[3 * i] = u[3]; ROT[3 * i + 1] = u[4]; ROT[3 * i + 2] = u[5];

@@ -1506,10 +1506,23 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int 
                 const float sd = (float)D, sr = (float)(D / x.w);
                 u[0] *= sd; u[1] *= sd; u[2] *= sd; u[3] *= sr; u[4] *= sr; u[5] *= sr;
             }
+            // a particle the platens held at the end of the last increment stays on its
+            // platen (the top one has moved by D): the prediction's error along the load
+            // axis must not lift it off
+            const double off = x.w - c.p_r_d;
+            const double a0 = KIND == RF_TEST_BRAZIL ? x.y : x.z;
+            const float q0 = (float)(x.x - cc.x), q1 = KIND == RF_TEST_BRAZIL ? (float)(x.z - cc.z) : (float)(x.y - cc.y);
+            const bool zone = q0 * q0 + q1 * q1 < RR && (KIND == RF_TEST_BRAZIL ? (double)(float)(x.z - cc.z) : a0) <
+                                                          (double)c.zcut;
+            const bool at_top = zone && a0 + off - (Top + D) > -1e-9;
+            const bool at_bottom = zone && a0 - off - Bottom < 1e-9;
             x.x += (double)u[0]; x.y += (double)u[1]; x.z += (double)u[2];
             v0 = u[0] * idt0; v1 = u[1] * idt0; v2 = u[2] * idt0;
             w = make_float4(u[3] * idt0, u[4] * idt0, u[5] * idt0, 0.f);
             rot = make_double4(u[3], u[4], u[5], 0.0);
+            double& ax = KIND == RF_TEST_BRAZIL ? x.y : x.z;
+            if (at_top) ax = Top - off;
+            else if (at_bottom) ax = Bottom + off;
         }
         // the platen pushes the particles it passed: clamp them now, so the first force
         // pass (and its convergence test) sees the loaded configuration

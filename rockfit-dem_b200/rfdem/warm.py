@@ -52,12 +52,20 @@ class WarmStart:
             losses.append(self.mlp.train_step(X, T, rows, a))
         return losses
 
-    def predict(self, engine):
+    def predict(self, engine, rotations=False):
         """The prediction for `engine`'s next increment: float32 [rows, 16] on the device.
-        The engine and the MLP run on their own streams: each hand-over synchronises."""
+        The engine and the MLP run on their own streams: each hand-over synchronises.
+        rotations=False starts the particles' rotations from zero instead of the predicted
+        ones: the converged rotations change much from one increment to the next, and
+        with a displacement prediction that is not exact, zero rotations let FIRE
+        converge in fewer iterations (measured on the 200k bench specimen: with the last
+        increment's displacements, 915 iterations with zero rotations, 1604 with the exact
+        rotations; 1759 plain)."""
         self.features(engine)
         self.torch.cuda.synchronize()
         self.mlp.forward(self.feat, self.N, self.Y)
+        if not rotations:
+            self.Y[:, 3:6] = 0.0
         self.torch.cuda.synchronize()
         return self.Y
 

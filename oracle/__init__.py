@@ -63,6 +63,8 @@ def _declare(L):
         "rfo_qs_ext_f": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
         "rfo_qs_ext_d": (i32, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, P, P, P, P, P, u64]),
         "rfo_warm_probe_ext_d": (None, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, u64, P]),
+        "rfo_warm_probe_ext_f": (None, [T, C.POINTER(rfdem.ExtParams), P, P, C.POINTER(rfdem.RelaxParams), u64, u64, P,
+                                        f64, f64]),
         "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
         "rfo_run_ext_pos_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P, i32]),
         "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
@@ -153,15 +155,21 @@ def qs_ext(task, x, R0, radius, params, n_inc, fp64=False, trace_cap=0):
     return dict(R=R, iters=it, converged=cv, residual=rs, stress=st, trace=tr[:trace_cap], status=status)
 
 
-def warm_probe(task, x, R0, radius, params, n_pre, warm_iters):
+def warm_probe(task, x, R0, radius, params, n_pre, warm_iters, fp64=True, scale=1.0, noise=0.0):
     """FP64 extended oracle: after n_pre plain FIRE increments, relax the next increment
     plainly and, from the same state, warm-started with that plain answer (displacements
-    and rotations) for at most warm_iters iterations. Returns a dict of iterations,
+    and rotations; fp64=False: float forces, the warm start scaled by scale + noise * U[-1, 1)
+    per particle) for at most warm_iters iterations. Returns a dict of iterations,
     residuals, platen stresses and the largest bond-state differences between the two."""
     L = load()
     out = np.zeros(15, np.float64)
-    L.rfo_warm_probe_ext_d(C.byref(task), C.byref(x), p(np.ascontiguousarray(R0, np.float64)),
-                           p(np.ascontiguousarray(radius, np.float64)), C.byref(params), n_pre, warm_iters, p(out))
+    args = [C.byref(task), C.byref(x), p(np.ascontiguousarray(R0, np.float64)),
+            p(np.ascontiguousarray(radius, np.float64)), C.byref(params), n_pre, warm_iters, p(out)]
+    if fp64:
+        assert scale == 1.0 and noise == 0.0, "the FP64 probe warm-starts with the exact answer"
+        L.rfo_warm_probe_ext_d(*args)
+    else:
+        L.rfo_warm_probe_ext_f(*args, scale, noise)
     keys = ["it_plain", "res_plain", "res_warm", "stress_plain", "stress_warm", "dOijt", "maxOijt", "dMijn", "maxMijn",
             "dMijt", "maxMijt", "dRij", "dx", "it_warm", "conv_warm"]
     return dict(zip(keys, out.tolist()))

@@ -1673,9 +1673,12 @@ namespace rfo {
 // (reference) and once from the same state warm-started with the plain answer; returns
 // the warm start's residual after `warm_iters` iterations the largest differences of the
 // bond state from the plain relaxed state, and the warm run's iterations and convergence flag.
+// scale != 1 or noise != 0 make the warm start inexact: each particle's displacement and
+// rotation times (scale + noise * u), u uniform in [-1, 1) from a fixed sequence.
 template <class TF>
 static void warm_probe(rf_task* t, const rf_ext_params* xp, const double* R0, const double* rad,
-                       const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out) {
+                       const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out,
+                       double scale = 1.0, double noise = 0.0) {
     RunExt<TF> a;
     a.t = t;
     a.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
@@ -1688,10 +1691,14 @@ static void warm_probe(rf_task* t, const rf_ext_params* xp, const double* R0, co
     b.t = &tb;
     const uint64_t it_plain = a.fire_increment(*p, &c, &res, nullptr, 0);
     std::vector<double> warm(6 * a.N);
+    uint64_t lcg = 0x2545F4914F6CDD1Dull;
     for (uint64_t i = 0; i < a.N; ++i)
         for (int k = 0; k < 3; ++k) {
-            warm[6 * i + k] = a.R[i + k * a.N] - a.X0[i + k * a.N];
-            warm[6 * i + 3 + k] = a.ROT[3 * i + k];
+            lcg = lcg * 6364136223846793005ull + 1442695040888963407ull;
+            const double u = (double)(lcg >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+            const double f = scale + noise * u;
+            warm[6 * i + k] = (a.R[i + k * a.N] - a.X0[i + k * a.N]) * f;
+            warm[6 * i + 3 + k] = a.ROT[3 * i + k] * f;
         }
     rf_relax_params q = *p;
     q.max_iter = warm_iters;
@@ -1720,6 +1727,12 @@ extern "C" {
 void rfo_warm_probe_ext_d(rf_task* t, const rf_ext_params* x, const double* R0, const double* rad,
                           const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out) {
     rfo::warm_probe<double>(t, x, R0, rad, p, n_pre, warm_iters, out);
+}
+// The same with float forces (the engine's arithmetic) and an inexact warm start.
+void rfo_warm_probe_ext_f(rf_task* t, const rf_ext_params* x, const double* R0, const double* rad,
+                          const rf_relax_params* p, uint64_t n_pre, uint64_t warm_iters, double* out, double scale,
+                          double noise) {
+    rfo::warm_probe<float>(t, x, R0, rad, p, n_pre, warm_iters, out, scale, noise);
 }
 int rfo_qs_ext_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, const rf_relax_params* p,
                  uint64_t n_inc, uint64_t* iters, int* conv, double* res, double* stress, double* trace,

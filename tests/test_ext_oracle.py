@@ -179,3 +179,20 @@ def test_position_precision_fp64_vs_hilo_vs_fp32():
     assert stress["f64"] < 1e-5 and stress["hilo"] < 1e-5
     assert err["f32"] > 1e4 * max(err["f64"], err["hilo"])
     assert stress["f32"] > 0.05
+
+
+def test_inexact_warm_starts_reach_the_plain_relaxed_state():
+    """Float forces (the engine's arithmetic): a warm start with the exact answer lands in a
+    few passes; one off by 20 % (over- or under-predicted, or with 20 % per-particle
+    noise) still converges, to the plain run's platen stress -- particles the platens held
+    stay on them, so the prediction cannot lift the specimen off a platen."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, min_stress=1e3)
+    p = rfdem.RelaxParams()
+    rfdem.lib.rf_relax_default_params(C.byref(p), C.byref(t))
+    p.max_iter, p.strain_inc = 40000, 1e-4
+    exact = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000, fp64=False)
+    assert exact["conv_warm"] == 1 and exact["it_warm"] * 20 < exact["it_plain"]
+    for scale, noise in ((1.2, 0.0), (0.8, 0.0), (1.0, 0.2)):
+        o = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000, fp64=False, scale=scale, noise=noise)
+        assert o["conv_warm"] == 1 and o["it_warm"] < o["it_plain"], (scale, noise)
+        assert abs(o["stress_warm"] / o["stress_plain"] - 1.0) < 1e-4, (scale, noise)

@@ -196,3 +196,19 @@ def test_inexact_warm_starts_reach_the_plain_relaxed_state():
         o = oracle.warm_probe(mc.clone(t), x, R, rad, p, 4, 40000, fp64=False, scale=scale, noise=noise)
         assert o["conv_warm"] == 1 and o["it_warm"] < o["it_plain"], (scale, noise)
         assert abs(o["stress_warm"] / o["stress_plain"] - 1.0) < 1e-4, (scale, noise)
+
+
+def test_brazil_fire_increments_and_exact_warm_start():
+    """The quasi-static path on a Brazilian disc (platens along y): float-force FIRE
+    converges every increment with the stress rising, and an exact warm start lands in a
+    few passes on the same stress."""
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_BRAZIL, 8.0, 3.0, min_stress=1e3)
+    p = rfdem.RelaxParams()
+    rfdem.lib.rf_relax_default_params(C.byref(p), C.byref(t))
+    p.max_iter, p.strain_inc = 20000, 1e-4
+    o = oracle.qs_ext(mc.clone(t), x, R, rad, p, 5)
+    assert o["status"] == 0 and np.all(o["converged"] == 1)
+    assert np.all(np.diff(o["stress"]) > 0) and o["stress"][0] > 0
+    w = oracle.warm_probe(mc.clone(t), x, R, rad, p, 3, 20000, fp64=False)
+    assert w["conv_warm"] == 1 and w["it_warm"] * 10 < w["it_plain"]
+    assert abs(w["stress_warm"] / w["stress_plain"] - 1.0) < 1e-5

@@ -169,14 +169,17 @@ rf_status md_CellDistribution(const float* R, uint_fast32_t N, uint_fast32_t* CI
 /*
  * md_CellDistribution without any allocation. No counterpart in the reference: it is
  * for callers that cannot allocate device memory where they bin -- a framework that
- * owns every device byte through its own allocator, or a step loop that cannot afford
- * cudaMalloc's implicit synchronisation. Same outputs as md_CellDistribution; the
- * scratch is a fixed array inside this library (cell grids up to 524,287 cells, about
- * 6.3 MB held by every GPU that loads the library, until exit). Larger grids are
- * rejected with RF_ERR_INVALID. The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture. All calls share the one array, so calls whose
- * work overlaps on the GPU (other streams, other host threads) race: serialise them.
+ * owns every device byte through its own allocator, or a plugin that is handed only
+ * its input and output buffers. Same outputs as md_CellDistribution; the scratch is a
+ * fixed array inside this library (cell grids up to 524,287 cells, about 6.3 MB held
+ * by every GPU that loads the library, until exit). Larger grids are rejected with
+ * RF_ERR_INVALID. The first call on a device (and the first after a cudaDeviceReset)
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture. Like every md_* entry
+ * point, the call blocks the calling thread until its work on `stream` has finished,
+ * because it reads the device status word back. All calls share the one array, so
+ * calls whose work overlaps on the GPU (other streams, other host threads) race:
+ * serialise them.
  */
 rf_status md_CellDistributionNoAlloc(const float* R, uint_fast32_t N, uint_fast32_t* CI, uint_fast32_t* CIs,
                                      uint_fast32_t* pnC, uint_fast32_t CN, float _1d_a, rf_uint3 cN,

@@ -14,9 +14,10 @@ Build recipe for the checkers:
   which its source needs on Linux) plus ``oracle/ref/ref_io_harness.cpp``, and its
   conjugate-gradient parameter update (mp_task.h) behind ``oracle/ref/ref_fit_harness.cpp``.
 
-The ``_ref`` builds read the reference sources where they lie (``--ref`` or
-``$RF_REFERENCE_DIR``, default ``/root/reference``) and are skipped when that tree
-is absent; their outputs are git-ignored but travel with the working tree.
+The ``_ref`` builds read the reference sources where they lie: the ``ref_dir``
+argument, else ``$RF_REFERENCE_DIR``, else a ``reference`` directory beside the
+repository checkout. They are skipped when that tree is absent; their outputs are
+git-ignored but travel with the working tree.
 """
 import os
 import subprocess
@@ -27,6 +28,8 @@ BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CUDA_INC = "/usr/local/cuda/include"
+# the reference checkout next to this repository's root directory
+REF_BESIDE_REPO = os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 # The reference translation units on the live hot path (and what they need to link).
 REF_GPU_SOURCES = [
@@ -73,7 +76,7 @@ def build_oracle(force=False):
 
 
 def build_ref(ref_dir=None, force=False, gpu=True, cpu=True):
-    ref_dir = ref_dir or os.environ.get("RF_REFERENCE_DIR", "/root/reference")
+    ref_dir = ref_dir or os.environ.get("RF_REFERENCE_DIR") or REF_BESIDE_REPO
     if not os.path.isdir(ref_dir):
         return None
     os.makedirs(REF_OUT, exist_ok=True)

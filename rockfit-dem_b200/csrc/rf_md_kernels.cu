@@ -37,12 +37,12 @@ __global__ void k_cell_index(const float* __restrict__ R, size_t N, mid_t* __res
         uint32_t cx, cy, cz;
         const uint32_t c = ref_cell(ld3p(R, N, i), g, &cx, &cy, &cz);
         CI[i] = (mid_t)c;
-        if (cx > g.nx - 1 || cy > g.ny - 1 || cz > g.nz - 1 || (uint64_t)c >= g.CN) {
+        if (cx > g.nx - 1 || cy > g.ny - 1 || cz > g.nz - 1 || (uint64_t)c >= g.CN)
             raise_status(err, RF_ERR_CELL_RANGE);
-            if (counts) atomicAdd(&counts[g.CN], 1u);         // out-of-grid keys go to a tail bin
-        } else if (counts) {
-            atomicAdd(&counts[c], 1u);
-        }
+        // binned by the key, as the sort orders it: a key past the grid goes to the tail
+        // bin; an out-of-range cell coordinate whose linear key still lands inside the grid
+        // (it wraps into another row) is binned under that key, as the scatter files it
+        if (counts) atomicAdd(&counts[(uint64_t)c < g.CN ? (uint64_t)c : g.CN], 1u);
     }
 }
 
@@ -404,19 +404,66 @@ __global__ void k_fdotv(const float* __restrict__ V, const float* __restrict__ F
     block_sum2(s, dummy);
     if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
-// Status word shared by the md_* launches of one host thread.
-static uint32_t* status_word() {
-    static thread_local uint32_t* w = nullptr;
-    if (!w) {
-        if (cudaMalloc(&w, sizeof(uint32_t)) != cudaSuccess) return nullptr;
-        cudaMemset(w, 0, sizeof(uint32_t));
+// Identity of the CUDA context current on the calling thread, unique within the process
+// (cuCtxGetId). A cudaDeviceReset destroys the device's primary context together with
+// every device address taken in it; the next runtime call makes a new context with a
+// new id, so an address cached with the id of the context it came from is known to be
+// stale when the ids differ. cudaSetDevice makes the device's primary context current
+// (creating it if needed) and allocates nothing. The driver functions come through
+// cudaGetDriverEntryPoint, so the library keeps linking against the runtime only.
+static rf_status current_context_id(int dev, unsigned long long* id) {
+    typedef int (*ctx_get_current_t)(void**);
+    typedef int (*ctx_get_id_t)(void*, unsigned long long*);
+    static ctx_get_current_t get_current = nullptr;
+    static ctx_get_id_t get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = (ctx_get_current_t)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (ctx_get_id_t)f;
+    });
+    if (!get_current || !get_id) { set_error("driver entry points cuCtxGetCurrent / cuCtxGetId unavailable"); return RF_ERR_CUDA; }
+    RF_CUDA(cudaSetDevice(dev));
+    void* ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) {
+        set_error("no CUDA context current on device %d", dev);
+        return RF_ERR_CUDA;
     }
-    return w;
+    return RF_OK;
+}
+
+// Status word of the md_* launches of one host thread on the current device (one per
+// device, re-made when the device's context was reset). nullptr if it cannot be had.
+static uint32_t* status_word() {
+    const int kMaxDev = 64;
+    static thread_local uint32_t* w[kMaxDev] = {nullptr};
+    static thread_local unsigned long long ctx[kMaxDev] = {0};
+    int dev = 0;
+    unsigned long long id = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return nullptr;
+    if (current_context_id(dev, &id) != RF_OK) return nullptr;
+    if (!w[dev] || ctx[dev] != id) {
+        // a word of an earlier context went away with it; a word of this one is kept
+        w[dev] = nullptr;
+        uint32_t* p = nullptr;
+        if (cudaMalloc(&p, sizeof(uint32_t)) != cudaSuccess) return nullptr;
+        if (cudaMemset(p, 0, sizeof(uint32_t)) != cudaSuccess) { cudaFree(p); return nullptr; }
+        w[dev] = p;
+        ctx[dev] = id;
+    }
+    return w[dev];
 }
 
 // Read and clear the status word after a launch sequence (synchronises the stream).
 static rf_status take_status(cudaStream_t s) {
     uint32_t* w = status_word();
+    if (!w) { set_error("md_* status word unavailable on the current device"); return RF_ERR_CUDA; }
     uint32_t h = 0;
     RF_CUDA(cudaMemcpyAsync(&h, w, sizeof(h), cudaMemcpyDeviceToHost, s));
     RF_CUDA(cudaStreamSynchronize(s));
@@ -655,12 +702,13 @@ rf_status md_FdotVEntire(const float* V, const float* F, double* FdotV, uint64_t
 //
 // Some callers cannot allocate device memory at the point where they bin: a host
 // framework that owns every device byte through its own allocator and forbids other
-// allocations, or a latency-critical step loop where cudaMalloc's implicit device
-// synchronisation is not acceptable. md_CellDistribution needs caller-provided
-// scratch; md_CellDistributionNoAlloc instead uses the file-scope device array below
-// as its scratch, so it allocates nothing. The array is fixed in size (cell grids of
-// up to RF_NOALLOC_MAX_CELLS - 1 cells, about 6.3 MB) and every GPU that loads this
-// library holds it until the process exits.
+// allocations, or a plugin handed only its input and output buffers.
+// md_CellDistribution needs caller-provided scratch; md_CellDistributionNoAlloc
+// instead uses the file-scope device array below as its scratch, so it allocates
+// nothing. The array is fixed in size (cell grids of up to RF_NOALLOC_MAX_CELLS - 1
+// cells, about 6.3 MB) and every GPU that loads this library holds it until the
+// process exits. Like the other md_* entry points, a call returns only once its work
+// on the stream has finished: it reads the device status word back.
 // ---------------------------------------------------------------------------
 #define RF_NOALLOC_MAX_CELLS (1u << 19)   /* cells + the out-of-grid tail bin */
 #define RF_NOALLOC_WORDS (3u * RF_NOALLOC_MAX_CELLS + 256u)
@@ -670,21 +718,28 @@ namespace rf {
 namespace {
 // Device address of g_noalloc_scratch per device. In host code the symbol name is
 // only a host-side stand-in, so the address comes from cudaGetSymbolAddress, once
-// per device, with that device current.
+// per device, with that device current. The address belongs to the context it was
+// taken in: after a cudaDeviceReset the array lives at a new address in the new
+// context, so the lookup is redone when the context id differs from the cached one.
 const int kMaxDevices = 64;
 uint32_t* g_noalloc_ptr[kMaxDevices] = {nullptr};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {0};
 std::mutex g_noalloc_mu;
 
 rf_status noalloc_scratch(uint32_t** out) {
     int dev = 0;
     RF_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) { set_error("md_CellDistributionNoAlloc: device %d out of range", dev); return RF_ERR_INVALID; }
+    unsigned long long id = 0;
+    rf_status st = current_context_id(dev, &id);
+    if (st) return st;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    if (!g_noalloc_ptr[dev] || g_noalloc_ctx[dev] != id) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_status(e, "md_CellDistributionNoAlloc: cudaGetSymbolAddress");
         g_noalloc_ptr[dev] = (uint32_t*)p;
+        g_noalloc_ctx[dev] = id;
     }
     *out = g_noalloc_ptr[dev];
     return RF_OK;

@@ -45,6 +45,8 @@ class WarmStart:
     def train(self, steps=400, lr=2e-3, lr_final=5e-4):
         X = self.torch.cat(self.X)
         T = self.torch.cat(self.T)
+        # the concatenations run on torch's stream, the training steps on the MLP's own
+        self.torch.cuda.synchronize()
         rows = X.shape[0]
         losses = []
         for it in range(steps):
@@ -64,6 +66,9 @@ class WarmStart:
         self.features(engine)
         self.torch.cuda.synchronize()
         self.mlp.forward(self.feat, self.N, self.Y)
+        # the forward pass runs on the MLP's stream: finish it before torch's stream
+        # touches Y (the engine reads Y on its own stream after this returns)
+        self.torch.cuda.synchronize()
         if not rotations:
             self.Y[:, 3:6] = 0.0
         self.torch.cuda.synchronize()

@@ -357,6 +357,15 @@ typedef struct rf_ext_params {
     double list_gap;          /* 0: a pair is listed within a_farcut (the reference's rule); g > 0:
                                  within min(a_farcut, r_i + r_j + g), which keeps the rows of small
                                  particles short when the radii span a wide range */
+    int32_t ref_mode;         /* 1: the reference's constants in this model (every radius must equal
+                                 t->Po.p_r): bonds where the centre distance is below Po.b_d, bond
+                                 radius Po.b_r, stiffness per area m_E / L0 and m_G / L0 from each
+                                 bond's own rest length, strengths m_Ec and m_Gc, and the bending
+                                 moment summed with the reference's extra dt*E/(4 L0) factor
+                                 (md_calculateforcesdem3.cu:131-152). The other fields of this
+                                 struct but post_peak_drop and list_gap are then ignored. Explicit
+                                 steps only. 0: the extended model as described above. */
+    int32_t reserved;         /* 0 */
 } rf_ext_params;
 
 /* Create an extended-model engine: h_R double[3N] planar (mm), h_radius double[N].

@@ -46,6 +46,8 @@ def _declare(L):
         "rfo_delete_far_links_f": (None, [P, u64, P, P, P, P, P, P, u64, f32]),
         "rfo_construct_bonds_f": (None, [P, u64, P, P, P, P, P, P, P, u64, f32]),
         "rfo_forces_22_f": (None, [P, P, P, P, P, P, P, P, P, P, P, P, u64, u64, f32, f32, f32, f32, f32, f32, P]),
+        "rfo_forces_22_crit_f": (None, [P, P, P, P, P, P, P, P, P, P, P, P, u64, u64, f32, f32, f32, f32, f32, f32,
+                                        P, P]),
         "rfo_forces_21_f": (None, [P, P, P, P, P, P, P, P, u64, u64, f32, f32, f32, f32, f32, f32, f32, f32]),
         "rfo_increments_f": (None, [P, P, P, P, P, u64, f32, f32, f32]),
         "rfo_brazil_platen_f": (None, [P, P, P, u64, f3, f32, f32, f32, f32, f32, f32, f32, P]),

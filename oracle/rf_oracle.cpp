@@ -293,7 +293,8 @@ static inline T norm3(T x, T y, T z) { return std::sqrt(x * x + y * y + z * z); 
 template <class T>
 void forces_22(const T* R, const T* V, const T* W, const id_t* IL, uint8_t* ILtype, const T* iL,
                V3<T>* Rij, V3<T>* Oijt, V3<T>* Mijn, V3<T>* Mijt, T* F, T* M, uint64_t N, uint64_t K,
-               const FP<T>& p, uint8_t* broke /* may be null: 1 where a bond broke */) {
+               const FP<T>& p, uint8_t* broke /* may be null: 1 where a bond broke */,
+               T* crit = nullptr /* may be null: the break criteria (Sc, Mc) of each bond slot */) {
     const T PI = pi_t<T>();
     for (uint64_t i = 0; i < N; ++i) {
         T fsx = 0, fsy = 0, fsz = 0, msx = 0, msy = 0, msz = 0;
@@ -382,6 +383,7 @@ void forces_22(const T* R, const T* V, const T* W, const id_t* IL, uint8_t* ILty
                 Mc *= norm3(o.x, o.y, o.z);
                 Sc += norm3(mt.x, mt.y, mt.z) * (T)4.0f * p.b_r;
                 Mc += norm3(mn.x, mn.y, mn.z) * (T)2.0f * p.b_r;
+                if (crit) { crit[2 * k] = Sc; crit[2 * k + 1] = Mc; }
                 if ((Sc > p.m_Gcritn) || (Mc > p.m_Gcritt)) {
                     ILtype[k] = 0;
                     Oijt[k] = {0, 0, 0};
@@ -850,7 +852,13 @@ struct ExtPar {
     uint64_t seed;
     double drop;      // post-peak stop: fracture once the stress is below (1 - drop) x peak (0: off)
     double lgap;      // list gap: 0 lists pairs within a_farcut; g > 0 within min(a_farcut, r_i + r_j + g)
+    int ref;          // reference constants (rf_ext_params.ref_mode): b_d bond rule, b_r, E/L0, G/L0,
+                      // global strengths, the Q1 bending factor (md_calculateforcesdem3.cu:131-152)
 };
+static inline ExtPar ext_par(const rf_ext_params* xp) {
+    return ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
+                  xp->post_peak_drop, xp->list_gap, xp->ref_mode};
+}
 
 static inline uint64_t mix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
@@ -898,6 +906,7 @@ struct RunExt {
     ExtPar x;
     uint64_t N, K, CN;
     std::vector<double> R, rad, L0, sig, tau;
+    std::vector<TF> iL0;        // 1 / rest length per slot (reference constants: stiffness E/L0, G/L0)
     std::vector<float> Rf;
     std::vector<TF> V, W;
     std::vector<id_t> IL, CI, CIs, pnC;
@@ -915,6 +924,7 @@ struct RunExt {
     int status;
     uint64_t steps, broken;
     TF dt, hm_E, hm_G, p_A, mu, mur, kn, ks, lambda, cmass;
+    TF mE, mG, b_r;             // the task's moduli and bond radius (reference constants)
 
     void to_float() {
         for (uint64_t q = 0; q < 3 * N; ++q) Rf[q] = (float)R[q];
@@ -946,7 +956,7 @@ struct RunExt {
             for (double& v : R) v = (double)(float)v;
         V.assign(3 * N, 0); W.assign(3 * N, 0);
         IL.assign(N * K, EMPTY); type.assign(N * K, 0); L0.assign(N * K, 1.0); sig.assign(N * K, 0.0);
-        tau.assign(N * K, 0.0);
+        tau.assign(N * K, 0.0); iL0.assign(N * K, (TF)0);
         Rij.assign(N * K, {0, 0, 0}); Oijt = Rij; Mijn = Rij; Mijt = Rij;
         CI.assign(N, 0); CIs.assign(2 * N, 0); pnC.assign(2 * CN, 0);
         sz0 = t->sz0 != 0.0 ? t->sz0 : (double)t->Compress.size.z;
@@ -954,6 +964,7 @@ struct RunExt {
         const rf_potential& P = t->Po;
         dt = (TF)P.dt; hm_E = (TF)P.hm_E; hm_G = (TF)P.hm_G; p_A = (TF)P.p_A; mu = (TF)P.p_mu; mur = (TF)P.p_mur;
         kn = (TF)x.kn; ks = (TF)x.ks; lambda = (TF)x.lambda; cmass = (TF)(P.p_m / (P.p_r * P.p_r * P.p_r));
+        mE = (TF)P.m_E; mG = (TF)P.m_G; b_r = (TF)P.b_r;
         aa_farcut = P.aa_farcut; aacut = (double)t->aacut; a_farcut = P.a_farcut;
         to_float();
         const float inv_a = t->C._1d_a, a = t->C.a;
@@ -963,7 +974,9 @@ struct RunExt {
         else s = construct_list<float>(Rf.data(), N, CIs.data(), pnC.data(), IL.data(), K, a, inv_a, t->aacut,
                                        t->C.Nr, CN);
         if (s) status = s;
-        // bonds: gap below gap_frac * min radius; FP64 rest length; Weibull strengths per pair
+        // bonds: gap below gap_frac * min radius; FP64 rest length; Weibull strengths per pair.
+        // With the reference constants: centre distance below b_d (md_boundinteractions_construct.cu:62,
+        // here on the FP64 distance), the global strengths m_Ec and m_Gc.
         for (uint64_t i = 0; i < N; ++i)
             for (uint64_t q = 0; q < K; ++q) {
                 const uint64_t k = i * K + q;
@@ -971,12 +984,21 @@ struct RunExt {
                 if (j == EMPTY || j >= N) continue;
                 const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
                 const double L = std::sqrt(dx * dx + dy * dy + dz * dz);
-                if (!(L - rad[i] - rad[j] < x.gap * std::fmin(rad[i], rad[j])) || !(L > 0)) continue;
+                if (x.ref) {
+                    if (!(L < P.b_d) || !(L > 0)) continue;
+                } else if (!(L - rad[i] - rad[j] < x.gap * std::fmin(rad[i], rad[j])) || !(L > 0)) {
+                    continue;
+                }
                 type[k] = 1;
                 L0[k] = L;
-                const double us = pair_uniform(x.seed, i, j, 0), ut = pair_uniform(x.seed, i, j, 1);
-                sig[k] = x.sig * std::pow(-std::log(us), 1.0 / x.wm);
-                tau[k] = x.tau * std::pow(-std::log(ut), 1.0 / x.wm);
+                iL0[k] = (TF)(1.0 / L);
+                if (x.ref) {
+                    sig[k] = P.m_Ec; tau[k] = P.m_Gc;
+                } else {
+                    const double us = pair_uniform(x.seed, i, j, 0), ut = pair_uniform(x.seed, i, j, 1);
+                    sig[k] = x.sig * std::pow(-std::log(us), 1.0 / x.wm);
+                    tau[k] = x.tau * std::pow(-std::log(ut), 1.0 / x.wm);
+                }
                 if (sizeof(TF) == 4) { sig[k] = (float)sig[k]; tau[k] = (float)tau[k]; }
             }
         // DeleteFarLinks on the float positions, as the initial build does (with a list gap
@@ -1066,10 +1088,14 @@ struct RunExt {
         }
     }
 
-    // One bond slot (engine bond_slot_ext).
+    // One bond slot (engine bond_slot_ext). With the reference constants the stiffness per
+    // area is E/L0 and G/L0 of the slot (the reference's E*_1d_iL, G*_1d_iL) and the bending
+    // moment carries the extra dt*E/(4 L0) factor (Q1, md_calculateforcesdem3.cu:131-152).
     bool bond(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& vi, const V3<TF>& vj, const V3<TF>& wi,
               const V3<TF>& wj, TF br, V3<TF>& fs, V3<TF>& ms, double& fnsum, double* kt, double* kr) {
         const TF PI = pi_t<TF>();
+        const TF kn = x.ref ? mE * iL0[k] : this->kn;
+        const TF ks = x.ref ? mG * iL0[k] : this->ks;
         const TF rijm = (TF)rlen;
         const TF inv_rm = rcp(rijm);
         const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
@@ -1113,7 +1139,12 @@ struct RunExt {
             const TF my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
             const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
             Mijt[k] = {mx, my, mz};
-            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;    // no Q1 factor in this model
+            if (x.ref) {                                        // Q1: the factor again
+                const TF q = c2 * J;
+                ms.x += mx * q; ms.y += my * q; ms.z += mz * q;
+            } else {
+                ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+            }
         }
         TF Mc;
         {
@@ -1317,7 +1348,7 @@ struct RunExt {
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
                 const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
-                const TF br = lambda * std::min(ri, (TF)rad[j]);
+                const TF br = x.ref ? b_r : lambda * std::min(ri, (TF)rad[j]);
                 bool broke;
                 if (qs_total) {
                     // the pair's relative displacement since the increment began, formed in
@@ -1366,7 +1397,12 @@ struct RunExt {
                 TF vt, double& sfb, double& sft) const {
         const rf_compression& Kc = t->Compress;
         const float cx = Kc.center.x, cy = Kc.center.y, cz = Kc.center.z, RR = Kc.RR;
-        const double Top = Kc.Top, Bottom = Kc.Bottom, TopR = Kc.TopR, BottomR = Kc.BottomR;
+        // with the reference constants the platen coordinates are rounded to float, as the
+        // reference's drivers pass them to d_UniaxialCompression3_simple / d_braziltest_simple2
+        const double Top = x.ref ? (double)(float)Kc.Top : Kc.Top;
+        const double Bottom = x.ref ? (double)(float)Kc.Bottom : Kc.Bottom;
+        const double TopR = x.ref ? (double)(float)Kc.TopR : Kc.TopR;
+        const double BottomR = x.ref ? (double)(float)Kc.BottomR : Kc.BottomR;
         const bool brz = t->kind == RF_TEST_BRAZIL;
         const double Zcut = brz ? (double)(float)((double)t->S.center.y + (double)t->S.spacesized2.y)
                                 : (double)(float)((double)t->S.center.z + (double)t->S.spacesized2.z);
@@ -1626,8 +1662,7 @@ static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const
     RunExt<TF> r;
     r.pos_mode = pos_mode;
     r.t = t;
-    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
-                 xp->post_peak_drop, xp->list_gap};
+    r.x = ext_par(xp);
     r.init(R_io, rad);
     uint64_t ns = 0;
     while (r.running() && r.steps < max_steps) r.step(curve, cap, &ns);   // max_steps 0: bonds only
@@ -1653,8 +1688,7 @@ static int qs_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const doubl
                   uint64_t trace_cap) {
     RunExt<TF> r;
     r.t = t;
-    r.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
-                 xp->post_peak_drop, xp->list_gap};
+    r.x = ext_par(xp);
     r.init(R_io, rad);
     for (uint64_t k = 0; k < n_inc; ++k) {
         int c = 0;
@@ -1681,8 +1715,7 @@ static void warm_probe(rf_task* t, const rf_ext_params* xp, const double* R0, co
                        double scale = 1.0, double noise = 0.0) {
     RunExt<TF> a;
     a.t = t;
-    a.x = ExtPar{xp->kn, xp->ks, xp->bond_lambda, xp->gap_frac, xp->weibull_m, xp->sigma_c, xp->tau_c, xp->seed,
-                 xp->post_peak_drop, xp->list_gap};
+    a.x = ext_par(xp);
     a.init(R0, rad);
     int c; double res;
     for (uint64_t k = 0; k < n_pre; ++k) a.fire_increment(*p, &c, &res, nullptr, 0);
@@ -1862,6 +1895,18 @@ void rfo_forces_22_f(const float* R, const float* V, const float* W, const uint6
     rfo::FP<float> p{};
     p.dt = dt; p.m_E = m_E; p.m_G = m_G; p.b_r = b_r; p.m_Gcritn = m_Gcritn; p.m_Gcritt = m_Gcritt;
     rfo::forces_22<float>(R, V, W, IL, ILtype, iL, (v*)Rij, (v*)Oijt, (v*)Mijn, (v*)Mijt, F, M, N, K, p, broke);
+}
+// forces_22 with the break criteria of every bond slot: crit[2k] = Sc (tensile stress
+// plus bending), crit[2k + 1] = Mc (shear plus torsion), as tested against m_Gcritn / m_Gcritt.
+void rfo_forces_22_crit_f(const float* R, const float* V, const float* W, const uint64_t* IL, uint8_t* ILtype,
+                          const float* iL, float* Rij, float* Oijt, float* Mijn, float* Mijt, float* F, float* M,
+                          uint64_t N, uint64_t K, float dt, float m_E, float m_G, float b_r, float m_Gcritn,
+                          float m_Gcritt, uint8_t* broke, float* crit) {
+    typedef rfo::V3<float> v;
+    rfo::FP<float> p{};
+    p.dt = dt; p.m_E = m_E; p.m_G = m_G; p.b_r = b_r; p.m_Gcritn = m_Gcritn; p.m_Gcritt = m_Gcritt;
+    rfo::forces_22<float>(R, V, W, IL, ILtype, iL, (v*)Rij, (v*)Oijt, (v*)Mijn, (v*)Mijt, F, M, N, K, p, broke,
+                          crit);
 }
 void rfo_forces_21_f(const float* R, const float* V, const float* W, const uint64_t* IL, const uint8_t* ILtype,
                      float* Oijt, float* F, float* M, uint64_t N, uint64_t K, float dt, float m_E, float m_G,

@@ -99,6 +99,11 @@ struct Consts {
     // delete test on aa_farcut, as the reference); lgap_d > 0 within min(a_farcut, r_i + r_j + g)
     double a_farcut_d, lgap_d;
     float lgap_f, skin_f;
+    // reference constants in the extended model (rf_ext_params.ref_mode): per-bond stiffness
+    // E/L0, G/L0 from the record's 1/L0, bond radius b_r, the Q1 bending factor, platen
+    // coordinates rounded to float as the reference's drivers pass them
+    int ref_mode;
+    float refE, refG, ref_br;
 };
 
 // Per-specimen geometry of a batch (constant during a run): the platen's cut height, the
@@ -1034,7 +1039,10 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     const bool frozen = MODE == 0 && i < N && S->done != 0;
     const bool valid = i < N && !frozen;
     const uint32_t FULL = 0xffffffffu;
-    const double Top = S->Top, Bottom = S->Bottom, TopR = S->TopR, BottomR = S->BottomR;
+    const double Top = c.ref_mode ? (double)(float)S->Top : S->Top;
+    const double Bottom = c.ref_mode ? (double)(float)S->Bottom : S->Bottom;
+    const double TopR = c.ref_mode ? (double)(float)S->TopR : S->TopR;
+    const double BottomR = c.ref_mode ? (double)(float)S->BottomR : S->BottomR;
     const float vt = MODE == 0 ? (float)S->V : 0.f, RR = S->RR;
     rf_float3 cc;
     cc.x = S->center[0]; cc.y = S->center[1]; cc.z = S->center[2];
@@ -1108,6 +1116,10 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             BondExt b;
             b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ri, (float)xj.w);
             b.sc = str.x; b.tc = str.y; b.L0 = L0;
+            if (MODE == 0 && c.ref_mode) {
+                const float il = __ldg(&d.bil[s]);
+                b.kn = c.refE * il; b.ks = c.refG * il; b.br = c.ref_br;
+            }
             const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
             f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
             f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
@@ -1123,7 +1135,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                                             oijt, mijn, mijt, fsb, msb, fnabs, kt, kr);
             } else {
                 broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(vj), wi, f4to3(wj), rij, oijt, mijn, mijt, fsb,
-                                      msb, fnabs, kt, kr);
+                                      msb, fnabs, kt, kr, c.ref_mode != 0);
             }
             ++npair;
             d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
@@ -1786,6 +1798,8 @@ struct BondSpec {
     double gap_frac, wm, sig, tau;
     uint64_t seed;
     uint32_t p0, p1;            // its particles
+    int ref_mode;               // reference constants: bonds below the centre distance bd, strengths sig, tau
+    double bd;
 };
 // Initial rows of the extended model with a list gap g: the reference's construction
 // (md_interaction_list_construct.cu:13-98: the 8 octant cells in visiting order, their
@@ -1841,10 +1855,16 @@ __global__ void k_bond_ext(const double4* __restrict__ P, const uint_fast32_t* _
             const double4 xj = P[j];
             const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
             const double L = sqrt(dx * dx + dy * dy + dz * dz);
-            if (!(L - xi.w - xj.w < gap_frac * fmin(xi.w, xj.w)) || !(L > 0)) continue;
+            if (bs[sp].ref_mode) {
+                // md_boundinteractions_construct.cu:62 (on the FP64 distance), global strengths
+                if (!(L < bs[sp].bd) || !(L > 0)) continue;
+            } else if (!(L - xi.w - xj.w < gap_frac * fmin(xi.w, xj.w)) || !(L > 0)) {
+                continue;
+            }
             type[r] = 1;
             iL[r] = (float)(1.0 / L);
             L0x[r] = L;
+            if (bs[sp].ref_mode) { strx[r] = make_float2((float)sig, (float)tau); continue; }
             const uint32_t li = i - pbase, lj = (uint32_t)j - pbase;
             const double us = pair_uniform(seed, li, lj, 0), ut = pair_uniform(seed, li, lj, 1);
             strx[r] = make_float2((float)(sig * pow(-log(us), inv_m)), (float)(tau * pow(-log(ut), inv_m)));
@@ -2219,10 +2239,20 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
     double rmax = 0.0, rmin = 1e300;
     if (ext) {
         for (uint64_t i = 0; i < t->N; ++i) { rmax = std::max(rmax, h_rad[i]); rmin = std::min(rmin, h_rad[i]); }
-        if (!(rmin > 0.0) || !(x->kn > 0.0) || !(x->ks >= 0.0) || !(x->bond_lambda > 0.0) || !(x->weibull_m > 0.0) ||
-            !(x->sigma_c > 0.0) || !(x->tau_c > 0.0) || !(x->post_peak_drop >= 0.0 && x->post_peak_drop < 1.0) ||
-            !(x->list_gap >= 0.0 && x->list_gap < 1e300)) {
+        if (x->ref_mode != 0 && x->ref_mode != 1) { set_error("rf_engine_create_ext: ref_mode must be 0 or 1"); return RF_ERR_INVALID; }
+        if (x->ref_mode) {
+            if (rmin != t->Po.p_r || rmax != t->Po.p_r) {
+                set_error("rf_engine_create_ext: ref_mode needs every radius equal to Po.p_r (%g)", t->Po.p_r);
+                return RF_ERR_INVALID;
+            }
+        } else if (!(x->kn > 0.0) || !(x->ks >= 0.0) || !(x->bond_lambda > 0.0) || !(x->weibull_m > 0.0) ||
+                   !(x->sigma_c > 0.0) || !(x->tau_c > 0.0)) {
             set_error("rf_engine_create_ext: radii and bond parameters must be positive");
+            return RF_ERR_INVALID;
+        }
+        if (!(rmin > 0.0) || !(x->post_peak_drop >= 0.0 && x->post_peak_drop < 1.0) ||
+            !(x->list_gap >= 0.0 && x->list_gap < 1e300)) {
+            set_error("rf_engine_create_ext: radii must be positive, post_peak_drop in [0, 1), list_gap >= 0");
             return RF_ERR_INVALID;
         }
         if (!(2.0 * rmax < std::sqrt(t->Po.aa_farcut))) {
@@ -2265,6 +2295,8 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         c.a_farcut_d = P.a_farcut;
         c.lgap_d = x->list_gap;
         c.lgap_f = (float)x->list_gap;
+        c.ref_mode = x->ref_mode;
+        c.refE = (float)P.m_E; c.refG = (float)P.m_G; c.ref_br = (float)P.b_r;
     }
     c.aacut = t->aacut; c.aa_farcut = (float)P.aa_farcut;
     c.g.a = t->C.a; c.g.inv_a = t->C._1d_a; c.g.nx = t->C.Nr.x; c.g.ny = t->C.Nr.y; c.g.nz = t->C.Nr.z; c.g.CN = t->C.N;
@@ -2454,8 +2486,10 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
             std::vector<BondSpec> hbs(nspec);
             for (uint32_t q = 0; q < nspec; ++q) {
                 const rf_ext_params& xq = bin ? bin->xs[q] : *x;
+                const rf_task& tq = bin ? bin->tasks[q] : *t;
                 hbs[q] = BondSpec{xq.gap_frac, xq.weibull_m, xq.sigma_c, xq.tau_c, xq.seed, bin ? bin->p0[q] : 0u,
-                                  bin ? bin->p0[q] + bin->n[q] : N};
+                                  bin ? bin->p0[q] + bin->n[q] : N, xq.ref_mode, tq.Po.b_d};
+                if (xq.ref_mode) { hbs[q].sig = tq.Po.m_Ec; hbs[q].tau = tq.Po.m_Gc; hbs[q].wm = 1.0; }
             }
             BondSpec* dbs = nullptr;
             ce = cudaMalloc(&dbs, nspec * sizeof(BondSpec));
@@ -2561,6 +2595,8 @@ rf_status rf_engine_create_batch(const rf_task* tasks, const rf_ext_params* xs, 
             tq.Po.p_A != t0.Po.p_A || tq.Po.p_mu != t0.Po.p_mu || tq.Po.p_mur != t0.Po.p_mur ||
             tq.Po.p_m != t0.Po.p_m || xs[q].kn != xs[0].kn || xs[q].ks != xs[0].ks ||
             xs[q].bond_lambda != xs[0].bond_lambda || xs[q].list_gap != xs[0].list_gap ||
+            xs[q].ref_mode != xs[0].ref_mode ||
+            (xs[0].ref_mode && (tq.Po.m_E != t0.Po.m_E || tq.Po.m_G != t0.Po.m_G || tq.Po.b_r != t0.Po.b_r)) ||
             !(xs[q].post_peak_drop >= 0.0 && xs[q].post_peak_drop < 1.0)) {
             set_error("rf_engine_create_batch: specimen %d must have >= 128 particles and the batch's test kind, "
                       "slots, grid cell, material, time step, bond stiffness and list gap, and a post-peak drop in [0, 1)", q);
@@ -2693,6 +2729,7 @@ rf_status load_increment(rf_engine* e, const rf_relax_params* p, const float* wa
     if (!e || !p) { set_error("rf_engine_load_increment: bad arguments"); return RF_ERR_INVALID; }
     if (!e->c.ext) { set_error("rf_engine_load_increment: quasi-static relaxation needs the extended model"); return RF_ERR_STATE; }
     if (e->d.nspec > 1) { set_error("rf_engine_load_increment: quasi-static relaxation runs one specimen per engine"); return RF_ERR_STATE; }
+    if (e->c.ref_mode) { set_error("rf_engine_load_increment: the reference-constants mode runs explicit steps only"); return RF_ERR_STATE; }
     if (!(p->dt0 > 0) || !(p->dt_max >= p->dt0) || !(p->dt_min > 0) || !(p->dt_min <= p->dt0) || !(p->tol > 0) ||
         p->max_iter == 0 || !(p->alpha0 >= 0 && p->alpha0 < 1) || !(p->f_inc >= 1) || !(p->f_dec > 0 && p->f_dec < 1)) {
         set_error("rf_engine_load_increment: bad FIRE parameters");

@@ -348,10 +348,12 @@ struct ExtParams {
 
 // One bond slot of the extended model (same structure and order as bond_slot).
 // rlen = |r| in double; r is the float rounding of the double separation.
+// q1: sum the bending moment with the reference's extra dt*E/(4 L0) factor (its Q1,
+// md_calculateforcesdem3.cu:131-152), as the reference-constants mode does.
 __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt& b, const f3 r, const double rlen,
                                               const f3 vi, const f3 vj, const f3 wi, const f3 wj, f3& Rij, f3& Oijt,
                                               f3& Mijn, f3& Mijt, f3& fs, f3& ms, float& fnabs, float& kt,
-                                              float& kr) {
+                                              float& kr, const bool q1 = false) {
     const float rijm = (float)rlen;
     const float inv_rm = __frcp_rn(rijm);
     const float nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
@@ -402,8 +404,13 @@ __device__ __forceinline__ bool bond_slot_ext(const ExtParams& p, const BondExt&
         const float mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
         Mijt = mk3(mx, my, mz);
         // bending moment kn * (pi br^4 / 4) * angle = Mijt * J; the reference's extra
-        // factor dt*E/(4 L0) here (its Q1) is not carried into this model
-        ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+        // factor dt*E/(4 L0) here (its Q1) is carried only in the reference-constants mode
+        if (q1) {
+            const float q = c2 * J;
+            ms.x += mx * q; ms.y += my * q; ms.z += mz * q;
+        } else {
+            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+        }
     }
     float Mc;
     {

@@ -106,7 +106,8 @@ class ExtParams(C.Structure):
     """rf_ext_params: bond constants and strength distribution of the extended model."""
     _fields_ = [("kn", C.c_double), ("ks", C.c_double), ("bond_lambda", C.c_double), ("gap_frac", C.c_double),
                 ("weibull_m", C.c_double), ("sigma_c", C.c_double), ("tau_c", C.c_double), ("seed", C.c_uint64),
-                ("post_peak_drop", C.c_double), ("list_gap", C.c_double)]
+                ("post_peak_drop", C.c_double), ("list_gap", C.c_double), ("ref_mode", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class RelaxParams(C.Structure):

@@ -8,6 +8,7 @@ import os
 import numpy as np
 import pytest
 
+import extspec
 import mdcall as mc
 import oracle
 import rfdem
@@ -29,13 +30,18 @@ def assert_state_equal(e, o, keys=KEYS):
                                                                                  b[bad[:5]]))
 
 
-CASES = [(rfdem.RF_TEST_UNIAXIAL, 9.0, 14.0, 400), (rfdem.RF_TEST_BRAZIL, 16.0, 6.0, 400),
-         (rfdem.RF_TEST_UNIAXIAL, 20.0, 30.0, 60)]
+# (kind, diameter, height, steps, platen speed factor, window must show damage). The two
+# damage windows break bonds, load contacts and change rows (asserted); the uniaxial one
+# drives its platen at 5x the reference's speed so that damage starts within 3000 steps.
+# The 10k-particle case checks the multi-CTA paths at a larger size over a short window.
+CASES = [(rfdem.RF_TEST_UNIAXIAL, 9.0, 14.0, 3000, 5.0, True), (rfdem.RF_TEST_BRAZIL, 16.0, 6.0, 3000, 1.0, True),
+         (rfdem.RF_TEST_UNIAXIAL, 20.0, 30.0, 60, 1.0, False)]
 
 
-@pytest.mark.parametrize("kind,d,h,steps", CASES, ids=["uniaxial", "brazil", "uniaxial-10k"])
-def test_engine_run_bitexact_vs_oracle(cuda, kind, d, h, steps):
-    t, R = rfdem.make_test(kind, d, h, seed=0xB2000000 + 21)
+@pytest.mark.parametrize("kind,d,h,steps,vf,damage", CASES, ids=["uniaxial", "brazil", "uniaxial-10k"])
+def test_engine_run_bitexact_vs_oracle(cuda, kind, d, h, steps, vf, damage):
+    v = (-10.0 if kind == rfdem.RF_TEST_UNIAXIAL else -100.0) * 0.02 / 1e3 * vf
+    t, R = rfdem.make_test(kind, d, h, seed=0xB2000000 + 21, v_load=v, max_strain=1.0)
     to = mc.clone(t)
     n, ost, curve_o, status = oracle.run_f(to, R, steps)
     assert status == 0
@@ -55,6 +61,14 @@ def test_engine_run_bitexact_vs_oracle(cuda, kind, d, h, steps):
     c = e.counters()
     assert c["bonds"] > 2 * t.N and c["steps"] == n
     e.close()
+    if damage:
+        N, K = int(t.N), int(t.K)
+        _, st0, _, _ = oracle.run_f(mc.clone(t), R, 0)
+        _, contacts = extspec.pair_counts(ost["R"], N, K, ost["IL"], ost["ILtype"], np.full(N, t.Po.p_r))
+        broken, changed = int(ost["broke"].sum()), int((ost["IL"] != st0["IL"]).sum())
+        print("%d steps: bonds broken %d, overlapping contact slots %d, row slots changed %d" %
+              (steps, broken, contacts, changed))
+        assert res.broken_bonds == broken > 0 and contacts > 0 and changed > 0
 
 
 def test_graph_and_stream_paths_agree(cuda):

@@ -24,10 +24,24 @@ def run_engine_ext(t, x, R, rad, steps, no_graph=False, monkeypatch=None):
     return res, st
 
 
-@pytest.mark.parametrize("kind,d,h,steps", [(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, 300),
-                                            (rfdem.RF_TEST_BRAZIL, 10.0, 4.0, 300)], ids=["uniaxial", "brazil"])
-def test_ext_engine_bitexact_vs_oracle(cuda, kind, d, h, steps):
-    t, R, rad, x = extspec.ext_case(kind, d, h, min_stress=1e3)
+def assert_damage(t, x, R, rad, o, res):
+    """The window broke bonds, loaded contacts and changed rows (so the break, contact
+    and list paths were compared, not only intact bonds)."""
+    N, K = int(t.N), int(t.K)
+    start = oracle.run_ext(mc.clone(t), x, R, rad, 0)
+    _, contacts = extspec.pair_counts(o["R"], N, K, o["IL"], o["ILtype"], rad)
+    changed = int((start["IL"] != o["IL"]).sum())
+    print("bonds broken %d, overlapping contact slots %d, row slots changed %d" % (o["broken"], contacts, changed))
+    assert res.broken_bonds == o["broken"] > 0 and contacts > 0 and changed > 0
+
+
+# The uniaxial window drives its platen at 5x the reference's speed so that damage starts
+# within 2000 steps.
+@pytest.mark.parametrize("kind,d,h,steps,vf", [(rfdem.RF_TEST_UNIAXIAL, 6.0, 10.0, 2000, 5.0),
+                                               (rfdem.RF_TEST_BRAZIL, 10.0, 4.0, 2000, 1.0)], ids=["uniaxial", "brazil"])
+def test_ext_engine_bitexact_vs_oracle(cuda, kind, d, h, steps, vf):
+    v = (-10.0 if kind == rfdem.RF_TEST_UNIAXIAL else -100.0) * 0.02 / 1e3 * vf
+    t, R, rad, x = extspec.ext_case(kind, d, h, min_stress=1e3, v_load=v, max_strain=1.0)
     o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
     res, st = run_engine_ext(t, x, R, rad, steps)
     assert res.steps == o["steps"] == steps
@@ -37,6 +51,7 @@ def test_ext_engine_bitexact_vs_oracle(cuda, kind, d, h, steps):
     assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
     assert np.array_equal(st["ILtype"], o["ILtype"])
     assert res.broken_bonds == o["broken"]
+    assert_damage(t, x, R, rad, o, res)
 
 
 def test_ext_engine_stream_equals_graph(cuda, monkeypatch):
@@ -141,13 +156,13 @@ def test_ext_log_uniform_radius_ratio_3_vs_oracle(cuda, gap):
 def test_ext_list_gap_lattice_vs_oracle(cuda):
     """A list gap on the lattice specimen (both test kinds' code paths share it): engine ==
     float oracle bit for bit over steps that break bonds and form contacts."""
-    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_BRAZIL, 10.0, 4.0, min_stress=1e3)
+    t, R, rad, x = extspec.ext_case(rfdem.RF_TEST_BRAZIL, 10.0, 4.0, min_stress=1e3, max_strain=1.0)
     x.list_gap = 0.1
-    steps = 300
+    steps = 2000
     o = oracle.run_ext(mc.clone(t), x, R, rad, steps)
     res, st = run_engine_ext(t, x, R, rad, steps)
     assert res.steps == o["steps"] == steps and res.error == 0 and o["status"] == 0
     assert np.array_equal(st["R64"], o["R"])
     assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
     assert np.array_equal(st["ILtype"], o["ILtype"])
-    assert res.broken_bonds == o["broken"]
+    assert_damage(t, x, R, rad, o, res)

@@ -2,6 +2,7 @@
 import numpy as np
 import pytest
 
+import extspec
 import mdcall as mc
 import oracle
 import rfdem
@@ -148,3 +149,24 @@ def test_forces_bitexact_on_evolved_state(cuda, case):
     for k in ["F", "M", "ty", "Rij", "Oijt", "Mijn", "Mijt"]:
         assert np.array_equal(g[k].view(np.uint8), o[k].view(np.uint8)), k
     assert np.abs(o["F"]).max() > 0
+
+
+def test_forces_bitexact_on_damaged_state(cuda):
+    """_22 then _21 on a state with broken bonds and loaded contacts (a 585-particle
+    cylinder after 3000 steps at 5x the reference's platen speed): forces, moments, slot
+    state and break flags bit for bit, and the state holds what the claim needs."""
+    t, R = rfdem.make_test(rfdem.RF_TEST_UNIAXIAL, 9.0, 14.0, seed=0xB2000000 + 21, max_strain=1.0,
+                           v_load=-10.0 * 0.02 / 1e3 * 5.0)
+    N, K = R.size // 3, int(t.K)
+    _, st = mc.oracle_state_after(t, R, 3000)
+    S = {k: st[k] for k in ["Rij", "Oijt", "Mijn", "Mijt"]}
+    g = mc.gpu_forces(cuda, t, st["R"], st["V"], st["W"], st["IL"], st["ILtype"], st["iL"], S)
+    o = mc.oracle_forces(t, st["R"], st["V"], st["W"], st["IL"], st["ILtype"], st["iL"], S)
+    for k in ["F", "M", "ty", "Rij", "Oijt", "Mijn", "Mijt"]:
+        assert np.array_equal(g[k].view(np.uint8), o[k].view(np.uint8)), k
+    _, contacts = extspec.pair_counts(st["R"], N, K, st["IL"], st["ILtype"], np.full(N, t.Po.p_r))
+    oz = np.abs(o["Oijt"].reshape(-1, 3)).sum(1) > 0
+    loaded = int((oz & (st["ILtype"] == 0) & (st["IL"] != rfdem.EMPTY)).sum())
+    print("broken bonds %d, overlapping contacts %d, contact slots with tangential overlap %d" %
+          (int(st["broke"].sum()), contacts, loaded))
+    assert int(st["broke"].sum()) > 0 and contacts > 0 and loaded > 0

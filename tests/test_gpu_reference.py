@@ -101,6 +101,87 @@ def test_bond_construction_vs_reference(cuda, case):
     assert np.array_equal(iL_r.view(np.uint32), iLo.view(np.uint32))
 
 
+def oracle_criteria(t, st, V, W, S):
+    """The oracle's break criteria (Sc, Mc) of every bond slot on a state, [N*K, 2]."""
+    L = oracle.load()
+    N, K = st["R"].size // 3, int(t.K)
+    S = {k: v.copy() for k, v in S.items()}
+    ty = st["ILtype"].copy()
+    F, M = np.zeros(3 * N, np.float32), np.zeros(3 * N, np.float32)
+    crit = np.zeros(2 * N * K, np.float32)
+    big = [float(np.float32(3e38))] * 2           # strengths nothing reaches: every criterion is evaluated
+    L.rfo_forces_22_crit_f(st["R"].ctypes.data, V.ctypes.data, W.ctypes.data, st["IL"].ctypes.data, ty.ctypes.data,
+                           st["iL"].ctypes.data, S["Rij"].ctypes.data, S["Oijt"].ctypes.data, S["Mijn"].ctypes.data,
+                           S["Mijt"].ctypes.data, F.ctypes.data, M.ctypes.data, N, K, *mc.bond_params(t)[:4], *big,
+                           None, crit.ctypes.data)
+    return crit.reshape(-1, 2)
+
+
+def threshold_eps(t, il):
+    """Stated epsilon of the tensile break test for a bond of 1/L0 = il: the criterion's
+    stress E*(|r| - L0)/L0 moves by E*il*ulp(|r|) for one ulp of |r| (the reference's
+    norm3df and FMA-contracted sums against the correctly rounded sqrt here), so four such
+    ulps; near_threshold adds 1e-5 of the criterion for its moment terms."""
+    P = t.Po
+    L0 = np.float32(1.0) / np.float32(il)
+    return 4.0 * P.m_E * float(il) * float(np.spacing(L0))
+
+
+def near_threshold(t, st, crit, k, sig_c, tau_c):
+    """Slot k's tensile criterion within threshold_eps + 1e-5 of itself + 4 ulp of sig_c of
+    sig_c, or its shear criterion within 1e-5 of itself + 4 ulp of tau_c of tau_c."""
+    Sc, Mc = float(crit[k, 0]), float(crit[k, 1])
+    eS = threshold_eps(t, st["iL"][k]) + 1e-5 * abs(Sc) + 4 * float(np.spacing(np.float32(sig_c)))
+    eM = 1e-5 * abs(Mc) + 4 * float(np.spacing(np.float32(tau_c)))
+    return abs(Sc - sig_c) <= eS or abs(Mc - tau_c) <= eM
+
+
+@needs_ref
+def test_break_decisions_vs_reference_near_threshold_only(cuda):
+    """Break decisions of d_CalculateForcesDEM_22 on a loaded state (a 585-particle
+    cylinder after 20,000 steps), with the strengths set to the median tensile and the
+    90th-percentile shear criterion of its bonds, so that one step decides hundreds of
+    breaks and several bonds sit near a threshold. The reference's own kernel, the oracle
+    and the engine's md_ kernel decide; the engine equals the oracle bit for bit, and every
+    decision where the reference differs is a bond listed as near the threshold (its
+    criterion within the stated epsilon of the strength)."""
+    t, R = rfdem.make_test(0, 9.0, 14.0, seed=0xB2000000 + 55, max_strain=1.0)
+    N, K = R.size // 3, int(t.K)
+    _, st = mc.oracle_state_after(t, R, 20000)
+    S = {k: st[k].copy() for k in ["Rij", "Oijt", "Mijn", "Mijt"]}
+    crit = oracle_criteria(t, st, st["V"], st["W"], S)
+    bond = np.nonzero(st["ILtype"] == 1)[0]
+    sig_c = float(np.float32(np.quantile(crit[bond, 0], 0.5)))
+    tau_c = float(np.float32(np.quantile(crit[bond, 1], 0.9)))
+    tq = mc.clone(t)
+    tq.Po.m_Ec, tq.Po.m_Gc = sig_c, tau_c
+    o = mc.oracle_forces(tq, st["R"], st["V"], st["W"], st["IL"], st["ILtype"], st["iL"], S)
+    g = mc.gpu_forces(cuda, tq, st["R"], st["V"], st["W"], st["IL"], st["ILtype"], st["iL"], S)
+    assert np.array_equal(g["ty"], o["ty"])
+    assert np.array_equal(g["F"].view(np.uint32), o["F"].view(np.uint32))
+    ref = {k: v.copy() for k, v in S.items()}
+    ty_r = st["ILtype"].copy()
+    F, M = np.zeros(3 * N, np.float32), np.zeros(3 * N, np.float32)
+    p22 = np.array(mc.bond_params(tq), np.float32)
+    p21 = np.array(mc.contact_params(tq), np.float32)
+    IL32 = to32(st["IL"])
+    assert REF.ref_forces(st["R"].ctypes.data, st["V"].ctypes.data, st["W"].ctypes.data, N, K, IL32.ctypes.data,
+                          ty_r.ctypes.data, st["iL"].ctypes.data, ref["Rij"].ctypes.data, ref["Oijt"].ctypes.data,
+                          ref["Mijn"].ctypes.data, ref["Mijt"].ctypes.data, F.ctypes.data, M.ctypes.data,
+                          p22.ctypes.data, p21.ctypes.data, 1) == 0
+    broke_o = bond[o["ty"][bond] == 0]
+    broke_r = bond[ty_r[bond] == 0]
+    listed = [int(k) for k in bond if near_threshold(tq, st, crit, k, sig_c, tau_c)]
+    flips = np.nonzero(ty_r != o["ty"])[0]
+    print("bond slots %d; breaks: oracle/engine %d, reference %d; near-threshold bonds listed separately %d; "
+          "decisions that differ %d" % (bond.size, broke_o.size, broke_r.size, len(listed), flips.size))
+    print("near-threshold list (slot, Sc - sig_c, Mc - tau_c):",
+          [(k, float(crit[k, 0]) - sig_c, float(crit[k, 1]) - tau_c) for k in listed[:20]])
+    assert broke_o.size > 100 and len(listed) > 0
+    off_list = [int(k) for k in flips if k not in set(listed)]
+    assert not off_list, [(k, float(crit[k, 0]) - sig_c, float(crit[k, 1]) - tau_c) for k in off_list[:10]]
+
+
 def _force_scale(F):
     n = F.size // 3
     return np.sqrt(F[:n] ** 2 + F[n:2 * n] ** 2 + F[2 * n:] ** 2).max()
@@ -127,9 +208,11 @@ def test_forces_vs_reference_within_tolerance(cuda, case):
                           ty_r.ctypes.data, st["iL"].ctypes.data, ref["Rij"].ctypes.data, ref["Oijt"].ctypes.data,
                           ref["Mijn"].ctypes.data, ref["Mijt"].ctypes.data, F.ctypes.data, M.ctypes.data,
                           p22.ctypes.data, p21.ctypes.data, 3) == 0
-    # break decisions: identical except for bonds whose criterion sits within 4 ulp of the strength
+    # break decisions: identical except for bonds whose criterion sits within the stated
+    # epsilon of the strength (near_threshold; none of these bonds is close to breaking)
     flips = np.nonzero(ty_r != o["ty"])[0]
-    assert flips.size <= max(2, N * K // 100000), flips
+    crit = oracle_criteria(t, st, V, W, S)
+    assert flips.size == 0 or all(near_threshold(t, st, crit, k, *mc.bond_params(t)[4:6]) for k in flips), flips
     # The bond normal force E*A*(|r| - L0)/L0 cancels |r| against L0 ~ 1 mm, so one ulp of
     # |r| (library norm3df in the reference, sqrt of the float sum here) moves it by
     # E*A*(1/L0)*ulp(|r|). Tolerance: 4 such ulps per particle; moments 4 ulps of the
@@ -196,7 +279,8 @@ def test_whole_run_vs_reference(cuda, kind, d, h, steps):
     print("pairs: reference %d engine %d, threshold pairs listed separately %d, other differences %d, "
           "bond-flag flips %d" % (len(pr), len(pe), len(set(pr) ^ set(pe)) - len(only), len(only), len(flips)))
     assert not only, only[:10]
-    assert len(flips) <= 2, flips
+    # no bond of this window comes near its strength: every bond flag must match
+    assert not flips, flips
     ext = np.ptp(R)
     np.testing.assert_allclose(out["R"], eg["R"], rtol=0, atol=1e-5 * ext)
     to = mc.clone(t)

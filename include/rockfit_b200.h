@@ -459,6 +459,17 @@ rf_status rf_engine_load_increment_pred(rf_engine* e, const rf_relax_params* p, 
                                         rf_relax_result* r);
 rf_status rf_engine_destroy(rf_engine* e);
 
+/*
+ * Homogeneous strain of the specimen (no reference counterpart; the bench and tests use it
+ * to start a run in a loaded, damaged state): every particle position x becomes
+ * c + (1 + strain[a]) (x - c) along each axis a about the platen box's centre c, the
+ * load axis's platens move with it (Strain is updated), and the platen zone's radius
+ * grows with the larger lateral strain. Rest lengths, slot state and velocities are kept,
+ * so from the next step on the bonds and contacts carry the strain (bonds stretched past
+ * their strength break on that step). Each component in (-0.5, 0.5); one specimen only.
+ */
+rf_status rf_engine_affine_strain(rf_engine* e, const double strain[3]);
+
 /* Advance nsteps explicit steps (stops early, on device, at fracture / max strain). */
 rf_status rf_engine_step(rf_engine* e, uint64_t nsteps);
 /* Same, with positions uploaded from host first and results read back after:

@@ -70,6 +70,7 @@ def _declare(L):
         "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
         "rfo_run_ext_pos_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P, i32]),
         "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
+        "rfo_run_ext_strained_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, P, u64, P, P, P, P, u64, P, P, P]),
     }
     for n, (r, a) in proto.items():
         f = getattr(L, n)
@@ -115,9 +116,10 @@ def run_d(task, R0, max_steps):
     return int(steps), R, curve[:3 * min(ns.value, cap)].reshape(-1, 3), ty, status.value
 
 
-def run_ext(task, x, R0, radius, max_steps, fp64=False, positions="f64"):
+def run_ext(task, x, R0, radius, max_steps, fp64=False, positions="f64", strain=None):
     """Extended model run (float forces as the engine computes them, or the FP64 oracle;
-    positions "hilo" / "f32": float forces with positions kept as hi/lo float pairs / floats).
+    positions "hilo" / "f32": float forces with positions kept as hi/lo float pairs / floats;
+    strain (float forces only): rf_engine_affine_strain applied to the built specimen first).
     Returns dict(steps, R (double planar, after the pending delete pass), V, IL, ILtype,
     curve, status, broken)."""
     L = load()
@@ -132,7 +134,10 @@ def run_ext(task, x, R0, radius, max_steps, fp64=False, positions="f64"):
     ns, status, broken = C.c_uint64(0), C.c_int(0), C.c_uint64(0)
     args = [C.byref(task), C.byref(x), p(R), p(rad), max_steps, p(V), p(IL), p(ty), p(curve), cap, C.byref(ns),
             C.byref(status), C.byref(broken)]
-    if positions != "f64" and not fp64:
+    if strain is not None:
+        sv = (C.c_double * 3)(*strain)
+        steps = L.rfo_run_ext_strained_f(*(args[:4] + [sv] + args[4:]))
+    elif positions != "f64" and not fp64:
         steps = L.rfo_run_ext_pos_f(*args, {"hilo": 1, "f32": 2}[positions])
     else:
         steps = (L.rfo_run_ext_d if fp64 else L.rfo_run_ext_f)(*args)

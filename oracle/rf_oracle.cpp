@@ -1044,7 +1044,11 @@ struct RunExt {
                 const id_t j = IL[k];
                 if (j == EMPTY || j >= N) continue;
                 const double d2 = rr(i, j);
-                if (d2 > cut2_del(i, j) || d2 < 1e-10) { IL[k] = EMPTY; type[k] = 0; zero_slot(k); }
+                // an intact bond of the extended model is kept up to 1.45 L0 (the
+                // reference's a_farcut / 2 p_r); the reference constants keep its rule
+                double cut = cut2_del(i, j);
+                if (type[k] == 1 && !x.ref) { const double q = 1.45 * L0[k]; cut = q * q; }
+                if (d2 > cut || d2 < 1e-10) { IL[k] = EMPTY; type[k] = 0; zero_slot(k); }
             }
     }
 
@@ -1326,6 +1330,32 @@ struct RunExt {
     }
 
     bool running() const { return t->Compress.Strain < t->Compress.MaxStrain && !t->Compress.Fracture; }
+
+    // rf_engine_affine_strain: positions scaled by 1 + e per axis about the platen box's
+    // centre, the load axis's platens with them, the platen zone by the larger lateral strain.
+    void affine(double ex, double ey, double ez) {
+        rf_compression& Kc = t->Compress;
+        const double cx = Kc.center_d.x, cy = Kc.center_d.y, cz = Kc.center_d.z;
+        for (uint64_t i = 0; i < N; ++i) {
+            R[i] = cx + (1.0 + ex) * (R[i] - cx);
+            R[i + N] = cy + (1.0 + ey) * (R[i + N] - cy);
+            R[i + 2 * N] = cz + (1.0 + ez) * (R[i + 2 * N] - cz);
+        }
+        const bool brz = t->kind == RF_TEST_BRAZIL;
+        const double e = brz ? ey : ez, el = brz ? std::fmax(ex, ez) : std::fmax(ex, ey);
+        const double ca = brz ? Kc.center_d.y : Kc.center_d.z;
+        const double dtr = Kc.TopR - Kc.Top, dbr = Kc.BottomR - Kc.Bottom;
+        Kc.Top = ca + (1.0 + e) * (Kc.Top - ca);
+        Kc.Bottom = ca + (1.0 + e) * (Kc.Bottom - ca);
+        Kc.TopR = Kc.Top + dtr;
+        Kc.BottomR = Kc.Bottom + dbr;
+        double* sz = brz ? &Kc.size_d.y : &Kc.size_d.z;
+        *sz *= 1.0 + e;
+        if (brz) { Kc.size.y = (float)*sz; Kc.sized2.y = (float)(0.5 * *sz); Kc.Hd2 = Kc.sized2.y; }
+        else { Kc.size.z = (float)*sz; Kc.sized2.z = (float)(0.5 * *sz); Kc.Hd2 = Kc.sized2.z; }
+        Kc.Strain = (*sz - Kc.Size0) / Kc.Size0;
+        Kc.RR = (float)((double)Kc.RR * (1.0 + el) * (1.0 + el));
+    }
 
     // Forces and moments of every particle (the _22 then _21 slot orders), and the sums
     // of |normal pair force| and of the pair count over bonds and overlapping contacts.
@@ -1658,12 +1688,14 @@ struct RunExt {
 template <class TF>
 static uint64_t run_ext(rf_task* t, const rf_ext_params* xp, double* R_io, const double* rad, uint64_t max_steps,
                         TF* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,
-                        uint64_t* nsaved, int* status, uint64_t* broken, int pos_mode = 0) {
+                        uint64_t* nsaved, int* status, uint64_t* broken, int pos_mode = 0,
+                        const double* strain = nullptr) {
     RunExt<TF> r;
     r.pos_mode = pos_mode;
     r.t = t;
     r.x = ext_par(xp);
     r.init(R_io, rad);
+    if (strain) r.affine(strain[0], strain[1], strain[2]);
     uint64_t ns = 0;
     while (r.running() && r.steps < max_steps) r.step(curve, cap, &ns);   // max_steps 0: bonds only
     r.delete_far();                         // the pending DeleteFarLinks of the last step
@@ -1793,6 +1825,14 @@ uint64_t rfo_run_ext_pos_f(rf_task* t, const rf_ext_params* x, double* R_io, con
                            uint64_t* nsaved, int* status, uint64_t* broken, int pos_mode) {
     return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
                                broken, pos_mode);
+}
+// rfo_run_ext_f after rf_engine_affine_strain(strain) applied to the built specimen.
+uint64_t rfo_run_ext_strained_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad,
+                                const double* strain, uint64_t max_steps, float* V_out, uint64_t* IL_out,
+                                uint8_t* type_out, double* curve, uint64_t cap, uint64_t* nsaved, int* status,
+                                uint64_t* broken) {
+    return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
+                               broken, 0, strain);
 }
 uint64_t rfo_run_ext_d(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad, uint64_t max_steps,
                        double* V_out, uint64_t* IL_out, uint8_t* type_out, double* curve, uint64_t cap,

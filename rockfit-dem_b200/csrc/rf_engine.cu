@@ -792,6 +792,29 @@ __device__ __forceinline__ double cut2_del(const Consts& c, double ri, double rj
     return c.aa_farcut_d;
 }
 
+// The reference removes a listed pair beyond a_farcut = 2.9 p_r, 1.45 times the contact
+// distance 2 p_r of its mono-sized particles, intact bonds included
+// (md_interaction_list_reconstructbpm.cu:141-186). With a list gap, or radii that span a
+// range, a pair cutoff can lie within a bond's failure stretch (a bond of two r_max
+// particles sits just inside a_farcut = 2.02 r_max), so list maintenance would remove
+// intact bonds that their strengths still hold. In the extended model an intact bond is
+// therefore removed by distance only beyond the same relative margin of its own rest
+// length, |r| > 1.45 L0; the reference-constants mode keeps the reference's rule.
+#define RF_BOND_KEEP_RATIO 1.45
+__device__ __forceinline__ double bond_cut2_del(const Consts& c, double ri, double rj, double L0) {
+    if (c.ref_mode) return cut2_del(c, ri, rj);
+    const double q = RF_BOND_KEEP_RATIO * L0;
+    return q * q;
+}
+// Rest length of the intact bond in slot k of particle i (its record's).
+__device__ __forceinline__ double slot_rest_length(const Dev& d, const Consts& c, uint32_t i, uint32_t k, uint32_t nbq) {
+    for (uint32_t q = 0; q < nbq; ++q) {
+        const size_t s = (size_t)q * c.N + i;
+        if (d.bk[s] == (uint8_t)k) return d.bL0[s];
+    }
+    return 0.0;
+}
+
 __device__ __forceinline__ void delete_far_ext(const Dev& d, const Consts& c, const double4* __restrict__ P,
                                                uint32_t i, const double4 xi, uint32_t ncand, uint32_t nbq,
                                                uint32_t& live, uint32_t& bond, uint32_t& cm, uint32_t& bmask,
@@ -804,7 +827,9 @@ __device__ __forceinline__ void delete_far_ext(const Dev& d, const Consts& c, co
         const uint32_t j = row[k];
         const double4 xj = ldg_d4(&P[j]);
         const double rr = dlen2(dsub(xj, xi));
-        if (rr > cut2_del(c, xi.w, xj.w) || rr < 1e-10)
+        const double cut = ((bond >> k) & 1u) ? bond_cut2_del(c, xi.w, xj.w, slot_rest_length(d, c, i, k, nbq))
+                                              : cut2_del(c, xi.w, xj.w);
+        if (rr > cut || rr < 1e-10)
             delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
     }
 }
@@ -1109,7 +1134,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             const float4 vj = __ldg(&Vv[j]), wj = __ldg(&Wv[j]);
             const double3 rd = dsub(xj, xi);
             const double rr = dlen2(rd);
-            if (rr > cut2_del(c, xi.w, xj.w) || rr < 1e-10) {
+            if (rr > bond_cut2_del(c, xi.w, xj.w, L0) || rr < 1e-10) {
                 delete_slot(d, c, i, d.bk[s], j, ncand, nbq, live, bond, cm, bmask, mem);
                 continue;
             }
@@ -1904,6 +1929,50 @@ __global__ void k_counters(Dev d, Consts c, unsigned long long* out) {
 
 __global__ void k_set_target(DevScalars* sc, unsigned long long n) { sc->target = sc->steps + n; }
 __global__ void k_force_rebuild(DevScalars* sc) { sc->rebuild = 1u; }
+
+// Homogeneous strain of the specimen about the platen box's centre: every position (and
+// the load axis's platens with them) scaled by 1 + eps per axis; the platen zone's radius
+// grows with the larger lateral strain. Rest lengths, slot state and velocities stay, so
+// the bonds and contacts carry the strain from the next step on.
+__global__ void k_affine_positions(Dev d, Consts c, double ex, double ey, double ez) {
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
+    const double cx = d.sc->center_d[0], cy = d.sc->center_d[1], cz = d.sc->center_d[2];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        if (c.ext) {
+            double4 x = d.posd[cur][i];
+            x.x = cx + (1.0 + ex) * (x.x - cx); x.y = cy + (1.0 + ey) * (x.y - cy); x.z = cz + (1.0 + ez) * (x.z - cz);
+            d.posd[cur][i] = x;
+        } else {
+            float4 x = d.pos[cur][i];
+            x.x = (float)(cx + (1.0 + ex) * ((double)x.x - cx));
+            x.y = (float)(cy + (1.0 + ey) * ((double)x.y - cy));
+            x.z = (float)(cz + (1.0 + ez) * ((double)x.z - cz));
+            d.pos[cur][i] = x;
+        }
+    }
+}
+template <int KIND>
+__global__ void k_affine_scalars(Dev d, Consts c, double ex, double ey, double ez) {
+    DevScalars* sc = d.sc;
+    if (blockIdx.x || threadIdx.x) return;
+    const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+    const double e = ax == 1 ? ey : ez, el = ax == 1 ? fmax(ex, ez) : fmax(ex, ey);
+    const double ca = sc->center_d[ax];
+    const double dtr = sc->TopR - sc->Top, dbr = sc->BottomR - sc->Bottom;
+    sc->Top = ca + (1.0 + e) * (sc->Top - ca);
+    sc->Bottom = ca + (1.0 + e) * (sc->Bottom - ca);
+    sc->TopR = sc->Top + dtr;
+    sc->BottomR = sc->Bottom + dbr;
+    sc->size_d[ax] *= 1.0 + e;
+    sc->size[ax] = (float)sc->size_d[ax];
+    sc->sized2[ax] = (float)(0.5 * sc->size_d[ax]);
+    sc->Hd2 = sc->sized2[ax];
+    sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
+    sc->RR = (float)((double)sc->RR * (1.0 + el) * (1.0 + el));
+    sc->dmax = 3.0e38f;          // positions jumped: the next add pass scans
+    sc->d2max_next = 0;
+    sc->rebuild = 1;             // and the candidate lists are rebuilt first
+}
 __global__ void k_planar_to_cur(const float* __restrict__ R, Dev d) {
     const uint32_t N = (uint32_t)(d.n_particles);
     if (d.posd[0]) {                      // extended model: keep the radius
@@ -2942,6 +3011,24 @@ rf_status rf_engine_step(rf_engine* e, uint64_t nsteps) {
         return RF_OK;
     }
     return launch_stream_steps(e, nsteps);
+}
+
+rf_status rf_engine_affine_strain(rf_engine* e, const double strain[3]) {
+    if (!e || !strain) { set_error("rf_engine_affine_strain: bad arguments"); return RF_ERR_INVALID; }
+    if (e->d.nspec > 1) { set_error("rf_engine_affine_strain: one specimen per engine"); return RF_ERR_STATE; }
+    for (int a = 0; a < 3; ++a)
+        if (!(strain[a] > -0.5 && strain[a] < 0.5)) {
+            set_error("rf_engine_affine_strain: strain components must lie in (-0.5, 0.5)");
+            return RF_ERR_INVALID;
+        }
+    cudaStream_t s = e->stream;
+    const uint32_t N = e->c.N;
+    k_affine_positions<<<(N + 255) / 256, 256, 0, s>>>(e->d, e->c, strain[0], strain[1], strain[2]);
+    RF_CHECK_LAUNCH("k_affine_positions");
+    if (e->c.kind == RF_TEST_BRAZIL) k_affine_scalars<RF_TEST_BRAZIL><<<1, 32, 0, s>>>(e->d, e->c, strain[0], strain[1], strain[2]);
+    else k_affine_scalars<RF_TEST_UNIAXIAL><<<1, 32, 0, s>>>(e->d, e->c, strain[0], strain[1], strain[2]);
+    RF_CHECK_LAUNCH("k_affine_scalars");
+    return RF_OK;
 }
 
 rf_status rf_engine_step_host(rf_engine* e, const float* h_R_in, uint64_t nsteps, float* h_R_out) {

@@ -158,6 +158,7 @@ _proto = {
     "rf_engine_create": (i32, [C.POINTER(Task), P, C.POINTER(P)]),
     "rf_engine_destroy": (i32, [P]),
     "rf_engine_step": (i32, [P, u64]),
+    "rf_engine_affine_strain": (i32, [P, C.POINTER(C.c_double)]),
     "rf_engine_step_host": (i32, [P, P, u64, P]),
     "rf_engine_sync": (i32, [P, C.POINTER(Task), C.POINTER(RunResult)]),
     "rf_engine_export": (i32, [P] + [P] * 10),
@@ -472,6 +473,11 @@ class Engine:
 
     def step(self, n):
         check(lib.rf_engine_step(self.h, n), "rf_engine_step")
+
+    def affine_strain(self, ex, ey, ez):
+        """Homogeneous strain of the specimen about the platen box's centre (platens move with it)."""
+        a = (C.c_double * 3)(ex, ey, ez)
+        check(lib.rf_engine_affine_strain(self.h, a), "rf_engine_affine_strain")
 
     def step_host(self, R_in, n, R_out):
         check(lib.rf_engine_step_host(self.h, ptr(R_in), n, ptr(R_out)), "rf_engine_step_host")

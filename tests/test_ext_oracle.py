@@ -212,3 +212,22 @@ def test_brazil_fire_increments_and_exact_warm_start():
     w = oracle.warm_probe(mc.clone(t), x, R, rad, p, 3, 20000, fp64=False)
     assert w["conv_warm"] == 1 and w["it_warm"] * 10 < w["it_plain"]
     assert abs(w["stress_warm"] / w["stress_plain"] - 1.0) < 1e-5
+
+
+def test_intact_bonds_outlive_the_list_cutoff(oracle):
+    """With a list gap (pairs listed within r_i + r_j + g) a bond stretched past that
+    cutoff but not past 1.45 times its rest length stays until its strength breaks it:
+    after a 20 % lateral pre-strain every bond lost in the window is a strength break."""
+    r0 = 0.25
+    R0, rad = extspec.lattice_ext(0, 24 * r0, 40 * r0, r0=r0, seed=0xB2000000 + 77, rlo=0.9, jitter=0.02)
+    t, R = rfdem.make_test_ext(0, R0, rad, r0, dt=0.01, v_load=-0.1 * 40 * r0 * 1e-6, max_strain=1.0)
+    x = rfdem.ext_params_si()
+    x.list_gap = 0.25 * r0
+    N, K = int(t.N), int(t.K)
+    b0, _ = extspec.pair_counts(R, N, K, oracle.run_ext(mc.clone(t), x, R, rad, 0)["IL"],
+                                oracle.run_ext(mc.clone(t), x, R, rad, 0)["ILtype"], rad)
+    o = oracle.run_ext(mc.clone(t), x, R, rad, 200, strain=(0.2, 0.2, -0.1))
+    b1, contacts = extspec.pair_counts(o["R"], N, K, o["IL"], o["ILtype"], rad)
+    print("bond slots %d -> %d, broken by strength %d, overlapping contacts %d" % (b0, b1, o["broken"], contacts))
+    assert o["broken"] > 0 and contacts > 0
+    assert b0 - b1 == o["broken"]

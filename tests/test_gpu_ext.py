@@ -166,3 +166,30 @@ def test_ext_list_gap_lattice_vs_oracle(cuda):
     assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
     assert np.array_equal(st["ILtype"], o["ILtype"])
     assert_damage(t, x, R, rad, o, res)
+
+
+def test_prestrained_window_bitexact_vs_oracle(cuda):
+    """rf_engine_affine_strain (20 % lateral, -10 % axial) on a polydisperse specimen with
+    the benchmark's bond constants and list gap, then explicit steps: engine == float
+    oracle bit for bit through the burst of strength breaks and the loaded contacts that
+    follow."""
+    r0 = 0.25
+    R0, rad = extspec.lattice_ext(0, 24 * r0, 40 * r0, r0=r0, seed=0xB2000000 + 77, rlo=0.9, jitter=0.02)
+    t, R = rfdem.make_test_ext(0, R0, rad, r0, dt=0.01, v_load=-0.1 * 40 * r0 * 1e-6, max_strain=1.0)
+    x = rfdem.ext_params_si()
+    x.list_gap = 0.25 * r0
+    steps, strain = 1500, (0.2, 0.2, -0.1)
+    o = oracle.run_ext(mc.clone(t), x, R, rad, steps, strain=strain)
+    e = rfdem.Engine(mc.clone(t), R, ext=x, radius=rad)
+    e.affine_strain(*strain)
+    e.step(steps)
+    _, res = e.sync()
+    st = e.export()
+    st["R64"] = e.positions_f64()
+    e.close()
+    assert res.error == 0 and o["status"] == 0 and res.steps == o["steps"] == steps
+    assert np.array_equal(st["R64"], o["R"]), np.abs(st["R64"] - o["R"]).max()
+    assert np.array_equal(st["V"], o["V"])
+    assert np.array_equal(st["IL"].astype(np.uint64), o["IL"])
+    assert np.array_equal(st["ILtype"], o["ILtype"])
+    assert_damage(t, x, R, rad, o, res)

@@ -70,6 +70,7 @@ def _declare(L):
         "rfo_run_ext_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
         "rfo_run_ext_pos_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P, i32]),
         "rfo_run_ext_d": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, u64, P, P, P, P, u64, P, P, P]),
+        "rfo_time_ext_f": (f64, [T, C.POINTER(rfdem.ExtParams), P, P, P, u64, i32, P]),
         "rfo_run_ext_strained_f": (u64, [T, C.POINTER(rfdem.ExtParams), P, P, P, u64, P, P, P, P, u64, P, P, P]),
     }
     for n, (r, a) in proto.items():
@@ -145,6 +146,18 @@ def run_ext(task, x, R0, radius, max_steps, fp64=False, positions="f64", strain=
                 status=status.value, broken=int(broken.value))
 
 
+def time_ext(task, x, R0, radius, steps, threads, strain=None):
+    """Seconds of `steps` explicit steps of the extended model on `threads` host threads
+    (bond construction and the pre-strain untimed); returns (seconds, steps done)."""
+    L = load()
+    R = np.ascontiguousarray(R0, np.float64)
+    rad = np.ascontiguousarray(radius, np.float64)
+    sv = None if strain is None else (C.c_double * 3)(*strain)
+    done = C.c_uint64(0)
+    secs = L.rfo_time_ext_f(C.byref(task), C.byref(x), p(R), p(rad), sv, steps, threads, C.byref(done))
+    return secs, int(done.value)
+
+
 def qs_ext(task, x, R0, radius, params, n_inc, fp64=False, trace_cap=0):
     """Quasi-static FIRE load increments of the extended model; returns dict(R, iters,
     converged, residual, stress, trace, status)."""
@@ -208,4 +221,7 @@ def ref_cpu():
     P, u32, f32 = C.c_void_p, C.c_uint32, C.c_float
     L.ref_cpu_bond_forces.argtypes = [P, P, P, P, P, P, u32, u32, f32, f32, f32, f32, f32, f32, C.c_int, C.c_int, P]
     L.ref_cpu_bond_forces.restype = C.c_double
+    L.ref_cpu_bond_forces_rb.argtypes = [P, P, P, P, P, P, u32, u32, f32, f32, f32, P, f32, f32, C.c_int, C.c_int,
+                                         P]
+    L.ref_cpu_bond_forces_rb.restype = C.c_double
     return L

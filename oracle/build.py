@@ -3,7 +3,8 @@
 Build recipe for the checkers:
 
 * ``oracle/_build/liboracle.so`` -- the CPU restatement ``oracle/rf_oracle.cpp``
-  (g++ -O2 -ffp-contract=off, so float arithmetic is plain IEEE in source order).
+  (g++ -O2 -ffp-contract=off, so float arithmetic is plain IEEE in source order;
+  -fopenmp for the multi-threaded timing path, which is serial at one thread).
 * ``oracle/_ref/libmdref_gpu.so`` -- the reference's own live kernels and host step
   functions, compiled unmodified from the reference tree for sm_100a, plus the
   harness ``oracle/ref/ref_gpu_harness.cu``.
@@ -71,7 +72,7 @@ def build_oracle(force=False):
     hdr = os.path.join(HERE, "..", "include", "rockfit_b200.h")
     out = os.path.join(BUILD, "liboracle.so")
     if force or not _newer(out, [src, hdr, __file__]):
-        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-o", out, src])
+        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-o", out, src])
     return out
 
 

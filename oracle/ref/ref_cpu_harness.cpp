@@ -25,15 +25,46 @@ extern "C" {
 // `threads` host threads, each thread on its own copy of the mutable state (the
 // function walks all N*K slots of one specimen and cannot be split). Returns the
 // wall time in seconds; *slot_evals gets the bond-slot evaluations done.
+static double run_bond_forces(const float* R, const float* V, const float* W, const uint32_t* IL,
+                              const uint8_t* ILtype, const float* iL, uint32_t N, uint32_t K, float dt,
+                              float m_E, float m_G, const float* slot_b_r, float b_r, float m_Gcritn,
+                              float m_Gcritt, int reps, int threads, uint64_t* slot_evals);
+
 double ref_cpu_bond_forces(const float* R, const float* V, const float* W, const uint32_t* IL,
                            const uint8_t* ILtype, const float* iL, uint32_t N, uint32_t K, float dt,
                            float m_E, float m_G, float b_r, float m_Gcritn, float m_Gcritt, int reps,
                            int threads, uint64_t* slot_evals) {
+    return run_bond_forces(R, V, W, IL, ILtype, iL, N, K, dt, m_E, m_G, nullptr, b_r, m_Gcritn, m_Gcritt, reps,
+                           threads, slot_evals);
+}
+
+// The same with a bond radius per slot (slot_b_r[N*K]), as the function's per-slot ab_r
+// and AxialMoment arguments allow: a polydisperse specimen's bonds each have their own.
+double ref_cpu_bond_forces_rb(const float* R, const float* V, const float* W, const uint32_t* IL,
+                              const uint8_t* ILtype, const float* iL, uint32_t N, uint32_t K, float dt,
+                              float m_E, float m_G, const float* slot_b_r, float m_Gcritn, float m_Gcritt, int reps,
+                              int threads, uint64_t* slot_evals) {
+    return run_bond_forces(R, V, W, IL, ILtype, iL, N, K, dt, m_E, m_G, slot_b_r, 0.f, m_Gcritn, m_Gcritt, reps,
+                           threads, slot_evals);
+}
+
+}  // extern "C"
+
+static double run_bond_forces(const float* R, const float* V, const float* W, const uint32_t* IL,
+                              const uint8_t* ILtype, const float* iL, uint32_t N, uint32_t K, float dt,
+                              float m_E, float m_G, const float* slot_b_r, float b_r, float m_Gcritn,
+                              float m_Gcritt, int reps, int threads, uint64_t* slot_evals) {
     const size_t nk = (size_t)N * K;
     uint64_t bonds = 0;
     for (size_t k = 0; k < nk; ++k) if (IL[k] < N && ILtype[k] == 1) ++bonds;
     const float PI = 3.14159265358979f;
     std::vector<float> ab_r(nk, b_r), axial(nk, PI * b_r * b_r * b_r * b_r * 0.25f);
+    if (slot_b_r)
+        for (size_t k = 0; k < nk; ++k) {
+            const float r = slot_b_r[k];
+            ab_r[k] = r;
+            axial[k] = PI * r * r * r * r * 0.25f;
+        }
     if (threads < 1) threads = 1;
     float3 z = make_float3(0.f, 0.f, 0.f);
     std::vector<float3> Rij(nk, z), Oijt(nk, z), Mijn(nk, z), Mijt(nk, z), Fij(nk, z), Fijn(nk, z), Fijt(nk, z),
@@ -67,5 +98,3 @@ double ref_cpu_bond_forces(const float* R, const float* V, const float* W, const
     if (slot_evals) *slot_evals = bonds * (uint64_t)reps * (uint64_t)threads;
     return std::chrono::duration<double>(t1 - t0).count();
 }
-
-}  // extern "C"

@@ -31,6 +31,7 @@
 #include <vector>
 #include <algorithm>
 #include <limits>
+#include <chrono>
 
 #include "../include/rockfit_b200.h"
 
@@ -902,6 +903,9 @@ static inline double hilo_add(double x, float d) {
 template <class TF>
 struct RunExt {
     int pos_mode = 0;           // positions as doubles (0), hi/lo float pairs (1, see hilo_add) or floats (2)
+    // host threads of the per-particle loops (OpenMP). 1: serial, in particle order; more
+    // threads reorder only the FP64 platen and force-magnitude sums, so they are for timing
+    int nthreads = 1;
     rf_task* t;
     ExtPar x;
     uint64_t N, K, CN;
@@ -1038,6 +1042,7 @@ struct RunExt {
     }
 
     void delete_far() {
+#pragma omp parallel for schedule(static) if (nthreads > 1) num_threads(nthreads)
         for (uint64_t i = 0; i < N; ++i)
             for (uint64_t q = 0; q < K; ++q) {
                 const uint64_t k = i * K + q;
@@ -1057,6 +1062,8 @@ struct RunExt {
         const float inv_a = t->C._1d_a, a = t->C.a;
         int s = cell_distribution<float>(Rf.data(), N, CI.data(), CIs.data(), pnC.data(), CN, inv_a, t->C.Nr);
         if (s && !status) status = s;
+        int overflow = 0;
+#pragma omp parallel for schedule(static) reduction(| : overflow) if (nthreads > 1) num_threads(nthreads)
         for (uint64_t i = 0; i < N; ++i) {
             int64_t cells[8];
             octant_cells<float>(Rf.data(), N, i, a, inv_a, t->C.Nr, cells);
@@ -1084,12 +1091,13 @@ struct RunExt {
                             kf = (int64_t)q;
                             break;
                         }
-                    if (kf < 0) { if (!status) status = ST_ROW_OVERFLOW; continue; }
+                    if (kf < 0) { overflow = 1; continue; }
                     IL[i * K + kf] = j;
                     type[i * K + kf] = 0;
                 }
             }
         }
+        if (overflow && !status) status = ST_ROW_OVERFLOW;
     }
 
     // One bond slot (engine bond_slot_ext). With the reference constants the stiffness per
@@ -1362,7 +1370,13 @@ struct RunExt {
     void pair_forces(std::vector<V3<TF>>& Fn, std::vector<V3<TF>>& Mn, double& fnsum, double& npair,
                      std::vector<double>* KT = nullptr, std::vector<double>* KR = nullptr) {
         fnsum = 0; npair = 0;
+        double fs_ = 0, np_ = 0;
+        uint64_t nb_ = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : fs_, np_, nb_) if (nthreads > 1) num_threads(nthreads)
         for (uint64_t i = 0; i < N; ++i) {
+            double& fnsum = fs_;
+            double& npair = np_;
+            uint64_t& broken = nb_;
             double* kt = KT ? &(*KT)[i] : nullptr;
             double* kr = KR ? &(*KR)[i] : nullptr;
             if (kt) { *kt = 0; *kr = 0; }
@@ -1419,6 +1433,8 @@ struct RunExt {
             Mx += msc.x; My += msc.y; Mz += msc.z;
             Fn[i] = {Fx, Fy, Fz}; Mn[i] = {Mx, My, Mz};
         }
+        fnsum = fs_; npair = np_;
+        broken += nb_;
     }
 
     // Platen of one particle (the extended model's d_braziltest_simple2 /
@@ -1504,6 +1520,7 @@ struct RunExt {
         double sfb = 0, sft = 0;
         const TF vt = (TF)(float)Kc.V;
         const rf_sample& S = t->S;
+#pragma omp parallel for schedule(static) reduction(+ : sfb, sft) if (nthreads > 1) num_threads(nthreads)
         for (uint64_t i = 0; i < N; ++i) {
             TF Fx = Fn[i].x, Fy = Fn[i].y, Fz = Fn[i].z;
             double Rx = R[i], Ry = R[i + N], Rz = R[i + 2 * N];
@@ -1825,6 +1842,24 @@ uint64_t rfo_run_ext_pos_f(rf_task* t, const rf_ext_params* x, double* R_io, con
                            uint64_t* nsaved, int* status, uint64_t* broken, int pos_mode) {
     return rfo::run_ext<float>(t, x, R_io, rad, max_steps, V_out, IL_out, type_out, curve, cap, nsaved, status,
                                broken, pos_mode);
+}
+// Wall time of `steps` explicit steps of the extended model (float forces, FP64 positions)
+// on `threads` host threads, after bond construction and rf_engine_affine_strain(strain)
+// (strain may be null); the set-up is not timed. The CPU baseline of the benchmark.
+double rfo_time_ext_f(rf_task* t, const rf_ext_params* xp, const double* R0, const double* rad, const double* strain,
+                      uint64_t steps, int threads, uint64_t* done) {
+    rfo::RunExt<float> r;
+    r.t = t;
+    r.x = rfo::ext_par(xp);
+    r.nthreads = threads < 1 ? 1 : threads;
+    r.init(R0, rad);
+    if (strain) r.affine(strain[0], strain[1], strain[2]);
+    uint64_t ns = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    while (r.running() && r.steps < steps) r.step(nullptr, 0, &ns);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (done) *done = r.steps;
+    return std::chrono::duration<double>(t1 - t0).count();
 }
 // rfo_run_ext_f after rf_engine_affine_strain(strain) applied to the built specimen.
 uint64_t rfo_run_ext_strained_f(rf_task* t, const rf_ext_params* x, double* R_io, const double* rad,

@@ -1,34 +1,42 @@
 """Benchmark: particle-steps/s of the explicit bonded-particle step, and wall time per
-relaxed quasi-static load step (FIRE, warm-started by the MLP vs plain).
+relaxed quasi-static load step (FIRE, warm-started vs plain).
 
-Workload: a 200,000-particle polydisperse cylinder packed on the GPU (radii U[0.8, 1.2]
-x 0.25 mm, aspect 2, packing fraction 0.58: D 24.6 x H 49.3 mm), bonded where the gap is
-below 0.05 r_min, kn = 1e11 N/m^3, ks = kn / 2.5, Weibull(m = 5) tensile / shear
-strengths with scales 10 / 30 MPa, granite contacts, FP64 positions and FP32 forces,
-dt = 1e-8 s, platen strain rate 0.1/s. One bench "step" is STEPS_PER_BENCH_STEP
-explicit steps of the whole specimen (list maintenance, bond and contact forces with
-the break check, platen, integration, cut, load reduction).
+Explicit workload (the large polydisperse uniaxial configuration): 4,000,000 particles
+packed on the GPU, radii log-uniform in [0.5, 1.5] x 0.25 mm (radius ratio 3), a cylinder
+of aspect 2 (D 65.7 x H 131.4 mm at packing fraction 0.58), bonded where the gap is below
+0.05 r_min, kn = 1e11 N/m^3, ks = kn / 2.5, Weibull(m = 5) tensile / shear strengths with
+scales 10 / 30 MPa, FP64 positions and FP32 forces, dt = 1e-8 s, platen strain rate
+0.1/s, pairs listed within min(a_farcut, r_i + r_j + 0.25 r0). With these bonds a bond
+fails only near 20 % stretch, which loading at 0.1/s does not reach in a benchmark's
+steps; so the specimen is first pre-strained (rf_engine_affine_strain: +20 % laterally,
+-10 % axially) and the timed steps run in that damaged state: bonds break and contacts
+carry load in the window (both reported in config). One bench "step" is
+STEPS_PER_BENCH_STEP explicit steps of the whole specimen (list maintenance, bond and
+contact forces with the break check, platen, integration, cut, load reduction).
 
 value : particle-steps/s of the fused engine, state resident in HBM, CUDA events on the
         engine's stream (max over ranks for N > 1).
 e2e   : the same metric through the public API with host buffers: rf_engine_create_ext
-        from pinned host positions and radii (bond construction included), the steps,
-        and the FP64 positions read back.
+        from pinned host positions and radii (bond construction included), the pre-strain,
+        the steps, and the FP64 positions read back.
 batch : 64 Brazilian discs of 5k-80k particles advanced by one step kernel
         (rf_engine_create_batch) vs one engine per specimen, particle-steps/s of both.
-fire  : quasi-static load increments (strain 2.5e-5) of the same specimen relaxed by
-        FIRE to a residual of 1e-6 x the mean normal pair force: plain FIRE vs FIRE
-        warm-started by the MLP trained on plain-FIRE pairs of the same run; wall time
-        per load step of each.
+fire  : quasi-static load increments (strain 2.5e-5) of a 1M-particle cylinder (radii
+        U[0.8, 1.2] x 0.25 mm) relaxed by FIRE to a residual of 1e-6 x the mean normal pair
+        force: plain FIRE vs FIRE warm-started by the MLP trained on plain-FIRE pairs, and
+        warm-started by the last increment's displacements; wall time per load step of each.
 --impl reference : the reference's own CPU force path (h_CalculateForceElastic,
-        md_calculateforcesbpm_cpu.cpp, built from its source into oracle/_ref) on a
-        198k-particle lattice specimen of the reference's own (mono-sized, FP32) model,
-        all host threads. The extended model has no reference implementation.
+        md_calculateforcesbpm_cpu.cpp, built from its source into oracle/_ref) over the
+        bond slots of a committed sample of the same specimen (a contiguous block of
+        SAMPLE_N particles from the middle of the spatially numbered 4M specimen, which
+        the engine arm checks bit for bit against its own), all host threads. It needs no
+        part of the engine: bonds are found with scipy.
 
 Multi-GPU: independent specimens per rank (different seeds), no data-path
 collective; only the elapsed time is max-reduced.
 """
 import argparse
+import ctypes as C
 import json
 import math
 import os
@@ -47,13 +55,16 @@ for _p in (ROOT, PKG):
 import numpy as np
 
 STEPS_PER_BENCH_STEP = 1000
-N_PARTICLES, R0, PHI = 200000, 0.25, 0.58
-DIAMETER, HEIGHT = 52.0, 104.0          # the reference-model lattice specimen (198,061 particles)
+R0_MM, PHI, ASPECT = 0.25, 0.58, 2.0
+N_PARTICLES, RMIN, RMAX, RADII = 4000000, 0.5, 1.5, "log-uniform"
+LIST_GAP = 0.25                          # x r0
+PRESTRAIN = (0.2, 0.2, -0.1)             # lateral, lateral, axial
+FIRE_PARTICLES = 1000000                 # the quasi-static configuration (radii U[0.8, 1.2] x r0)
+FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 1, 2, 20
+SAMPLE_N = 65536                         # particles of the committed specimen sample
+SAMPLE_FILE = os.path.join(ROOT, "oracle", "data", "bench_sample_4m.npz")
+DIAMETER, HEIGHT = 52.0, 104.0           # the reference-model lattice specimen (198,061 particles)
 METRIC = "particle-steps/s; wall time per relaxed load step, warm-start vs plain FIRE"
-REF_WORKLOAD = ("reference model (mono-sized granite BPM, FP32): 198k-particle lattice cylinder D52xH104 mm; "
-                "the reference has no polydisperse / FP64 / Weibull model, so its own model is timed")
-WORKLOAD = ("explicit BPM uniaxial compression, 200k-particle polydisperse cylinder (radii U[0.8,1.2] x 0.25 mm, "
-            "D 24.6 x H 49.3 mm), Weibull bond strengths, FP64 positions / FP32 forces, dt 1e-8 s, 0.1/s")
 
 
 def peaks():
@@ -64,8 +75,8 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_particle_step(name="k_step_ext_uniaxial-200k.md"):
-    """dram read+write bytes per particle-step of the step kernel from the committed ncu summary."""
+def traffic_per_particle_step(name):
+    """dram read+write bytes per particle-step of the step kernel from a committed ncu summary."""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
@@ -73,6 +84,237 @@ def traffic_per_particle_step(name="k_step_ext_uniaxial-200k.md"):
         if line.startswith("traffic_bytes_per_particle_step:"):
             return float(line.split(":")[1])
     return None
+
+
+def workload_name(args):
+    dist = "U[%g,%g]" % (args.rmin, args.rmax) if args.radii == "uniform" else \
+        "log-uniform [%g,%g]" % (args.rmin, args.rmax)
+    pre = ("pre-strained %+g/%+g/%+g (x/y/z) into the damage regime" % tuple(args.prestrain)) if any(args.prestrain) \
+        else "no pre-strain"
+    return ("explicit BPM uniaxial compression, %d-particle polydisperse cylinder (radii %s x 0.25 mm, aspect 2, "
+            "packing 0.58), gap < 0.05 r_min bonds, kn 1e11 N/m^3, ks kn/2.5, Weibull(5) strengths 10/30 MPa, "
+            "FP64 positions / FP32 forces, dt 1e-8 s, 0.1/s, %s" % (args.particles, dist, pre))
+
+
+def sample_block(N):
+    """Index range of the specimen sample: SAMPLE_N consecutive particles from the middle
+    of the spatially numbered specimen (a slab across the cylinder)."""
+    n = min(SAMPLE_N, N)
+    a = N // 2 - n // 2
+    return a, a + n
+
+
+def sample_bonds(R, rad, K=32, gap_frac=0.05, lam=0.330015):
+    """Bond rows of a specimen sample by the extended model's rule (gap < gap_frac * min
+    radius), in the reference's row layout, with each slot's bond radius lam * min(r_i, r_j)
+    and 1/L0; found with a k-d tree (scipy), no part of the engine."""
+    from scipy.spatial import cKDTree
+    n = rad.size
+    X = np.ascontiguousarray(R.reshape(3, n).T)
+    tree = cKDTree(X)
+    pairs = tree.query_pairs(2.0 * rad.max() * (1.0 + gap_frac), output_type="ndarray")
+    i, j = pairs[:, 0], pairs[:, 1]
+    d = np.sqrt(((X[i] - X[j]) ** 2).sum(1))
+    keep = d - rad[i] - rad[j] < gap_frac * np.minimum(rad[i], rad[j])
+    i, j, d = i[keep], j[keep], d[keep]
+    a = np.concatenate([i, j])
+    b = np.concatenate([j, i])
+    dd = np.concatenate([d, d])
+    order = np.lexsort((b, a))
+    a, b, dd = a[order], b[order], dd[order]
+    first = np.searchsorted(a, np.arange(n))
+    slot = np.arange(a.size) - first[a]
+    ok = slot < K
+    IL = np.full(n * K, 0xFFFFFFFF, np.uint32)
+    ty = np.zeros(n * K, np.uint8)
+    iL = np.zeros(n * K, np.float32)
+    br = np.zeros(n * K, np.float32)
+    k = a[ok] * K + slot[ok]
+    IL[k] = b[ok]
+    ty[k] = 1
+    iL[k] = (1.0 / dd[ok]).astype(np.float32)
+    br[k] = (lam * np.minimum(rad[a[ok]], rad[b[ok]])).astype(np.float32)
+    return IL, ty, iL, br, int(ok.sum())
+
+
+def run_reference(args):
+    """The reference's own CPU force path on the committed sample of the benchmark's
+    specimen, all host threads (one sample copy per thread: the function walks a whole
+    specimen). Loads only oracle/_ref/libmdref_cpu.so; nothing of the engine."""
+    rank, ws, dist = dist_init()
+    if rank != 0:
+        return
+    import oracle
+    ref = oracle.ref_cpu()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmdref_cpu.so not built "
+                                                               "(reference tree absent at build time)"}))
+        return
+    if not os.path.exists(SAMPLE_FILE):
+        print(json.dumps({"impl": "reference", "unavailable": "specimen sample %s missing" % SAMPLE_FILE}))
+        return
+    z = np.load(SAMPLE_FILE)
+    R, rad = z["R"], z["radius"]
+    n, K = rad.size, 32
+    IL, ty, iL, br, bonds = sample_bonds(R, rad, K)
+    Rf = R.astype(np.float32)
+    V = np.zeros(3 * n, np.float32)
+    W = np.zeros(3 * n, np.float32)
+    # model units (mm, mg, us): stiffness per area kn = 1e11 N/m^3 -> E = kn * L0 at the mean
+    # rest length; strengths 10 / 30 MPa; dt 1e-8 s
+    kn = 1e11 / 1e12
+    E = kn * float(np.mean(1.0 / iL[ty == 1]))
+    G = E / 2.494
+    threads = os.cpu_count() or 1
+    ev = C.c_uint64(0)
+    call = lambda reps: ref.ref_cpu_bond_forces_rb(Rf.ctypes.data, V.ctypes.data, W.ctypes.data, IL.ctypes.data,
+                                                   ty.ctypes.data, iL.ctypes.data, n, K, 0.01, E, G, br.ctypes.data,
+                                                   0.01, 0.03, reps, threads, C.byref(ev))
+    call(1)
+    for _ in range(max(args.warmup, 1) - 1):
+        call(1)
+    secs = call(args.steps)
+    value = threads * n * args.steps / secs
+    sample = ("reference h_CalculateForceElastic (md_calculateforcesbpm_cpu.cpp:20-288; bond slots only, no "
+              "contacts, lists or integration) over all %d directed bond slots of the committed %d-particle "
+              "sample of the benchmark specimen (particles %d..%d of the 4M specimen), per-bond radius "
+              "0.330015 min(r_i, r_j), %d passes per thread, %d threads each on its own sample copy; one pass = "
+              "one particle-step of every sample particle" % (bonds, n, int(z["first"]), int(z["first"]) + n - 1,
+                                                              args.steps, threads))
+    out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "impl": "reference", "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": workload_name(args), "particles": args.particles, "sample_particles": n,
+                      "cpu_threads": threads, "same_specimen": "committed sample of the engine arm's specimen"},
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def ext_specimen(rfdem, N, seed, dist, rmin, rmax):
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, R0_MM, rmin=rmin, rmax=rmax, aspect=ASPECT, phi=PHI, seed=seed,
+                                            dist=dist)
+    v = -0.1 * H * 1e-6                        # strain rate 0.1/s in mm per microsecond
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, R0_MM, dt=0.01, v_load=v, max_strain=1.0)
+    return t, R, rad, D, H
+
+
+def ext_bytes_per_particle_step(K, bbar, cbar):
+    """Algorithmic bytes per particle-step of the fused extended-model step: FP64
+    position (32 B) and FP32 velocity and spin (32 B) read and written, the K-slot row
+    (id + type) once, the binning share, per bond record its partner id and slot (5),
+    state read and written (96), rest length and strengths (16), per active contact its
+    tangential overlap read and written (24)."""
+    return 128 + 5 * K + 32 + 117 * bbar + 24 * cbar
+
+
+def run_explicit(rfdem, torch, t, R, rad, x, args, dist):
+    S = STEPS_PER_BENCH_STEP
+    e = rfdem.Engine(t, R, ext=x, radius=rad)
+    stream = torch.cuda.ExternalStream(e.stream())
+    if any(args.prestrain):
+        e.affine_strain(*args.prestrain)
+    tuned = e.autotune(200)            # trial steps on a snapshot, state restored
+    for _ in range(args.warmup):
+        e.step(S)
+    torch.cuda.synchronize()
+    c0 = e.counters()
+    _, r0 = e.sync()
+    clocks = Clocks(torch.cuda.current_device())
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e.step(S)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist is not None:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    c1 = e.counters()
+    _, res = e.sync()
+    done_steps = c1["steps"] - c0["steps"]
+    if done_steps != S * args.steps:
+        raise SystemExit("bench: the specimen finished early (%d of %d steps)" % (done_steps, S * args.steps))
+    if res.error:
+        raise SystemExit("bench: engine error %d (%s)" % (res.error, rfdem.STATUS.get(res.error, "?")))
+    graph = e.uses_graph()
+    e.close()
+    return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, tuned=tuned,
+                broken_window=int(res.broken_bonds - r0.broken_bonds), broken_total=int(res.broken_bonds),
+                bonds_initial=int(res.bonds_initial))
+
+
+def run_fire(rfdem, torch, seed, n_eval):
+    """Quasi-static load steps of the 1M-particle cylinder: two engines in lockstep take
+    FIRE_PRE + FIRE_COLLECT plain increments (the MLP is trained on the plain engine's
+    FIRE_COLLECT relaxation pairs), then n_eval increments each: one plain, one
+    warm-started by the MLP. Wall time per relaxed load step of each. A third engine,
+    warm-started by its own last increment's displacements (rotations from zero), is the
+    predictor-free reference the MLP has to beat."""
+    from rfdem.warm import WarmStart
+    t, R, rad, D, H = ext_specimen(rfdem, FIRE_PARTICLES, seed, "uniform", 0.8, 1.2)
+    x = rfdem.ext_params_si()
+    x.list_gap = LIST_GAP * R0_MM
+    FIRE_N = int(t.N)
+    A = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
+    B = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
+    Cn = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
+    p = A.relax_params(max_iter=60000)
+    ws = WarmStart(FIRE_N, p.strain_inc, seed=seed)
+    for k in range(FIRE_PRE + FIRE_COLLECT):
+        collect = k >= FIRE_PRE
+        if collect:
+            ws.features(A)
+        A.load_increment(p)
+        B.load_increment(p)
+        Cn.load_increment(p)
+        if collect:
+            ws.collect(A)
+    t0 = time.perf_counter()
+    losses = ws.train()
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    plain, warm, last = [], [], []
+    for k in range(n_eval):
+        t0 = time.perf_counter()
+        ra = A.load_increment(p)
+        ta = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Y = ws.predict(B)
+        rb = B.load_increment_pred(p, Y, 16)
+        tb = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        _, dxc, _ = Cn.increment_fields()
+        wc = torch.from_numpy(np.concatenate([dxc, np.zeros_like(dxc)], 1).astype(np.float32)).cuda()
+        rc = Cn.load_increment(p, wc)
+        tc = time.perf_counter() - t0
+        plain.append((ta, ra.iterations, ra.converged, ra.stress))
+        warm.append((tb, rb.iterations, rb.converged, rb.stress))
+        last.append((tc, rc.iterations, rc.converged, rc.stress))
+    A.close(); B.close(); Cn.close(); ws.close()
+    tp = sum(a[0] for a in plain) / n_eval
+    tw = sum(a[0] for a in warm) / n_eval
+    return {"workload": "quasi-static uniaxial load steps of strain 2.5e-5 of a %d-particle cylinder (radii "
+                        "U[0.8,1.2] x 0.25 mm, D %.1f x H %.1f mm), FIRE (stiffness-scaled masses) to RMS net force "
+                        "<= 1e-6 x mean normal pair force" % (FIRE_N, D, H),
+            "particles": FIRE_N, "evaluated_increments": n_eval,
+            "wall_s_per_load_step_plain": tp, "wall_s_per_load_step_warm": tw, "speedup_warm_vs_plain": tp / tw,
+            "iterations_plain": [a[1] for a in plain], "iterations_warm": [a[1] for a in warm],
+            "converged_plain": [a[2] for a in plain], "converged_warm": [a[2] for a in warm],
+            "stress_plain": [a[3] for a in plain], "stress_warm": [a[3] for a in warm],
+            "wall_s_per_load_step_last_increment_warm": sum(a[0] for a in last) / n_eval,
+            "iterations_last_increment_warm": [a[1] for a in last],
+            "converged_last_increment_warm": [a[2] for a in last],
+            "stress_last_increment_warm": [a[3] for a in last],
+            "training_pairs": ws.pairs(), "training_loss": [losses[0], losses[-1]], "training_s": t_train,
+            "warm_start_includes": "feature build + MLP forward (tcgen05 BF16) per load step"}
 
 
 class Clocks:
@@ -158,200 +400,6 @@ def sum_over_ranks(x, dist):
 def rank_seed(rank):
     """Each rank packs its own specimen: weak scaling, no data-path collective."""
     return 0xB2000000 + 2000 + rank
-
-
-def cpu_reference(task, R, reps, threads):
-    """The reference's own h_CalculateForceElastic over the specimen's bond slots.
-    Rows come from the oracle's restatement of the reference's initial build."""
-    import ctypes as C
-    import oracle
-    L = oracle.load()
-    ref = oracle.ref_cpu()
-    N, K = int(task.N), int(task.K)
-    CN = int(task.C.N)
-    CI, CIs, pnC = np.zeros(N, np.uint64), np.zeros(2 * N, np.uint64), np.zeros(2 * CN, np.uint64)
-    L.rfo_cell_distribution_f(R.ctypes.data, N, CI.ctypes.data, CIs.ctypes.data, pnC.ctypes.data, CN, task.C._1d_a,
-                              task.C.Nr)
-    IL = np.zeros(N * K, np.uint64)
-    L.rfo_construct_list_f(R.ctypes.data, N, CIs.ctypes.data, pnC.ctypes.data, IL.ctypes.data, K, task.C.a,
-                           task.C._1d_a, task.aacut, task.C.Nr, CN)
-    ty, iL = np.zeros(N * K, np.uint8), np.zeros(N * K, np.float32)
-    z = np.zeros(3 * N * K, np.float32)
-    L.rfo_construct_bonds_f(R.ctypes.data, N, IL.ctypes.data, ty.ctypes.data, iL.ctypes.data, z.ctypes.data,
-                            z.ctypes.data, z.ctypes.data, z.ctypes.data, K, float(np.float32(task.Po.b_dd)))
-    bonds = int(((IL != np.uint64(2 ** 64 - 1)) & (ty == 1)).sum())
-    if ref is None:
-        return None, bonds
-    IL32 = IL.astype(np.uint32)
-    IL32[IL == np.uint64(2 ** 64 - 1)] = np.uint32(0xFFFFFFFF)
-    V = np.zeros(3 * N, np.float32)
-    W = np.zeros(3 * N, np.float32)
-    f = lambda x: float(np.float32(x))
-    P = task.Po
-    ev = C.c_uint64(0)
-    secs = ref.ref_cpu_bond_forces(R.ctypes.data, V.ctypes.data, W.ctypes.data, IL32.ctypes.data, ty.ctypes.data,
-                                   iL.ctypes.data, N, K, f(P.dt), f(P.m_E), f(P.m_G), f(P.b_r), f(P.m_Ec), f(P.m_Gc),
-                                   reps, threads, C.byref(ev))
-    return secs, bonds
-
-
-def run_reference(args):
-    rank, ws, dist = dist_init()
-    if rank != 0:
-        return
-    import rfdem
-    t, R = rfdem.make_test(rfdem.RF_TEST_UNIAXIAL, DIAMETER, HEIGHT, seed=0xB2000000 + 2000, max_strain=1.0)
-    threads = os.cpu_count() or 1
-    cpu_reference(t, R, 1, 1)                      # builds rows once (and warms the library)
-    secs_w, _ = cpu_reference(t, R, max(args.warmup, 1), threads)
-    if secs_w is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmdref_cpu.so not built (reference tree absent at build time)"}))
-        return
-    secs, bonds = cpu_reference(t, R, args.steps, threads)
-    N = int(t.N)
-    value = threads * N * args.steps / secs
-    sample = ("reference h_CalculateForceElastic (md_calculateforcesbpm_cpu.cpp:20-288, bond slots only) over all "
-              "%d directed bond slots of the %d-particle specimen, %d passes per thread, %d threads each on its own "
-              "specimen copy; one pass = one particle-step of every particle" % (bonds, N, args.steps, threads))
-    out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "impl": "reference", "n_gpus": ws,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": REF_WORKLOAD, "particles": N, "cpu_threads": threads},
-           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
-                            "sample": sample},
-           "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out))
-
-
-def workload_name(args):
-    if args.particles == N_PARTICLES and args.radii == "uniform" and (args.rmin, args.rmax) == (0.8, 1.2):
-        return WORKLOAD
-    dist = "U[%g,%g]" % (args.rmin, args.rmax) if args.radii == "uniform" else \
-        "log-uniform [%g,%g]" % (args.rmin, args.rmax)
-    return ("explicit BPM uniaxial compression, %d-particle polydisperse cylinder (radii %s x 0.25 mm, aspect 2), "
-            "Weibull bond strengths, FP64 positions / FP32 forces, dt 1e-8 s, 0.1/s" % (args.particles, dist))
-
-
-def ext_specimen(rfdem, N, seed, dist="uniform", rmin=0.8, rmax=1.2):
-    R0, rad, D, H, mo = rfdem.pack_cylinder(N, R0_MM, rmin=rmin, rmax=rmax, aspect=2.0, phi=PHI, seed=seed,
-                                            dist=dist)
-    v = -0.1 * H * 1e-6                        # strain rate 0.1/s in mm per microsecond
-    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, R0_MM, dt=0.01, v_load=v, max_strain=1.0)
-    return t, R, rad, D, H
-
-
-R0_MM = R0
-
-
-def ext_bytes_per_particle_step(K, bbar, cbar):
-    """Algorithmic bytes per particle-step of the fused extended-model step: FP64
-    position (32 B) and FP32 velocity and spin (32 B) read and written, the K-slot row
-    (id + type) once, the binning share, per bond record its partner id and slot (5),
-    state read and written (96), rest length and strengths (16), per active contact its
-    tangential overlap read and written (24)."""
-    return 128 + 5 * K + 32 + 117 * bbar + 24 * cbar
-
-
-def run_explicit(rfdem, torch, t, R, rad, x, args, dist, stream_of):
-    S = STEPS_PER_BENCH_STEP
-    N = int(t.N)
-    e = rfdem.Engine(t, R, ext=x, radius=rad)
-    stream = torch.cuda.ExternalStream(e.stream())
-    tuned = e.autotune(200)            # trial steps on a snapshot, state restored
-    for _ in range(args.warmup):
-        e.step(S)
-    torch.cuda.synchronize()
-    c0 = e.counters()
-    clocks = Clocks(torch.cuda.current_device())
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        e.step(S)
-    ev1.record(stream)
-    ev1.synchronize()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    if dist is not None:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    c1 = e.counters()
-    _, res = e.sync()
-    done_steps = c1["steps"] - c0["steps"]
-    if done_steps != S * args.steps:
-        raise SystemExit("bench: the specimen finished early (%d of %d steps)" % (done_steps, S * args.steps))
-    graph = e.uses_graph()
-    if res.error:
-        raise SystemExit("bench: engine error %d (%s)" % (res.error, rfdem.STATUS.get(res.error, "?")))
-    e.close()
-    return dict(ms=ms, c0=c0, c1=c1, clocks=clk, graph=graph, error=res.error, tuned=tuned)
-
-
-FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 1, 2, 4
-
-
-def run_fire(rfdem, torch, t, R, rad, x, seed):
-    """Quasi-static load steps on the benchmark specimen: two engines in lockstep take
-    FIRE_PRE + FIRE_COLLECT plain increments (the MLP is trained on the plain engine's
-    FIRE_COLLECT relaxation pairs), then FIRE_EVAL increments each: one plain, one
-    warm-started by the MLP. Wall time per relaxed load step of each. A third engine,
-    warm-started by its own last increment's displacements (rotations from zero), is the
-    predictor-free reference the MLP has to beat."""
-    from rfdem.warm import WarmStart
-    FIRE_N = int(t.N)
-    A = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
-    B = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
-    Cn = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
-    p = A.relax_params(max_iter=60000)
-    ws = WarmStart(FIRE_N, p.strain_inc, seed=seed)
-    for k in range(FIRE_PRE + FIRE_COLLECT):
-        collect = k >= FIRE_PRE
-        if collect:
-            ws.features(A)
-        A.load_increment(p)
-        B.load_increment(p)
-        Cn.load_increment(p)
-        if collect:
-            ws.collect(A)
-    t0 = time.perf_counter()
-    losses = ws.train()
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    plain, warm, last = [], [], []
-    for k in range(FIRE_EVAL):
-        t0 = time.perf_counter()
-        ra = A.load_increment(p)
-        ta = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        Y = ws.predict(B)
-        rb = B.load_increment_pred(p, Y, 16)
-        tb = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        _, dxc, _ = Cn.increment_fields()
-        wc = torch.from_numpy(np.concatenate([dxc, np.zeros_like(dxc)], 1).astype(np.float32)).cuda()
-        rc = Cn.load_increment(p, wc)
-        tc = time.perf_counter() - t0
-        plain.append((ta, ra.iterations, ra.converged, ra.stress))
-        warm.append((tb, rb.iterations, rb.converged, rb.stress))
-        last.append((tc, rc.iterations, rc.converged, rc.stress))
-    A.close(); B.close(); Cn.close(); ws.close()
-    tp = sum(a[0] for a in plain) / FIRE_EVAL
-    tw = sum(a[0] for a in warm) / FIRE_EVAL
-    return {"workload": "quasi-static uniaxial load steps of strain 2.5e-5 of the same %d-particle specimen, "
-                        "FIRE (stiffness-scaled masses) to RMS net force <= 1e-6 x mean normal pair force" % FIRE_N,
-            "wall_s_per_load_step_plain": tp, "wall_s_per_load_step_warm": tw, "speedup_warm_vs_plain": tp / tw,
-            "iterations_plain": [a[1] for a in plain], "iterations_warm": [a[1] for a in warm],
-            "converged_plain": [a[2] for a in plain], "converged_warm": [a[2] for a in warm],
-            "stress_plain": [a[3] for a in plain], "stress_warm": [a[3] for a in warm],
-            "wall_s_per_load_step_last_increment_warm": sum(a[0] for a in last) / FIRE_EVAL,
-            "iterations_last_increment_warm": [a[1] for a in last],
-            "converged_last_increment_warm": [a[2] for a in last],
-            "stress_last_increment_warm": [a[3] for a in last],
-            "training_pairs": ws.pairs(), "training_loss": [losses[0], losses[-1]], "training_s": t_train,
-            "warm_start_includes": "feature build + MLP forward (tcgen05 BF16) per load step"}
 
 
 BATCH_SPECIMENS, BATCH_STEPS, BATCH_FULL_CAP = 64, 1000, 300000
@@ -473,32 +521,73 @@ def run_fit_step(rfdem):
     return out
 
 
+def check_sample(R, rad, write_path=None):
+    """The specimen's sample block against the committed file (bit for bit), or written."""
+    N = rad.size
+    a, b = sample_block(N)
+    P = R.reshape(3, N)[:, a:b]
+    if write_path:
+        os.makedirs(os.path.dirname(os.path.abspath(write_path)), exist_ok=True)
+        np.savez_compressed(write_path, R=np.ascontiguousarray(P).reshape(-1), radius=rad[a:b].copy(), first=a,
+                            total=N)
+    if not os.path.exists(SAMPLE_FILE):
+        return None
+    z = np.load(SAMPLE_FILE)
+    return bool(int(z["first"]) == a and int(z["total"]) == N and np.array_equal(z["R"], P.reshape(-1)) and
+                np.array_equal(z["radius"], rad[a:b]))
+
+
+def cpu_port_sample(rfdem, t, x, R, rad, prestrain):
+    """The oracle's restatement of the extended-model step (the engine's arithmetic) on the
+    committed sample block of the same specimen, pre-strained the same way, on all host
+    threads; bond construction and pre-strain untimed."""
+    import oracle
+    N = rad.size
+    a, b = sample_block(N)
+    Rb = np.ascontiguousarray(R.reshape(3, N)[:, a:b]).reshape(-1)
+    ts, Rs = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, Rb, rad[a:b], R0_MM, dt=0.01, v_load=float(t.Compress.VLoad),
+                                 max_strain=1.0)
+    threads = os.cpu_count() or 1
+    secs, n = oracle.time_ext(rfdem.Task.from_buffer_copy(ts), x, Rs, rad[a:b], 2, threads, prestrain)
+    steps = max(2, min(200, int(15.0 / max(secs / 2, 1e-3))))
+    secs, n = oracle.time_ext(rfdem.Task.from_buffer_copy(ts), x, Rs, rad[a:b], steps, threads, prestrain)
+    return {"value": (b - a) * n / secs, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": "oracle restatement of the extended-model explicit step (float forces, FP64 positions, lists, "
+                      "bonds, contacts, integration), %d steps of the %d-particle sample block of the same specimen "
+                      "(its own platens), pre-strained the same way, on %d host threads (OpenMP); construction "
+                      "untimed" % (n, b - a, threads)}
+
+
 def run_engine(args):
     import torch
     rank, ws, dist = dist_init()
     import rfdem
     S = STEPS_PER_BENCH_STEP
+    t0 = time.perf_counter()
     t, R, rad, Dm, Hm = ext_specimen(rfdem, args.particles, rank_seed(rank), args.radii, args.rmin, args.rmax)
+    t_pack = time.perf_counter() - t0
+    same_sample = check_sample(R, rad, args.write_sample if rank == 0 else None) if rank == 0 else None
     x = rfdem.ext_params_si()
     x.list_gap = args.list_gap * R0_MM
     N = int(t.N)
     K = int(t.K)
-    r = run_explicit(rfdem, torch, t, R, rad, x, args, dist, None)
+    r = run_explicit(rfdem, torch, rfdem.Task.from_buffer_copy(t), R, rad, x, args, dist)
     ms = r["ms"]
     ms_max = max_over_ranks(ms, dist)
     total_particles = sum_over_ranks(float(N), dist)
     value = total_particles * S * args.steps / (ms_max * 1e-3)
     c1, c0 = r["c1"], r["c0"]
-    bbar, cbar = c1["bonds"] / N, c1["contacts"] / N
+    bbar = 0.5 * (c0["bonds"] + c1["bonds"]) / N
+    cbar = 0.5 * (c0["contacts"] + c1["contacts"]) / N
     b_step = ext_bytes_per_particle_step(K, bbar, cbar)
     per_step_s = (ms * 1e-3) / (S * args.steps)
     achieved = b_step * N / per_step_s / 1e9
     peak, peak_kind = peaks()
-    tr = traffic_per_particle_step()
+    tr = traffic_per_particle_step("k_step_ext_uniaxial-4m-prestrained.md")
     rebuilds = c1["rebuilds"] - c0["rebuilds"]
     launches = S * args.steps + 7 * rebuilds + 2 * args.steps
 
-    # e2e through the public API with host buffers (pinned)
+    # e2e through the public API with host buffers (pinned): create, pre-strain, steps, read back
     import ctypes as C
     e2e_value = None
     e2e_calls = 0 if args.no_e2e else 3
@@ -506,12 +595,15 @@ def run_engine(args):
         hR = torch.from_numpy(R).pin_memory()
         hrad = torch.from_numpy(rad).pin_memory()
         hout = torch.empty_like(hR).pin_memory()
+        strain = (C.c_double * 3)(*args.prestrain)
 
         def e2e_call():
             tt = rfdem.Task.from_buffer_copy(t)
             h = rfdem.P()
             rfdem.check(rfdem.lib.rf_engine_create_ext(C.byref(tt), C.byref(x), hR.data_ptr(), hrad.data_ptr(),
                                                        C.byref(h)), "e2e create")
+            if any(args.prestrain):
+                rfdem.check(rfdem.lib.rf_engine_affine_strain(h, strain), "e2e pre-strain")
             rfdem.check(rfdem.lib.rf_engine_step(h, S), "e2e step")
             rfdem.check(rfdem.lib.rf_engine_positions_f64(h, hout.data_ptr()), "e2e positions")
             rfdem.lib.rf_engine_destroy(h)
@@ -519,11 +611,11 @@ def run_engine(args):
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-        t0 = time.perf_counter()
+        t1 = time.perf_counter()
         for _ in range(e2e_calls):
             e2e_call()
         torch.cuda.synchronize()
-        e2e_s = max_over_ranks(time.perf_counter() - t0, dist)
+        e2e_s = max_over_ranks(time.perf_counter() - t1, dist)
         e2e_value = total_particles * S * e2e_calls / e2e_s
 
     # the reference's own model (mono-sized lattice, FP32 state), reference-exact engine
@@ -552,13 +644,10 @@ def run_engine(args):
                     "unit": "particle-steps/s", "ms_per_step": mr / args.steps,
                     "bytes_per_particle_step": round(72 + 5 * K + 32 + 105 * cr["bonds"] / Nr
                                                      + 24 * cr["contacts"] / Nr, 1)}
-        trr = traffic_per_particle_step("k_step_uniaxial-200k.md")
-        if trr:
-            refmodel["traffic_bytes_per_particle_step"] = trr
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_port_sample(t, x, R, rad)
+        cpu = cpu_port_sample(rfdem, t, x, R, rad, args.prestrain)
 
     batch = None
     if rank == 0 and ws == 1 and not args.no_batch:
@@ -570,25 +659,29 @@ def run_engine(args):
 
     fire = None
     if rank == 0 and ws == 1 and not args.no_fire:
-        fire = run_fire(rfdem, torch, t, R, rad, x, 0xB2000000 + 3000)
+        fire = run_fire(rfdem, torch, 0xB2000000 + 3000, args.fire_eval)
     if rank != 0:
         return
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 forces, f64 positions", "data": "synthetic",
            "config": {"workload": workload_name(args), "particles": N, "specimen_mm": [round(Dm, 2), round(Hm, 2)],
-                      "explicit_steps_per_bench_step": S, "slots_K": K,
+                      "packing_s": round(t_pack, 1), "explicit_steps_per_bench_step": S, "slots_K": K,
                       "list_rule": ("pairs within min(a_farcut, r_i + r_j + %g mm)" % x.list_gap) if x.list_gap > 0
                       else "pairs within a_farcut (the reference's)",
+                      "prestrain_xyz": list(args.prestrain),
                       "bonds_per_particle": round(bbar, 3), "contacts_per_particle": round(cbar, 3),
+                      "bonds_broken_in_window": r["broken_window"], "bonds_broken_total": r["broken_total"],
+                      "bond_slots_initial": r["bonds_initial"],
+                      "sample_matches_committed_file": same_sample,
                       "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 16 + N * 300 + c1["bonds"] * 129) / 1e6),
                       "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": r["graph"],
                       "autotune": {"ctas_per_sm": r["tuned"][0],
                                    "ms_per_200_steps_for_6_5_4": [round(v, 3) for v in r["tuned"][1]]}},
            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * N,
                    "d2h_bytes_per_step": 24 * N,
-                   "path": "rf_engine_create_ext (host positions + radii, bond build) + %d explicit steps + "
-                           "rf_engine_positions_f64 per call" % S},
+                   "path": "rf_engine_create_ext (host positions + radii, bond build) + rf_engine_affine_strain + %d "
+                           "explicit steps + rf_engine_positions_f64 per call" % S},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "traffic": (tr * N) if tr else None, "peak_source": peak_kind,
                         "kernel": "k_step_ext (fused explicit step, extended model)",
@@ -606,47 +699,31 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
-def cpu_port_sample(t, x, R, rad):
-    """The oracle's restatement of the extended-model step (the engine's arithmetic, one
-    host thread) on the same specimen: bond construction once, then explicit steps;
-    the per-step time excludes the construction."""
-    import oracle
-    import rfdem
-    t1 = time.perf_counter()
-    oracle.run_ext(rfdem.Task.from_buffer_copy(t), x, R, rad, 0)
-    t_init = time.perf_counter() - t1
-    steps = 3
-    t1 = time.perf_counter()
-    oracle.run_ext(rfdem.Task.from_buffer_copy(t), x, R, rad, steps)
-    t_run = time.perf_counter() - t1 - t_init
-    N = int(t.N)
-    return {"value": N * steps / t_run, "unit": "particle-steps/s", "cores": 1, "kind": "port",
-            "sample": "oracle restatement of the extended-model explicit step (float forces, FP64 positions), "
-                      "%d steps of the same %d-particle specimen on one host thread (construction excluded)"
-                      % (steps, N)}
-
-
 def main():
     global STEPS_PER_BENCH_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the driver-call leg (profiling runs)")
     ap.add_argument("--no-fire", action="store_true", help="skip the quasi-static FIRE comparison")
+    ap.add_argument("--fire-eval", type=int, default=FIRE_EVAL, help="evaluated FIRE load increments")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-specimen comparison")
     ap.add_argument("--explicit-steps", type=int, default=STEPS_PER_BENCH_STEP,
                     help="explicit steps per bench step (profiling runs use fewer)")
     ap.add_argument("--no-reference-model", action="store_true", help="skip the reference-model line")
     ap.add_argument("--particles", type=int, default=N_PARTICLES, help="particles of the benchmark specimen")
-    ap.add_argument("--radii", default="uniform", choices=["uniform", "log-uniform"])
-    ap.add_argument("--rmin", type=float, default=None, help="smallest radius / 0.25 mm (0.8; 0.5 log-uniform)")
-    ap.add_argument("--rmax", type=float, default=None, help="largest radius / 0.25 mm (1.2; 1.5 log-uniform)")
-    ap.add_argument("--list-gap", type=float, default=None,
+    ap.add_argument("--radii", default=RADII, choices=["uniform", "log-uniform"])
+    ap.add_argument("--rmin", type=float, default=None, help="smallest radius / 0.25 mm (0.5; 0.8 uniform)")
+    ap.add_argument("--rmax", type=float, default=None, help="largest radius / 0.25 mm (1.5; 1.2 uniform)")
+    ap.add_argument("--list-gap", type=float, default=LIST_GAP,
                     help="list gap / 0.25 mm: pairs listed within min(a_farcut, r_i + r_j + gap) "
-                         "(default 0.25; 0 is the reference's uniform cutoff a_farcut)")
+                         "(0 is the reference's uniform cutoff a_farcut)")
+    ap.add_argument("--prestrain", type=float, nargs=3, default=list(PRESTRAIN),
+                    help="homogeneous pre-strain x y z applied before the warm-up (0 0 0: none)")
+    ap.add_argument("--write-sample", default=None, help="write the specimen's sample block to this .npz")
     ap.add_argument("--fit", action="store_true", help="time one material-fitter step (12 runs to fracture)")
     ap.add_argument("--batch-full", action="store_true",
                     help="run the 64-disc batch to every specimen's post-peak drop instead of the timed window")
@@ -655,8 +732,6 @@ def main():
         args.rmin = 0.8 if args.radii == "uniform" else 0.5
     if args.rmax is None:
         args.rmax = 1.2 if args.radii == "uniform" else 1.5
-    if args.list_gap is None:
-        args.list_gap = 0.25
     if args.warmup < 3:
         args.warmup = 3
     STEPS_PER_BENCH_STEP = max(1, args.explicit_steps)

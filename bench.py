@@ -9,7 +9,7 @@ scales 10 / 30 MPa, FP64 positions and FP32 forces, dt = 1e-8 s, platen strain r
 0.1/s, pairs listed within min(a_farcut, r_i + r_j + 0.25 r0). With these bonds a bond
 fails only near 20 % stretch, which loading at 0.1/s does not reach in a benchmark's
 steps; so the specimen is first pre-strained (rf_engine_affine_strain: +20 % laterally,
--10 % axially) and the timed steps run in that damaged state: bonds break and contacts
+-3 % axially) and the timed steps run in that damaged state: bonds break and contacts
 carry load in the window (both reported in config). One bench "step" is
 STEPS_PER_BENCH_STEP explicit steps of the whole specimen (list maintenance, bond and
 contact forces with the break check, platen, integration, cut, load reduction).
@@ -58,7 +58,7 @@ STEPS_PER_BENCH_STEP = 1000
 R0_MM, PHI, ASPECT = 0.25, 0.58, 2.0
 N_PARTICLES, RMIN, RMAX, RADII = 4000000, 0.5, 1.5, "log-uniform"
 LIST_GAP = 0.25                          # x r0
-PRESTRAIN = (0.2, 0.2, -0.1)             # lateral, lateral, axial
+PRESTRAIN = (0.2, 0.2, -0.03)            # lateral, lateral, axial
 FIRE_PARTICLES = 1000000                 # the quasi-static configuration (radii U[0.8, 1.2] x r0)
 FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 1, 2, 20
 SAMPLE_N = 65536                         # particles of the committed specimen sample
@@ -677,7 +677,7 @@ def run_engine(args):
                       "l2": "inputs larger than L2 (state %.0f MB)" % ((N * K * 16 + N * 300 + c1["bonds"] * 129) / 1e6),
                       "parallelism": "specimen-per-gpu" if ws > 1 else "single", "graph": r["graph"],
                       "autotune": {"ctas_per_sm": r["tuned"][0],
-                                   "ms_per_200_steps_for_6_5_4": [round(v, 3) for v in r["tuned"][1]]}},
+                                   "ms_per_200_steps_for_8_6_5": [round(v, 3) for v in r["tuned"][1]]}},
            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 32 * N,
                    "d2h_bytes_per_step": 24 * N,
                    "path": "rf_engine_create_ext (host positions + radii, bond build) + rf_engine_affine_strain + %d "

@@ -500,10 +500,10 @@ rf_status rf_engine_curve(rf_engine* e, double* curve, uint64_t cap, uint64_t* n
 rf_status rf_engine_counters(rf_engine* e, uint64_t* out, int n);
 
 /* Autotuner (extended model): times `steps` explicit steps with each compiled variant of
-   the step kernel (register caps for 6, 5 and 4 resident 128-thread CTAs per SM) on a
+   the step kernel (register caps for 8, 6 and 5 resident 128-thread CTAs per SM) on a
    snapshot of the engine's state, restores the state, and keeps the fastest variant
    for the step graph. All variants compute identical results. *choice: CTAs per SM of
-   the pick; ms_out[3] (may be NULL): time of each variant for 6, 5, 4. The reference
+   the pick; ms_out[3] (may be NULL): time of each variant for 8, 6, 5. The reference
    model's step has a single variant (choice 6, no timing). Needs a second copy of the
    engine's device memory while it runs. */
 rf_status rf_engine_autotune(rf_engine* e, int steps, int* choice, float* ms_out);

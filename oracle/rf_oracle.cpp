@@ -1100,176 +1100,76 @@ struct RunExt {
         if (overflow && !status) status = ST_ROW_OVERFLOW;
     }
 
-    // One bond slot (engine bond_slot_ext). With the reference constants the stiffness per
-    // area is E/L0 and G/L0 of the slot (the reference's E*_1d_iL, G*_1d_iL) and the bending
-    // moment carries the extra dt*E/(4 L0) factor (Q1, md_calculateforcesdem3.cu:131-152).
-    bool bond(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& vi, const V3<TF>& vj, const V3<TF>& wi,
-              const V3<TF>& wj, TF br, V3<TF>& fs, V3<TF>& ms, double& fnsum, double* kt, double* kr) {
-        const TF PI = pi_t<TF>();
-        const TF kn = x.ref ? mE * iL0[k] : this->kn;
-        const TF ks = x.ref ? mG * iL0[k] : this->ks;
-        const TF rijm = (TF)rlen;
-        const TF inv_rm = rcp(rijm);
-        const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
-        const TF stretch = (TF)(rlen - L0[k]);
-        const TF A = br * br * PI;
-        const TF J = PI * br * br * br * br;
-        if (kt) {
-            *kt += (double)((kn + ks) * A);
-            *kr += (double)((TF)0.25f * kn * J + (TF)0.5f * ks * J + (TF)0.25f * ks * A * rijm * rijm);
-        }
-        TF cef = kn * stretch;
-        TF Sc = cef;
-        cef *= A;
-        fnsum += std::fabs((double)cef);
-        fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
-        V3<TF>& Rk = Rij[k];
-        const TF tx = Rk.y * nz - Rk.z * ny, ty = Rk.z * nx - Rk.x * nz, tz = Rk.x * ny - Rk.y * nx;
-        const TF wsx = wj.x + wi.x, wsy = wj.y + wi.y, wsz = wj.z + wi.z;
-        const TF cphi = (wsx * nx + wsy * ny + wsz * nz) * dt * (TF)0.5f;
-        const TF phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
-        Rk = {nx, ny, nz};
-        const TF M1x = (TF)1.0f + tz * phz + ty * phy, M1y = phz - tz - ty * phx, M1z = -phy - tz * phx + ty;
-        const TF M2x = tz - phz - tx * phy, M2y = tz * phz + (TF)1.0f + tx * phx, M2z = -tz * phy + phx - tx;
-        const TF M3x = -ty - tx * phz + phy, M3y = -ty * phz + tx - phx, M3z = ty * phy + tx * phx + (TF)1.0f;
-        const TF dwx = wj.x - wi.x, dwy = wj.y - wi.y, dwz = wj.z - wi.z;
-        {
-            TF c1 = nx * dwx + ny * dwy + nz * dwz;
-            c1 *= dt * (TF)0.5f * ks;
-            const V3<TF> o = Mijn[k];
-            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
-            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
-            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
-            Mijn[k] = {mx, my, mz};
-            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
-        }
-        {
-            const TF c1 = nx * dwx + ny * dwy + nz * dwz;
-            TF c2 = dt * (TF)0.25f * kn;
-            const V3<TF> o = Mijt[k];
-            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
-            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
-            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
-            Mijt[k] = {mx, my, mz};
-            if (x.ref) {                                        // Q1: the factor again
-                const TF q = c2 * J;
-                ms.x += mx * q; ms.y += my * q; ms.z += mz * q;
-            } else {
-                ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
-            }
-        }
-        TF Mc;
-        {
-            const TF hx = (TF)0.5f * wsx, hy = (TF)0.5f * wsy, hz = (TF)0.5f * wsz;
-            const TF vx = vj.x - vi.x - hy * r.z + hz * r.y;
-            const TF vy = vj.y - vi.y - hz * r.x + hx * r.z;
-            const TF vz = vj.z - vi.z - hx * r.y + hy * r.x;
-            TF c = nx * vx + ny * vy + nz * vz;
-            const V3<TF> o = Oijt[k];
-            const TF ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c) * dt;
-            const TF oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (vy - ny * c) * dt;
-            const TF oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (vz - nz * c) * dt;
-            c = ks;
-            Mc = c;
-            c *= A;
-            fs.x += ox * c; fs.y += oy * c; fs.z += oz * c;
-            Oijt[k] = {ox, oy, oz};
-            ms.x += (TF)0.5f * (r.y * oz - r.z * oy) * c;
-            ms.y += (TF)0.5f * (r.z * ox - r.x * oz) * c;
-            ms.z += (TF)0.5f * (r.x * oy - r.y * ox) * c;
-        }
-        const V3<TF>& O = Oijt[k];
-        const V3<TF>& Mt = Mijt[k];
-        const V3<TF>& Mn = Mijn[k];
-        Mc *= norm3(O.x, O.y, O.z);
-        Sc += norm3(Mt.x, Mt.y, Mt.z) * (TF)4.0f * br;
-        Mc += norm3(Mn.x, Mn.y, Mn.z) * (TF)2.0f * br;
-        if ((Sc > (TF)sig[k]) || (Mc > (TF)tau[k])) {
-            Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
-            return true;
-        }
-        return false;
-    }
+    // The extended model's arithmetic is written with explicit fused multiply-adds, as the
+    // engine's (rf_physics.cuh: fm, dot3, bond_core, contact_pair_ext); std::fma is the same
+    // correctly rounded operation, so the float instance stays bit-exact with the engine.
+    static TF fm(TF a, TF b, TF c) { return std::fma(a, b, c); }
+    static TF dot3(TF ax, TF ay, TF az, TF bx, TF by, TF bz) { return fm(ax, bx, fm(ay, by, az * bz)); }
+    static TF len_sq(double rr) { return std::sqrt((TF)rr); }
+    static TF stretch_sq(double rr, double L0, TF rlen) { return (TF)std::fma(-L0, L0, rr) * rcp(rlen + (TF)L0); }
 
-    // One bond slot inside a quasi-static increment: the state is the increment's start
-    // state carried to the current configuration in one step -- start normal Rij0 to the
-    // current normal n, the particles' rotations ti, tj and displacements ui, uj since the
-    // increment began -- with bond()'s formulas, so it depends on where the particles are,
-    // not on the path the relaxation took to get there.
-    // du: the pair's relative motion since the increment began less the mean rotation's
-    // part, (r - r0) - ((ti + tj) / 2) x r, formed in double by the caller (in float its
-    // terms cancel and the relaxation stalls on the rounding).
-    bool bond_total(uint64_t k, const V3<TF>& r, double rlen, const V3<TF>& du, const V3<TF>& ti,
-                    const V3<TF>& tj, TF br, V3<TF>& fs, V3<TF>& ms, double& fnsum, double* kt, double* kr) {
+    // engine bond_core: the bond update shared by the explicit step (dts = dt, rates) and
+    // the quasi-static total (dts = 1, displacements); Rp, Ot0, Mn0, Mt0 the state it
+    // starts from, results into slot k. kt, kr, fnabs: the particle's float accumulators.
+    bool bond_core(uint64_t k, TF kn, TF ks, TF br, const V3<TF>& r, TF rlen, TF stretch, TF dts, V3<TF> Rp,
+                   V3<TF> ws, V3<TF> dw, V3<TF> du, V3<TF> Ot0, V3<TF> Mn0, V3<TF> Mt0, V3<TF>& fs, V3<TF>& ms,
+                   TF& fnabs, TF& kt, TF& kr, bool q1) {
         const TF PI = pi_t<TF>();
-        const TF rijm = (TF)rlen;
-        const TF inv_rm = rcp(rijm);
+        const TF inv_rm = rcp(rlen);
         const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
-        const TF stretch = (TF)(rlen - L0[k]);
         const TF A = br * br * PI;
-        const TF J = PI * br * br * br * br;
-        if (kt) {
-            *kt += (double)((kn + ks) * A);
-            *kr += (double)((TF)0.25f * kn * J + (TF)0.5f * ks * J + (TF)0.25f * ks * A * rijm * rijm);
-        }
-        TF cef = kn * stretch;
-        TF Sc = cef;
-        cef *= A;
-        fnsum += std::fabs((double)cef);
-        fs.x += nx * cef; fs.y += ny * cef; fs.z += nz * cef;
-        const V3<TF>& R0 = Rij0[k];
-        const TF tx = R0.y * nz - R0.z * ny, ty = R0.z * nx - R0.x * nz, tz = R0.x * ny - R0.y * nx;
-        const TF wsx = tj.x + ti.x, wsy = tj.y + ti.y, wsz = tj.z + ti.z;
-        const TF cphi = (wsx * nx + wsy * ny + wsz * nz) * (TF)0.5f;
+        const TF J = A * (br * br);
+        kt = fm(kn + ks, A, kt);
+        kr = fm((TF)0.25f * ks * A, rlen * rlen, fm(fm((TF)0.25f, kn, (TF)0.5f * ks), J, kr));
+        const TF Sn = kn * stretch;
+        const TF cef = Sn * A;
+        fnabs += std::fabs(cef);
+        fs.x = fm(nx, cef, fs.x); fs.y = fm(ny, cef, fs.y); fs.z = fm(nz, cef, fs.z);
+        const TF tx = fm(Rp.y, nz, -(Rp.z * ny)), ty = fm(Rp.z, nx, -(Rp.x * nz)), tz = fm(Rp.x, ny, -(Rp.y * nx));
+        const TF cphi = dot3(ws.x, ws.y, ws.z, nx, ny, nz) * (dts * (TF)0.5f);
         const TF phx = nx * cphi, phy = ny * cphi, phz = nz * cphi;
         Rij[k] = {nx, ny, nz};
-        const TF M1x = (TF)1.0f + tz * phz + ty * phy, M1y = phz - tz - ty * phx, M1z = -phy - tz * phx + ty;
-        const TF M2x = tz - phz - tx * phy, M2y = tz * phz + (TF)1.0f + tx * phx, M2z = -tz * phy + phx - tx;
-        const TF M3x = -ty - tx * phz + phy, M3y = -ty * phz + tx - phx, M3z = ty * phy + tx * phx + (TF)1.0f;
-        const TF dwx = tj.x - ti.x, dwy = tj.y - ti.y, dwz = tj.z - ti.z;
+        const TF one = (TF)1.0f;
+        const TF M1x = fm(tz, phz, fm(ty, phy, one)), M1y = fm(-ty, phx, phz - tz), M1z = fm(-tz, phx, ty - phy);
+        const TF M2x = fm(-tx, phy, tz - phz), M2y = fm(tz, phz, fm(tx, phx, one)), M2z = fm(-tz, phy, phx - tx);
+        const TF M3x = fm(-tx, phz, phy - ty), M3y = fm(-ty, phz, tx - phx), M3z = fm(ty, phy, fm(tx, phx, one));
+        const TF c1 = dot3(nx, ny, nz, dw.x, dw.y, dw.z);
         {
-            TF c1 = nx * dwx + ny * dwy + nz * dwz;
-            c1 *= (TF)0.5f * ks;
-            const V3<TF> o = Mijn0[k];
-            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + nx * c1;
-            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + ny * c1;
-            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + nz * c1;
+            const TF ct = c1 * (dts * (TF)0.5f * ks);
+            const TF mx = fm(M1x, Mn0.x, fm(M1y, Mn0.y, fm(M1z, Mn0.z, nx * ct)));
+            const TF my = fm(M2x, Mn0.x, fm(M2y, Mn0.y, fm(M2z, Mn0.z, ny * ct)));
+            const TF mz = fm(M3x, Mn0.x, fm(M3y, Mn0.y, fm(M3z, Mn0.z, nz * ct)));
             Mijn[k] = {mx, my, mz};
-            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+            ms.x = fm(mx, J, ms.x); ms.y = fm(my, J, ms.y); ms.z = fm(mz, J, ms.z);
         }
         {
-            const TF c1 = nx * dwx + ny * dwy + nz * dwz;
-            const TF c2 = (TF)0.25f * kn;
-            const V3<TF> o = Mijt0[k];
-            const TF mx = M1x * o.x + M1y * o.y + M1z * o.z + (dwx - nx * c1) * c2;
-            const TF my = M2x * o.x + M2y * o.y + M2z * o.z + (dwy - ny * c1) * c2;
-            const TF mz = M3x * o.x + M3y * o.y + M3z * o.z + (dwz - nz * c1) * c2;
+            const TF c2 = dts * (TF)0.25f * kn;
+            const TF mx = fm(M1x, Mt0.x, fm(M1y, Mt0.y, fm(M1z, Mt0.z, fm(-nx, c1, dw.x) * c2)));
+            const TF my = fm(M2x, Mt0.x, fm(M2y, Mt0.y, fm(M2z, Mt0.z, fm(-ny, c1, dw.y) * c2)));
+            const TF mz = fm(M3x, Mt0.x, fm(M3y, Mt0.y, fm(M3z, Mt0.z, fm(-nz, c1, dw.z) * c2)));
             Mijt[k] = {mx, my, mz};
-            ms.x += mx * J; ms.y += my * J; ms.z += mz * J;
+            const TF q = q1 ? c2 * J : J;       // Q1 (md_calculateforcesdem3.cu:131-152) with the reference constants
+            ms.x = fm(mx, q, ms.x); ms.y = fm(my, q, ms.y); ms.z = fm(mz, q, ms.z);
         }
         TF Mc;
         {
-            const TF vx = du.x, vy = du.y, vz = du.z;
-            TF c = nx * vx + ny * vy + nz * vz;
-            const V3<TF> o = Oijt0[k];
-            const TF ox = (M1x * o.x + M1y * o.y + M1z * o.z) + (vx - nx * c);
-            const TF oy = (M2x * o.x + M2y * o.y + M2z * o.z) + (vy - ny * c);
-            const TF oz = (M3x * o.x + M3y * o.y + M3z * o.z) + (vz - nz * c);
-            c = ks;
-            Mc = c;
-            c *= A;
-            fs.x += ox * c; fs.y += oy * c; fs.z += oz * c;
+            const TF c = dot3(nx, ny, nz, du.x, du.y, du.z);
+            const TF ox = fm(M1x, Ot0.x, fm(M1y, Ot0.y, fm(M1z, Ot0.z, fm(-nx, c, du.x) * dts)));
+            const TF oy = fm(M2x, Ot0.x, fm(M2y, Ot0.y, fm(M2z, Ot0.z, fm(-ny, c, du.y) * dts)));
+            const TF oz = fm(M3x, Ot0.x, fm(M3y, Ot0.y, fm(M3z, Ot0.z, fm(-nz, c, du.z) * dts)));
             Oijt[k] = {ox, oy, oz};
-            ms.x += (TF)0.5f * (r.y * oz - r.z * oy) * c;
-            ms.y += (TF)0.5f * (r.z * ox - r.x * oz) * c;
-            ms.z += (TF)0.5f * (r.x * oy - r.y * ox) * c;
+            const TF kk = ks * A;
+            fs.x = fm(ox, kk, fs.x); fs.y = fm(oy, kk, fs.y); fs.z = fm(oz, kk, fs.z);
+            const TF hk = (TF)0.5f * kk;
+            ms.x = fm(fm(r.y, oz, -(r.z * oy)), hk, ms.x);
+            ms.y = fm(fm(r.z, ox, -(r.x * oz)), hk, ms.y);
+            ms.z = fm(fm(r.x, oy, -(r.y * ox)), hk, ms.z);
+            Mc = ks * std::sqrt(dot3(ox, oy, oz, ox, oy, oz));
         }
-        const V3<TF>& O = Oijt[k];
         const V3<TF>& Mt = Mijt[k];
         const V3<TF>& Mn = Mijn[k];
-        Mc *= norm3(O.x, O.y, O.z);
-        Sc += norm3(Mt.x, Mt.y, Mt.z) * (TF)4.0f * br;
-        Mc += norm3(Mn.x, Mn.y, Mn.z) * (TF)2.0f * br;
+        const TF Sc = fm(std::sqrt(dot3(Mt.x, Mt.y, Mt.z, Mt.x, Mt.y, Mt.z)), (TF)4.0f * br, Sn);
+        Mc = fm(std::sqrt(dot3(Mn.x, Mn.y, Mn.z, Mn.x, Mn.y, Mn.z)), (TF)2.0f * br, Mc);
         if ((Sc > (TF)sig[k]) || (Mc > (TF)tau[k])) {
             Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
             return true;
@@ -1277,60 +1177,98 @@ struct RunExt {
         return false;
     }
 
-    // One overlapping pair (engine contact_pair_ext).
-    void contact(uint64_t k, const V3<TF>& r, TF rijm, TF delta, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
-                 const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms, double& fnsum,
-                 double* kt, double* kr) {
+    // One bond slot in an explicit step (engine bond_slot_ext). With the reference constants
+    // the stiffness per area is E/L0 and G/L0 of the slot (the reference's E*_1d_iL,
+    // G*_1d_iL) and the bending moment carries the extra dt*E/(4 L0) factor.
+    bool bond(uint64_t k, const V3<TF>& r, double rr, const V3<TF>& vi, const V3<TF>& vj, const V3<TF>& wi,
+              const V3<TF>& wj, TF br, V3<TF>& fs, V3<TF>& ms, TF& fnabs, TF& kt, TF& kr) {
+        const TF kn_ = x.ref ? mE * iL0[k] : kn;
+        const TF ks_ = x.ref ? mG * iL0[k] : ks;
+        const TF rlen = len_sq(rr);
+        const TF stretch = stretch_sq(rr, L0[k], rlen);
+        const V3<TF> ws = {wj.x + wi.x, wj.y + wi.y, wj.z + wi.z};
+        const V3<TF> dw = {wj.x - wi.x, wj.y - wi.y, wj.z - wi.z};
+        const TF hx = (TF)0.5f * ws.x, hy = (TF)0.5f * ws.y, hz = (TF)0.5f * ws.z;
+        const V3<TF> du = {fm(hz, r.y, fm(-hy, r.z, vj.x - vi.x)), fm(hx, r.z, fm(-hz, r.x, vj.y - vi.y)),
+                           fm(hy, r.x, fm(-hx, r.y, vj.z - vi.z))};
+        return bond_core(k, kn_, ks_, br, r, rlen, stretch, dt, Rij[k], ws, dw, du, Oijt[k], Mijn[k], Mijt[k], fs,
+                         ms, fnabs, kt, kr, x.ref != 0);
+    }
+
+    // One bond slot inside a quasi-static increment (engine bond_slot_ext_total): the
+    // increment's start state carried to the current configuration in one step -- start
+    // normal Rij0 to the current normal, the particles' rotations ti, tj and the pair's
+    // relative motion since the increment began less the mean rotation's part,
+    // du = (r - r0) - ((ti + tj) / 2) x r, formed in double by the caller (in float its
+    // terms cancel and the relaxation stalls on the rounding) -- so the state depends on
+    // where the particles are, not on the path the relaxation took to get there.
+    bool bond_total(uint64_t k, const V3<TF>& r, double rr, const V3<TF>& du, const V3<TF>& ti, const V3<TF>& tj,
+                    TF br, V3<TF>& fs, V3<TF>& ms, TF& fnabs, TF& kt, TF& kr) {
+        const TF rlen = len_sq(rr);
+        const TF stretch = stretch_sq(rr, L0[k], rlen);
+        const V3<TF> ws = {tj.x + ti.x, tj.y + ti.y, tj.z + ti.z};
+        const V3<TF> dw = {tj.x - ti.x, tj.y - ti.y, tj.z - ti.z};
+        return bond_core(k, kn, ks, br, r, rlen, stretch, (TF)1.0f, Rij0[k], ws, dw, du, Oijt0[k], Mijn0[k],
+                         Mijt0[k], fs, ms, fnabs, kt, kr, false);
+    }
+
+    // One overlapping pair (engine contact_pair_ext): rr = |r|^2 and sr = r_i + r_j in
+    // double with rr < sr^2; the overlap is (sr^2 - rr) / (sr + |r|).
+    void contact(uint64_t k, const V3<TF>& r, double rr, double sr, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
+                 const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms, TF& fnabs, TF& kt,
+                 TF& kr) {
+        const TF rijm = len_sq(rr);
+        const TF delta = (TF)std::fma(sr, sr, -rr) * rcp((TF)sr + rijm);
         const TF inv_rm = rcp(rijm);
         const TF nx = r.x * inv_rm, ny = r.y * inv_rm, nz = r.z * inv_rm;
-        const TF Rs = ri * rj / (ri + rj);
-        const TF ms_ = mi * mj / (mi + mj);
-        TF c1 = std::sqrt(Rs * std::fabs(delta));
-        const TF Kn = (TF)2.0f * hm_E * c1;
-        const TF Kt = (TF)8.0f * hm_G * c1;
-        if (kt) { *kt += (double)(Kn + Kt); *kr += (double)(Kt * ri * ri); }
-        const TF ax = ri * wi.x + rj * wj.x, ay = ri * wi.y + rj * wj.y, az = ri * wi.z + rj * wj.z;
-        const TF vx = vj.x - vi.x + (ny * az - nz * ay);
-        const TF vy = vj.y - vi.y + (nz * ax - nx * az);
-        const TF vz = vj.z - vi.z + (nx * ay - ny * ax);
-        const TF vn = nx * vx + ny * vy + nz * vz;
+        const TF Rs = ri * rj * rcp(ri + rj);
+        const TF ms_ = mi * mj * rcp(mi + mj);
+        const TF c0 = std::sqrt(Rs * delta);
+        const TF Kn = (TF)2.0f * hm_E * c0;
+        const TF Kt = (TF)8.0f * hm_G * c0;
+        kt += Kn + Kt;
+        kr = fm(Kt, ri * ri, kr);
+        const TF ax = fm(ri, wi.x, rj * wj.x), ay = fm(ri, wi.y, rj * wj.y), az = fm(ri, wi.z, rj * wj.z);
+        const TF vx = fm(ny, az, fm(-nz, ay, vj.x - vi.x));
+        const TF vy = fm(nz, ax, fm(-nx, az, vj.y - vi.y));
+        const TF vz = fm(nx, ay, fm(-ny, ax, vj.z - vi.z));
+        const TF vn = dot3(nx, ny, nz, vx, vy, vz);
         const TF fn = -delta * Kn * two_thirds_t<TF>();
-        fnsum += std::fabs((double)fn);
-        c1 = (TF)-1.8257f * p_A * vn * std::sqrt(Kn * ms_);
-        fs.x += nx * (fn + c1); fs.y += ny * (fn + c1); fs.z += nz * (fn + c1);
-        const TF vtx = vx - nx * vn, vty = vy - ny * vn, vtz = vz - nz * vn;
+        fnabs += std::fabs(fn);
+        const TF fnd = fm((TF)-1.8257f * p_A * vn, std::sqrt(Kn * ms_), fn);
+        fs.x = fm(nx, fnd, fs.x); fs.y = fm(ny, fnd, fs.y); fs.z = fm(nz, fnd, fs.z);
+        const TF vtx = fm(-nx, vn, vx), vty = fm(-ny, vn, vy), vtz = fm(-nz, vn, vz);
         const V3<TF> o = Oijt[k];
-        TF c = nx * o.x + ny * o.y + nz * o.z;
-        TF ox = o.x - nx * c, oy = o.y - ny * c, oz = o.z - nz * c;
-        c = ox * ox + oy * oy + oz * oz;
+        TF c = dot3(nx, ny, nz, o.x, o.y, o.z);
+        TF ox = fm(-nx, c, o.x), oy = fm(-ny, c, o.y), oz = fm(-nz, c, o.z);
+        c = dot3(ox, oy, oz, ox, oy, oz);
         if ((double)c > 1e-18) {
-            c = rcp(c);
-            c *= o.x * o.x + o.y * o.y + o.z * o.z;
-            c = std::sqrt(c);
+            c = std::sqrt(dot3(o.x, o.y, o.z, o.x, o.y, o.z) * rcp(c));
             ox *= c; oy *= c; oz *= c;
         }
-        ox += vtx * dt; oy += vty * dt; oz += vtz * dt;
+        ox = fm(vtx, dt, ox); oy = fm(vty, dt, oy); oz = fm(vtz, dt, oz);
         TF ftx = ox * Kt, fty = oy * Kt, ftz = oz * Kt;
-        const TF ftm = ftx * ftx + fty * fty + ftz * ftz;
-        if (ftm > mu * mu * fn * fn) {
+        const TF ftm = dot3(ftx, fty, ftz, ftx, fty, ftz);
+        const TF fmax = mu * fn;
+        if (ftm > fmax * fmax) {
             c = mu * std::fabs(fn) * rsqrt_rn<TF>(ftm);
             ftx *= c; fty *= c; ftz *= c;
             c = rcp(Kt);
             ox = ftx * c; oy = fty * c; oz = ftz * c;
         } else {
             c = (TF)-1.8257f * p_A * std::sqrt(Kt * ms_);
-            ftx += vtx * c; fty += vty * c; ftz += vtz * c;
+            ftx = fm(vtx, c, ftx); fty = fm(vty, c, fty); ftz = fm(vtz, c, ftz);
         }
         Oijt[k] = {ox, oy, oz};
         fs.x += ftx; fs.y += fty; fs.z += ftz;
-        ms.x += (ny * ftz - nz * fty) * ri;
-        ms.y += (nz * ftx - nx * ftz) * ri;
-        ms.z += (nx * fty - ny * ftx) * ri;
+        ms.x = fm(fm(ny, ftz, -(nz * fty)), ri, ms.x);
+        ms.y = fm(fm(nz, ftx, -(nx * ftz)), ri, ms.y);
+        ms.z = fm(fm(nx, fty, -(ny * ftx)), ri, ms.z);
         if (mur != (TF)0) {
-            const TF wim = wi.x * wi.x + wi.y * wi.y + wi.z * wi.z;
+            const TF wim = dot3(wi.x, wi.y, wi.z, wi.x, wi.y, wi.z);
             if ((double)wim > 1e-18) {
                 const TF cr = -mur * std::fabs(fn) * rsqrt_rn<TF>(wim);
-                ms.x += wi.x * cr; ms.y += wi.y * cr; ms.z += wi.z * cr;
+                ms.x = fm(wi.x, cr, ms.x); ms.y = fm(wi.y, cr, ms.y); ms.z = fm(wi.z, cr, ms.z);
             } else {
                 ms = {0, 0, 0};    // QUIRK (md_calculateforcesdem3.cu:316-336): clears the contact sum
             }
@@ -1377,9 +1315,9 @@ struct RunExt {
             double& fnsum = fs_;
             double& npair = np_;
             uint64_t& broken = nb_;
-            double* kt = KT ? &(*KT)[i] : nullptr;
-            double* kr = KR ? &(*KR)[i] : nullptr;
-            if (kt) { *kt = 0; *kr = 0; }
+            // the particle's float sums of |normal pair force| and of its pair stiffnesses,
+            // bonds and contacts apart, as the engine keeps them
+            TF fnb = 0, ktb = 0, krb = 0, fnc = 0, ktc = 0, krc = 0;
             const V3<TF> vi = {V[i], V[i + N], V[i + 2 * N]}, wi = {W[i], W[i + N], W[i + 2 * N]};
             const TF ri = (TF)rad[i];
             const TF mi = cmass * ri * ri * ri;
@@ -1405,9 +1343,9 @@ struct RunExt {
                     const V3<TF> du = {(TF)(dx - (X0[j] - X0[i]) - (hy * dz - hz * dy)),
                                        (TF)(dy - (X0[j + N] - X0[i + N]) - (hz * dx - hx * dz)),
                                        (TF)(dz - (X0[j + 2 * N] - X0[i + 2 * N]) - (hx * dy - hy * dx))};
-                    broke = bond_total(k, r, std::sqrt(d2), du, ti, tj, br, fsb, msb, fnsum, kt, kr);
+                    broke = bond_total(k, r, d2, du, ti, tj, br, fsb, msb, fnb, ktb, krb);
                 } else {
-                    broke = bond(k, r, std::sqrt(d2), vi, vj, wi, wj, br, fsb, msb, fnsum, kt, kr);
+                    broke = bond(k, r, d2, vi, vj, wi, wj, br, fsb, msb, fnb, ktb, krb);
                 }
                 if (broke) { type[k] = 0; ++broken; }
                 npair += 1;
@@ -1419,14 +1357,16 @@ struct RunExt {
                 const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const TF rj = (TF)rad[j];
-                const double rl = std::sqrt(d2), dl = (rad[i] + rad[j]) - rl;   // overlap in double
-                if (!(dl > 0.0)) { Oijt[k] = {0, 0, 0}; continue; }
-                const TF rijm = (TF)rl;
+                const double sr = rad[i] + rad[j];
+                if (!(d2 < sr * sr)) { Oijt[k] = {0, 0, 0}; continue; }
                 const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
                 const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
-                contact(k, r, rijm, (TF)dl, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsc, msc, fnsum, kt, kr);
+                contact(k, r, d2, sr, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsc, msc, fnc, ktc, krc);
                 npair += 1;
             }
+            fnb += fnc; ktb += ktc; krb += krc;
+            fnsum += (double)fnb;
+            if (KT) { (*KT)[i] = (double)ktb; (*KR)[i] = (double)krb; }
             TF Fx = (TF)0 + fsb.x, Fy = (TF)0 + fsb.y, Fz = (TF)0 + fsb.z;
             Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
             TF Mx = (TF)0 + msb.x, My = (TF)0 + msb.y, Mz = (TF)0 + msb.z;

@@ -1155,11 +1155,11 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                 const f3 du = mk3((float)(rd.x - (xj0.x - xi0.x) - (hy * rd.z - hz * rd.y)),
                                   (float)(rd.y - (xj0.y - xi0.y) - (hz * rd.x - hx * rd.z)),
                                   (float)(rd.z - (xj0.z - xi0.z) - (hx * rd.y - hy * rd.x)));
-                broke = bond_slot_ext_total(ep, b, r, sqrt(rr), du, mk3((float)ri0.x, (float)ri0.y, (float)ri0.z),
+                broke = bond_slot_ext_total(b, r, rr, du, mk3((float)ri0.x, (float)ri0.y, (float)ri0.z),
                                             mk3((float)rj0.x, (float)rj0.y, (float)rj0.z), rij, oijt, mijn, mijt, rij,
                                             oijt, mijn, mijt, fsb, msb, fnabs, kt, kr);
             } else {
-                broke = bond_slot_ext(ep, b, r, sqrt(rr), vi, f4to3(vj), wi, f4to3(wj), rij, oijt, mijn, mijt, fsb,
+                broke = bond_slot_ext(ep, b, r, rr, vi, f4to3(vj), wi, f4to3(wj), rij, oijt, mijn, mijt, fsb,
                                       msb, fnabs, kt, kr, c.ref_mode != 0);
             }
             ++npair;
@@ -1191,14 +1191,13 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                 continue;
             }
             const float rj = (float)xj.w;
-            const double rl = sqrt(rr), dl = (xi.w + xj.w) - rl;
-            if (!(dl > 0.0)) continue;
-            const float rijm = (float)rl;
+            const double sr = xi.w + xj.w;
+            if (!(rr < sr * sr)) continue;
             const uint32_t bit = 1u << k;
             // cm: step-start contacts minus slots deleted this step (a refilled slot starts at zero)
             f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
             const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
-            contact_pair_ext(ep, r, rijm, (float)dl, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(__ldg(&Vv[j])), wi,
+            contact_pair_ext(ep, r, rr, sr, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(__ldg(&Vv[j])), wi,
                              f4to3(__ldg(&Wv[j])), o, fsc, msc, fnc, ktc, krc);
             ++npc;
             oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
@@ -1240,7 +1239,8 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             live |= 1u << k;
             mem |= 1ull << best_q;
             const double4 xj = ldg_d4(&P[j]);
-            if ((xi.w + xj.w) - sqrt(dlen2(dsub(xj, xi))) > 0.0) replay = true;
+            const double sr = xi.w + xj.w;
+            if (dlen2(dsub(xj, xi)) < sr * sr) replay = true;
         }
     }
     if (replay) {
@@ -2052,7 +2052,7 @@ template <class T> rf_status dalloc(rf_engine* e, T** p, size_t n) {
 // Explicit extended-model step kernels compiled for 4, 5 or 6 CTAs per SM.
 void* ext_step_variant(bool brazil, int minb) {
     switch (minb) {
-        case 4: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 4> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 4>;
+        case 8: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 8> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 8>;
         case 5: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 5> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 5>;
         default: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 6> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 6>;
     }
@@ -2932,7 +2932,7 @@ rf_status rf_engine_autotune(rf_engine* e, int steps, int* choice, float* ms_out
         }
         return cudaStreamSynchronize(s);
     };
-    const int variants[3] = {6, 5, 4};
+    const int variants[3] = {8, 6, 5};
     float best = 1e30f;
     int pick = e->step_minb;
     float times[3] = {0, 0, 0};

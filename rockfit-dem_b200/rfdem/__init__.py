@@ -449,7 +449,7 @@ class Engine:
 
     def autotune(self, steps=200):
         """Pick the fastest compiled step-kernel variant (state restored afterwards);
-        returns (CTAs per SM of the pick, [ms for 6, 5, 4])."""
+        returns (CTAs per SM of the pick, [ms for 8, 6, 5])."""
         ch = C.c_int(0)
         ms = np.zeros(3, np.float32)
         check(lib.rf_engine_autotune(self.h, steps, C.byref(ch), ms.ctypes.data), "rf_engine_autotune")

@@ -226,7 +226,7 @@ def test_intact_bonds_outlive_the_list_cutoff(oracle):
     N, K = int(t.N), int(t.K)
     b0, _ = extspec.pair_counts(R, N, K, oracle.run_ext(mc.clone(t), x, R, rad, 0)["IL"],
                                 oracle.run_ext(mc.clone(t), x, R, rad, 0)["ILtype"], rad)
-    o = oracle.run_ext(mc.clone(t), x, R, rad, 200, strain=(0.2, 0.2, -0.1))
+    o = oracle.run_ext(mc.clone(t), x, R, rad, 200, strain=(0.2, 0.2, -0.03))
     b1, contacts = extspec.pair_counts(o["R"], N, K, o["IL"], o["ILtype"], rad)
     print("bond slots %d -> %d, broken by strength %d, overlapping contacts %d" % (b0, b1, o["broken"], contacts))
     assert o["broken"] > 0 and contacts > 0

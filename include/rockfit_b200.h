@@ -598,6 +598,16 @@ rf_status rf_save_lammps_data(const char* path, const rf_task* t, uint64_t N, ui
                               const float* V, const float* W, const uint_fast32_t* IL, const uint8_t* ILtype,
                               int with_energy);
 /*
+ * Particle positions as text, the reference's sample files (SaveParticleDATAtxt /
+ * LoadParticleDATAtxt, md_createcylindersample.cu:104-133): the particle count on the first
+ * line, then "x y z" per particle in metres (float mm times 1e-3 as a double, the stream's
+ * default 6 significant digits). R is float[3n] planar in mm. Loading: call with R == NULL
+ * to learn n, then with cap >= n (RF_ERR_CAPACITY otherwise).
+ */
+rf_status rf_save_positions_txt(const char* path, const float* R, uint64_t n);
+rf_status rf_load_positions_txt(const char* path, float* R, uint64_t cap, uint64_t* n);
+
+/*
  * Versioned checkpoint of a reference-model engine: a header ("RFB2CKPT", version 1, id
  * width, the rf_task as rf_engine_sync returns it) followed by the rf_save_all_data
  * payload of the engine's exported state. rf_engine_restore makes an engine from such a

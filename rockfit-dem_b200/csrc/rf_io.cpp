@@ -284,3 +284,43 @@ rf_status rf_save_lammps_data(const char* path, const rf_task* t, uint64_t N, ui
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Particle positions as text (md_createcylindersample.cu:104-133, SaveParticleDATAtxt /
+// LoadParticleDATAtxt): the count on the first line, then one line "x y z" per particle
+// in metres -- each float coordinate (mm) times the length unit 1e-3 as a double, in the
+// stream's default format (6 significant digits). Reading multiplies by 1 / 1e-3 and
+// stores floats, planar x | y | z.
+// ---------------------------------------------------------------------------
+extern "C" rf_status rf_save_positions_txt(const char* path, const float* R, uint64_t n) {
+    if (!path || (!R && n)) { rf::set_error("rf_save_positions_txt: bad arguments"); return RF_ERR_INVALID; }
+    std::ofstream f(path, std::ios::out);
+    if (!f) { rf::set_error("rf_save_positions_txt: cannot open %s", path); return RF_ERR_INVALID; }
+    const double lc = 1e-3;
+    f << n << "\n";
+    for (uint64_t i = 0; i < n; ++i)
+        f << R[i] * lc << " " << R[i + n] * lc << " " << R[i + 2 * n] * lc << "\n";
+    f.close();
+    if (!f) { rf::set_error("rf_save_positions_txt: write to %s failed", path); return RF_ERR_INVALID; }
+    return RF_OK;
+}
+
+extern "C" rf_status rf_load_positions_txt(const char* path, float* R, uint64_t cap, uint64_t* n) {
+    if (!path || !n) { rf::set_error("rf_load_positions_txt: bad arguments"); return RF_ERR_INVALID; }
+    std::ifstream f(path, std::ios::in);
+    if (!f) { rf::set_error("rf_load_positions_txt: cannot open %s", path); return RF_ERR_INVALID; }
+    uint64_t m = 0;
+    if (!(f >> m)) { rf::set_error("rf_load_positions_txt: %s has no particle count", path); return RF_ERR_INVALID; }
+    *n = m;
+    if (!R) return RF_OK;
+    if (cap < m) { rf::set_error("rf_load_positions_txt: capacity %llu < %llu particles", (unsigned long long)cap, (unsigned long long)m); return RF_ERR_CAPACITY; }
+    const double lc = 1.0 / 1e-3;
+    for (uint64_t i = 0; i < m; ++i) {
+        double x, y, z;
+        if (!(f >> x >> y >> z)) { rf::set_error("rf_load_positions_txt: %s ends at particle %llu", path, (unsigned long long)i); return RF_ERR_INVALID; }
+        R[i] = (float)(x * lc);
+        R[i + m] = (float)(y * lc);
+        R[i + 2 * m] = (float)(z * lc);
+    }
+    return RF_OK;
+}

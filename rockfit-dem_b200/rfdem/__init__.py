@@ -159,6 +159,8 @@ _proto = {
     "rf_engine_destroy": (i32, [P]),
     "rf_engine_step": (i32, [P, u64]),
     "rf_engine_affine_strain": (i32, [P, C.POINTER(C.c_double)]),
+    "rf_save_positions_txt": (i32, [C.c_char_p, P, u64]),
+    "rf_load_positions_txt": (i32, [C.c_char_p, P, u64, C.POINTER(u64)]),
     "rf_engine_step_host": (i32, [P, P, u64, P]),
     "rf_engine_sync": (i32, [P, C.POINTER(Task), C.POINTER(RunResult)]),
     "rf_engine_export": (i32, [P] + [P] * 10),
@@ -682,3 +684,18 @@ def save_lammps_data(path, task, st, with_energy=True):
                                   ptr(np.ascontiguousarray(st["IL"], ID_NP)),
                                   ptr(np.ascontiguousarray(st["ILtype"], np.uint8)), 1 if with_energy else 0),
           "rf_save_lammps_data")
+
+
+def save_positions_txt(path, R):
+    """The reference's position text file (SaveParticleDATAtxt) of planar float32 R (mm)."""
+    R = np.ascontiguousarray(R, np.float32)
+    check(lib.rf_save_positions_txt(os.fsencode(path), R.ctypes.data, R.size // 3), "rf_save_positions_txt")
+
+
+def load_positions_txt(path):
+    """Positions of a reference position text file (LoadParticleDATAtxt), planar float32 (mm)."""
+    n = C.c_uint64(0)
+    check(lib.rf_load_positions_txt(os.fsencode(path), None, 0, C.byref(n)), "rf_load_positions_txt")
+    R = np.zeros(3 * n.value, np.float32)
+    check(lib.rf_load_positions_txt(os.fsencode(path), R.ctypes.data, n.value, C.byref(n)), "rf_load_positions_txt")
+    return R

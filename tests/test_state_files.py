@@ -113,3 +113,22 @@ def test_state_file_error_paths(tmp_path):
         rfdem.Engine.restore(str(good))                        # a dump, not a checkpoint
     with pytest.raises(rfdem.RFError):
         rfdem.Engine.restore(str(tmp_path / "missing.ckpt"))
+
+
+def test_position_text_matches_the_reference_format(rfdem, tmp_path):
+    """rf_save_positions_txt writes SaveParticleDATAtxt's text (md_createcylindersample.cu:104-114):
+    the count, then x y z in metres -- float mm times the length unit 1e-3 as doubles in the
+    stream's default format, which is C's %g at 6 significant digits -- and
+    rf_load_positions_txt reads it back as LoadParticleDATAtxt does (x / 1e-3 to float)."""
+    t, R = rfdem.make_test(rfdem.RF_TEST_UNIAXIAL, 9.0, 14.0, seed=0xB2000000 + 61)
+    n = R.size // 3
+    path = tmp_path / "Sample_0.txt"
+    rfdem.save_positions_txt(str(path), R)
+    lines = [str(n)] + ["%g %g %g" % tuple(float(v) * 1e-3 for v in (R[i], R[i + n], R[i + 2 * n]))
+                        for i in range(n)]
+    assert path.read_text() == "\n".join(lines) + "\n"
+    back = rfdem.load_positions_txt(str(path))
+    want = np.array([float(w) for line in lines[1:] for w in line.split()], np.float64).reshape(n, 3).T
+    assert np.array_equal(back, (want * (1.0 / 1e-3)).astype(np.float32).reshape(-1))
+    # six digits: the round trip moves a coordinate by at most half a unit of the sixth digit
+    assert np.max(np.abs(back - R) / np.maximum(np.abs(R), 1e-3)) < 5.1e-6

@@ -44,6 +44,9 @@
 #ifndef RF_GRAPH_UNROLL
 #define RF_GRAPH_UNROLL 8         // explicit steps per iteration of the graph's WHILE loop
 #endif
+#ifndef RF_REBUILD_EACH_STEP_N
+#define RF_REBUILD_EACH_STEP_N (1u << 20)   // from this many particles the rebuild condition is evaluated every step
+#endif
 
 namespace rf {
 
@@ -2092,13 +2095,16 @@ rf_status build_graph(rf_engine* e) {
     cudaGraphNode_t wnode;
     RF_CUDA(cudaGraphAddNode(&wnode, g, &pro, 1, &wp));
     cudaGraph_t body = wp.conditional.phGraph_out[0];
-    // The loop body is IF(rebuild) {rebuild kernels} followed by RF_GRAPH_UNROLL steps: the
-    // WHILE condition and the rebuild condition are evaluated once per RF_GRAPH_UNROLL
-    // steps (conditional nodes cost more than the kernels between them). The rebuild
-    // trigger is set at 0.3 of the skin so that the particles' motion over those steps
-    // stays within the 0.5 skin the candidate lists are complete for; a step that finds
-    // a particle beyond 0.5 skin reports RF_ERR_CAPACITY. A step whose step count has
-    // reached the target returns at once, so the target is kept exactly.
+    // The loop body is RF_GRAPH_UNROLL steps, each preceded by IF(rebuild) {rebuild
+    // kernels} or, for specimens below RF_REBUILD_EACH_STEP_N particles, only the first:
+    // there a conditional node costs as much as a few percent of a step, and the rebuild
+    // condition is evaluated once per RF_GRAPH_UNROLL steps. The rebuild trigger is set at
+    // 0.3 of the skin so that the particles' motion until the next evaluation stays within
+    // the 0.5 skin the candidate lists are complete for; a step that finds a particle beyond
+    // 0.5 skin reports RF_ERR_CAPACITY. Evaluating before every step lets particles move 0.2
+    // skin per step (fragments of a damaged large specimen), against 0.2 skin per
+    // RF_GRAPH_UNROLL steps otherwise. The WHILE condition is evaluated once per body. A step
+    // whose step count has reached the target returns at once, so the target is kept exactly.
     const unsigned gN = (e->c.N + 255) / 256;
     const unsigned gC = (e->c.cg_cells + 1 + 255) / 256;
     struct { void* fn; unsigned grid, block; } seq[] = {
@@ -2107,24 +2113,28 @@ rf_status build_graph(rf_engine* e) {
         {(void*)k_rb_scan_apply, e->cg_nb, 1024}, {(void*)k_rb_scatter, gN, 256},
         {(void*)k_rb_cand, (e->c.N + 127) / 128, 128},
     };
-    cudaGraphNodeParams ip = {};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = e->c.h_rebuild;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    cudaGraphNode_t inode;
-    RF_CUDA(cudaGraphAddNode(&inode, body, nullptr, 0, &ip));
-    cudaGraph_t rb = ip.conditional.phGraph_out[0];
-    cudaGraphNode_t prev = nullptr;
-    for (auto& q : seq) {
-        cudaGraphNode_t n;
-        kp = kparams(q.fn, q.grid, q.block);
-        RF_CUDA(cudaGraphAddKernelNode(&n, rb, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
-        prev = n;
-    }
+    const int every = e->c.N >= RF_REBUILD_EACH_STEP_N ? 1 : RF_GRAPH_UNROLL;
     void* fn = step_kernel(e);
-    cudaGraphNode_t last = inode;
+    cudaGraphNode_t last = nullptr;
     for (int u = 0; u < RF_GRAPH_UNROLL; ++u) {
+        if (u % every == 0) {
+            cudaGraphNodeParams ip = {};
+            ip.type = cudaGraphNodeTypeConditional;
+            ip.conditional.handle = e->c.h_rebuild;
+            ip.conditional.type = cudaGraphCondTypeIf;
+            ip.conditional.size = 1;
+            cudaGraphNode_t inode;
+            RF_CUDA(cudaGraphAddNode(&inode, body, last ? &last : nullptr, last ? 1 : 0, &ip));
+            cudaGraph_t rb = ip.conditional.phGraph_out[0];
+            cudaGraphNode_t prev = nullptr;
+            for (auto& q : seq) {
+                cudaGraphNode_t n;
+                kp = kparams(q.fn, q.grid, q.block);
+                RF_CUDA(cudaGraphAddKernelNode(&n, rb, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
+                prev = n;
+            }
+            last = inode;
+        }
         cudaGraphNode_t step;
         kp = kparams(fn, e->nblocks, 128);
         RF_CUDA(cudaGraphAddKernelNode(&step, body, &last, 1, &kp));

@@ -916,6 +916,10 @@ struct RunExt {
     std::vector<id_t> IL, CI, CIs, pnC;
     std::vector<uint8_t> type;
     std::vector<V3<TF>> Rij, Oijt, Mijn, Mijt;
+    // tangential overlap of the contact an overlapping bonded pair carries in parallel with
+    // its bond (the extended model; the reference constants have none); it becomes the
+    // slot's contact state (Oijt) when the bond breaks
+    std::vector<V3<TF>> Ocb;
     // bond state at the start of a quasi-static increment; during the increment's FIRE
     // iterations (qs_total) a bond's state is computed from it and the motion since then
     std::vector<V3<TF>> Rij0, Oijt0, Mijn0, Mijt0;
@@ -948,7 +952,7 @@ struct RunExt {
         return aa_farcut;
     }
     void zero_slot(uint64_t k) {
-        Rij[k] = {0, 0, 0}; Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0};
+        Rij[k] = {0, 0, 0}; Oijt[k] = {0, 0, 0}; Mijn[k] = {0, 0, 0}; Mijt[k] = {0, 0, 0}; Ocb[k] = {0, 0, 0};
     }
 
     void init(const double* R0, const double* r0) {
@@ -961,7 +965,7 @@ struct RunExt {
         V.assign(3 * N, 0); W.assign(3 * N, 0);
         IL.assign(N * K, EMPTY); type.assign(N * K, 0); L0.assign(N * K, 1.0); sig.assign(N * K, 0.0);
         tau.assign(N * K, 0.0); iL0.assign(N * K, (TF)0);
-        Rij.assign(N * K, {0, 0, 0}); Oijt = Rij; Mijn = Rij; Mijt = Rij;
+        Rij.assign(N * K, {0, 0, 0}); Oijt = Rij; Mijn = Rij; Mijt = Rij; Ocb = Rij;
         CI.assign(N, 0); CIs.assign(2 * N, 0); pnC.assign(2 * CN, 0);
         sz0 = t->sz0 != 0.0 ? t->sz0 : (double)t->Compress.size.z;
         status = 0; steps = 0; broken = 0;
@@ -1322,6 +1326,7 @@ struct RunExt {
             const TF ri = (TF)rad[i];
             const TF mi = cmass * ri * ri * ri;
             V3<TF> fsb = {0, 0, 0}, msb = {0, 0, 0}, fsc = {0, 0, 0}, msc = {0, 0, 0};
+            uint32_t pc = 0;                                     // slots whose contact the bond pass took
             for (uint64_t q = 0; q < K; ++q) {                   // _22 order: bonds by slot
                 const uint64_t k = i * K + q;
                 const id_t j = IL[k];
@@ -1349,11 +1354,26 @@ struct RunExt {
                 }
                 if (broke) { type[k] = 0; ++broken; }
                 npair += 1;
+                // the contact an overlapping bonded pair carries in parallel with the bond, its
+                // overlap counted from min(r_i + r_j, L0) (explicit steps only: inside a FIRE
+                // increment its state would depend on the path)
+                const double sr = std::fmin(rad[i] + rad[j], L0[k]);
+                if (!x.ref && !in_fire && d2 < sr * sr) {
+                    const TF rj = (TF)rad[j];
+                    std::swap(Oijt[k], Ocb[k]);
+                    contact(k, r, d2, sr, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsb, msb, fnb, ktb, krb);
+                    std::swap(Oijt[k], Ocb[k]);
+                    npair += 1;
+                    pc |= 1u << q;
+                } else {
+                    Ocb[k] = {0, 0, 0};
+                }
+                if (broke) Oijt[k] = Ocb[k];                     // the slot goes on as that contact
             }
             for (uint64_t q = 0; q < K; ++q) {                   // _21 order: type-0 slots by slot
                 const uint64_t k = i * K + q;
                 const id_t j = IL[k];
-                if (j == EMPTY || type[k] != 0) continue;
+                if (j == EMPTY || type[k] != 0 || ((pc >> q) & 1u)) continue;
                 const double dx = R[j] - R[i], dy = R[j + N] - R[i + N], dz = R[j + 2 * N] - R[i + 2 * N];
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 const TF rj = (TF)rad[j];

@@ -1117,6 +1117,12 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
 
     f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
     uint32_t nbroken = 0;
+    const uint32_t* row = d.ids + (size_t)i * c.K;
+    const float* oin = d.cO[cur] + (size_t)i * c.K * 3;
+    float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
+    // bond slots whose pair overlaps: their contact (in parallel with the bond) was taken
+    // in the bond pass, with its tangential overlap kept in the slot's contact state
+    uint32_t pc = 0;
     {
         const uint32_t wb = __reduce_or_sync(FULL, bmask);
         const uint32_t qend = 32u - __clz(wb);
@@ -1169,19 +1175,33 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
             d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
             d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
-            if (broke) { bmask &= ~(1u << q); bond &= ~(1u << d.bk[s]); ++nbroken; }
+            const uint32_t k = d.bk[s];
+            if (broke) { bmask &= ~(1u << q); bond &= ~(1u << k); ++nbroken; }
+            // parallel contact (extended model, explicit steps): an overlapping bonded pair also
+            // carries the Hertz-Mindlin contact, and a broken bond's slot keeps that contact's
+            // state. Its overlap counts from min(r_i + r_j, L0), so a bond formed between
+            // overlapping particles is force-free at its rest length. FIRE relaxation leaves
+            // it out: its state would depend on the path.
+            const double sr = fmin(xi.w + xj.w, L0);
+            if (MODE == 0 && !c.ref_mode && rr < sr * sr) {
+                const uint32_t bit = 1u << k;
+                const float rj = (float)xj.w;
+                f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
+                contact_pair_ext(ep, r, rr, sr, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(vj), wi, f4to3(wj), o,
+                                 fsb, msb, fnabs, kt, kr);
+                ++npair;
+                oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
+                pc |= bit;
+            }
         }
     }
 
-    const uint32_t* row = d.ids + (size_t)i * c.K;
-    const float* oin = d.cO[cur] + (size_t)i * c.K * 3;
-    float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
     f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
     uint32_t cm_out = 0;
     float fnc = 0.f, ktc = 0.f, krc = 0.f;   // contact force magnitudes and stiffness (recounted on a replay)
     uint32_t npc = 0;
     auto contact_pass = [&](bool with_delete) {
-        uint32_t m = live & ~bond;
+        uint32_t m = live & ~bond & ~pc;
         while (m) {
             const uint32_t k = __ffs(m) - 1;
             m &= m - 1;
@@ -1250,7 +1270,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         fsc = mk3(0.f, 0.f, 0.f); msc = fsc; cm_out = 0; fnc = 0.f; ktc = 0.f; krc = 0.f; npc = 0;
         contact_pass(false);
     }
-    cm = cm_out;
+    cm = cm_out | pc;
     fnabs += fnc;
     npair += npc;
     kt += ktc;

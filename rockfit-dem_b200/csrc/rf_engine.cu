@@ -2091,21 +2091,38 @@ rf_status build_graph(rf_engine* e) {
     cudaGraph_t g;
     RF_CUDA(cudaGraphCreate(&g, 0));
     e->graph = g;
+    // The loop body is RF_GRAPH_UNROLL steps, each preceded by IF(rebuild) {rebuild
+    // kernels} or, for specimens below RF_REBUILD_EACH_STEP_N particles, only the first:
+    // there a conditional node costs as much as a few percent of a step, and the rebuild
+    // condition is evaluated once per RF_GRAPH_UNROLL steps. The rebuild trigger is set at
+    // 0.3 of the skin so that the particles' motion until the next evaluation stays within
+    // the 0.5 skin the candidate lists are complete for; a step that finds a particle beyond
+    // 0.5 skin reports RF_ERR_CAPACITY. Evaluating before every step lets particles move 0.2
+    // skin per step (fragments of a damaged large specimen), against 0.2 skin per
+    // RF_GRAPH_UNROLL steps otherwise. Each IF node has its own conditional handle (a handle
+    // drives one conditional node); a step node's parameters carry the handle of the IF
+    // node after it (the last step's: the body's first IF, evaluated on the next iteration),
+    // the prologue's the first. The WHILE condition is evaluated once per body. A step
+    // whose step count has reached the target returns at once, so the target is kept exactly.
+    const int every = e->c.N >= RF_REBUILD_EACH_STEP_N ? 1 : RF_GRAPH_UNROLL;
+    const int nif = RF_GRAPH_UNROLL / every;
+    cudaGraphConditionalHandle hif[RF_GRAPH_UNROLL];
     RF_CUDA(cudaGraphConditionalHandleCreate(&e->c.h_loop, g, 0, 0));
-    RF_CUDA(cudaGraphConditionalHandleCreate(&e->c.h_rebuild, g, 0, 0));
+    for (int q = 0; q < nif; ++q) RF_CUDA(cudaGraphConditionalHandleCreate(&hif[q], g, 0, 0));
+    e->c.h_rebuild = hif[0];
     e->c.use_graph = 1;
     Dev d = e->d;
     Consts c = e->c;
     void* args[] = {&d, &c};
-    auto kparams = [&](void* fn, unsigned grid, unsigned block) {
+    auto kparams = [&](void* fn, unsigned grid, unsigned block, void** a) {
         cudaKernelNodeParams kp = {};
         kp.func = fn; kp.gridDim = dim3(grid); kp.blockDim = dim3(block);
-        kp.sharedMemBytes = 0; kp.kernelParams = args; kp.extra = nullptr;
+        kp.sharedMemBytes = 0; kp.kernelParams = a; kp.extra = nullptr;
         return kp;
     };
     // prologue -> WHILE
     cudaGraphNode_t pro;
-    cudaKernelNodeParams kp = kparams((void*)k_prologue, 1, 32);
+    cudaKernelNodeParams kp = kparams((void*)k_prologue, 1, 32, args);
     RF_CUDA(cudaGraphAddKernelNode(&pro, g, nullptr, 0, &kp));
     cudaGraphNodeParams wp = {};
     wp.type = cudaGraphNodeTypeConditional;
@@ -2115,16 +2132,6 @@ rf_status build_graph(rf_engine* e) {
     cudaGraphNode_t wnode;
     RF_CUDA(cudaGraphAddNode(&wnode, g, &pro, 1, &wp));
     cudaGraph_t body = wp.conditional.phGraph_out[0];
-    // The loop body is RF_GRAPH_UNROLL steps, each preceded by IF(rebuild) {rebuild
-    // kernels} or, for specimens below RF_REBUILD_EACH_STEP_N particles, only the first:
-    // there a conditional node costs as much as a few percent of a step, and the rebuild
-    // condition is evaluated once per RF_GRAPH_UNROLL steps. The rebuild trigger is set at
-    // 0.3 of the skin so that the particles' motion until the next evaluation stays within
-    // the 0.5 skin the candidate lists are complete for; a step that finds a particle beyond
-    // 0.5 skin reports RF_ERR_CAPACITY. Evaluating before every step lets particles move 0.2
-    // skin per step (fragments of a damaged large specimen), against 0.2 skin per
-    // RF_GRAPH_UNROLL steps otherwise. The WHILE condition is evaluated once per body. A step
-    // whose step count has reached the target returns at once, so the target is kept exactly.
     const unsigned gN = (e->c.N + 255) / 256;
     const unsigned gC = (e->c.cg_cells + 1 + 255) / 256;
     struct { void* fn; unsigned grid, block; } seq[] = {
@@ -2133,14 +2140,17 @@ rf_status build_graph(rf_engine* e) {
         {(void*)k_rb_scan_apply, e->cg_nb, 1024}, {(void*)k_rb_scatter, gN, 256},
         {(void*)k_rb_cand, (e->c.N + 127) / 128, 128},
     };
-    const int every = e->c.N >= RF_REBUILD_EACH_STEP_N ? 1 : RF_GRAPH_UNROLL;
     void* fn = step_kernel(e);
+    // per step node: Consts with the handle of the IF node that follows it (node parameters
+    // are copied when the node is added, so one slot per step suffices until then)
+    Consts cs[RF_GRAPH_UNROLL];
+    void* sargs[RF_GRAPH_UNROLL][2];
     cudaGraphNode_t last = nullptr;
     for (int u = 0; u < RF_GRAPH_UNROLL; ++u) {
         if (u % every == 0) {
             cudaGraphNodeParams ip = {};
             ip.type = cudaGraphNodeTypeConditional;
-            ip.conditional.handle = e->c.h_rebuild;
+            ip.conditional.handle = hif[u / every];
             ip.conditional.type = cudaGraphCondTypeIf;
             ip.conditional.size = 1;
             cudaGraphNode_t inode;
@@ -2149,14 +2159,18 @@ rf_status build_graph(rf_engine* e) {
             cudaGraphNode_t prev = nullptr;
             for (auto& q : seq) {
                 cudaGraphNode_t n;
-                kp = kparams(q.fn, q.grid, q.block);
+                kp = kparams(q.fn, q.grid, q.block, args);
                 RF_CUDA(cudaGraphAddKernelNode(&n, rb, prev ? &prev : nullptr, prev ? 1 : 0, &kp));
                 prev = n;
             }
             last = inode;
         }
+        cs[u] = c;
+        cs[u].h_rebuild = hif[((u + 1) / every) % nif];
+        sargs[u][0] = &d;
+        sargs[u][1] = &cs[u];
         cudaGraphNode_t step;
-        kp = kparams(fn, e->nblocks, 128);
+        kp = kparams(fn, e->nblocks, 128, sargs[u]);
         RF_CUDA(cudaGraphAddKernelNode(&step, body, &last, 1, &kp));
         last = step;
     }

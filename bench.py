@@ -196,7 +196,10 @@ def ext_specimen(rfdem, N, seed, dist, rmin, rmax):
     R0, rad, D, H, mo = rfdem.pack_cylinder(N, R0_MM, rmin=rmin, rmax=rmax, aspect=ASPECT, phi=PHI, seed=seed,
                                             dist=dist)
     v = -0.1 * H * 1e-6                        # strain rate 0.1/s in mm per microsecond
-    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, R0_MM, dt=0.01, v_load=v, max_strain=1.0)
+    # the reference's fracture stop (stress above MinStress, then below ZeroStress) is kept
+    # out of reach: a timed window is a fixed number of steps of the damaged specimen
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, R0_MM, dt=0.01, v_load=v, max_strain=1.0,
+                               min_stress=1e30)
     return t, R, rad, D, H
 
 
@@ -546,7 +549,7 @@ def cpu_port_sample(rfdem, t, x, R, rad, prestrain):
     a, b = sample_block(N)
     Rb = np.ascontiguousarray(R.reshape(3, N)[:, a:b]).reshape(-1)
     ts, Rs = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, Rb, rad[a:b], R0_MM, dt=0.01, v_load=float(t.Compress.VLoad),
-                                 max_strain=1.0)
+                                 max_strain=1.0, min_stress=1e30)
     threads = os.cpu_count() or 1
     secs, n = oracle.time_ext(rfdem.Task.from_buffer_copy(ts), x, Rs, rad[a:b], 2, threads, prestrain)
     steps = max(2, min(200, int(15.0 / max(secs / 2, 1e-3))))

@@ -1192,6 +1192,8 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                 ++npair;
                 oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
                 pc |= bit;
+            } else {
+                cm &= ~(1u << k);      // not in contact: the parallel contact's state ends here
             }
         }
     }

@@ -218,7 +218,7 @@ def run_explicit(rfdem, torch, t, R, rad, x, args, dist):
     stream = torch.cuda.ExternalStream(e.stream())
     if any(args.prestrain):
         e.affine_strain(*args.prestrain)
-    tuned = e.autotune(200)            # trial steps on a snapshot, state restored
+    tuned = e.autotune(200) if not args.no_autotune else (0, [0.0, 0.0, 0.0])   # trials on a snapshot
     for _ in range(args.warmup):
         e.step(S)
     torch.cuda.synchronize()
@@ -717,6 +717,7 @@ def main():
     ap.add_argument("--explicit-steps", type=int, default=STEPS_PER_BENCH_STEP,
                     help="explicit steps per bench step (profiling runs use fewer)")
     ap.add_argument("--no-reference-model", action="store_true", help="skip the reference-model line")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default step variant (profiling runs)")
     ap.add_argument("--particles", type=int, default=N_PARTICLES, help="particles of the benchmark specimen")
     ap.add_argument("--radii", default=RADII, choices=["uniform", "log-uniform"])
     ap.add_argument("--rmin", type=float, default=None, help="smallest radius / 0.25 mm (0.5; 0.8 uniform)")

@@ -1217,8 +1217,9 @@ struct RunExt {
     }
 
     // One overlapping pair (engine contact_pair_ext): rr = |r|^2 and sr = r_i + r_j in
-    // double with rr < sr^2; the overlap is (sr^2 - rr) / (sr + |r|).
-    void contact(uint64_t k, const V3<TF>& r, double rr, double sr, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
+    // double with rr < sr^2; the overlap is (sr^2 - rr) / (sr + |r|). Returns true when the
+    // zero-spin rule of the rolling resistance cleared the moment sum ms.
+    bool contact(uint64_t k, const V3<TF>& r, double rr, double sr, TF ri, TF rj, TF mi, TF mj, const V3<TF>& vi,
                  const V3<TF>& vj, const V3<TF>& wi, const V3<TF>& wj, V3<TF>& fs, V3<TF>& ms, TF& fnabs, TF& kt,
                  TF& kr) {
         const TF rijm = len_sq(rr);
@@ -1275,8 +1276,10 @@ struct RunExt {
                 ms.x = fm(wi.x, cr, ms.x); ms.y = fm(wi.y, cr, ms.y); ms.z = fm(wi.z, cr, ms.z);
             } else {
                 ms = {0, 0, 0};    // QUIRK (md_calculateforcesdem3.cu:316-336): clears the contact sum
+                return true;
             }
         }
+        return false;
     }
 
     bool running() const { return t->Compress.Strain < t->Compress.MaxStrain && !t->Compress.Fracture; }
@@ -1336,7 +1339,12 @@ struct RunExt {
                 const V3<TF> r = {(TF)dx, (TF)dy, (TF)dz};
                 const V3<TF> vj = {V[j], V[j + N], V[j + 2 * N]}, wj = {W[j], W[j + N], W[j + 2 * N]};
                 const TF br = x.ref ? b_r : lambda * std::min(ri, (TF)rad[j]);
-                bool broke;
+                // the record's force, moment and float sums are formed from zero and then
+                // added to the particle's, record by record (the engine hands each record
+                // from the lane that evaluates it to the particle's lane)
+                V3<TF> fr = {0, 0, 0}, mr = {0, 0, 0};
+                TF fnr = 0, ktr = 0, krr = 0;
+                bool broke, clear = false;
                 if (qs_total) {
                     // the pair's relative displacement since the increment began, formed in
                     // double as (r - r0) so that it keeps its own precision (a difference of
@@ -1348,9 +1356,9 @@ struct RunExt {
                     const V3<TF> du = {(TF)(dx - (X0[j] - X0[i]) - (hy * dz - hz * dy)),
                                        (TF)(dy - (X0[j + N] - X0[i + N]) - (hz * dx - hx * dz)),
                                        (TF)(dz - (X0[j + 2 * N] - X0[i + 2 * N]) - (hx * dy - hy * dx))};
-                    broke = bond_total(k, r, d2, du, ti, tj, br, fsb, msb, fnb, ktb, krb);
+                    broke = bond_total(k, r, d2, du, ti, tj, br, fr, mr, fnr, ktr, krr);
                 } else {
-                    broke = bond(k, r, d2, vi, vj, wi, wj, br, fsb, msb, fnb, ktb, krb);
+                    broke = bond(k, r, d2, vi, vj, wi, wj, br, fr, mr, fnr, ktr, krr);
                 }
                 if (broke) { type[k] = 0; ++broken; }
                 npair += 1;
@@ -1361,7 +1369,8 @@ struct RunExt {
                 if (!x.ref && !in_fire && d2 < sr * sr) {
                     const TF rj = (TF)rad[j];
                     std::swap(Oijt[k], Ocb[k]);
-                    contact(k, r, d2, sr, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fsb, msb, fnb, ktb, krb);
+                    clear = contact(k, r, d2, sr, ri, rj, mi, cmass * rj * rj * rj, vi, vj, wi, wj, fr, mr, fnr, ktr,
+                                    krr);
                     std::swap(Oijt[k], Ocb[k]);
                     npair += 1;
                     pc |= 1u << q;
@@ -1369,6 +1378,10 @@ struct RunExt {
                     Ocb[k] = {0, 0, 0};
                 }
                 if (broke) Oijt[k] = Ocb[k];                     // the slot goes on as that contact
+                fsb.x += fr.x; fsb.y += fr.y; fsb.z += fr.z;
+                if (clear) msb = {0, 0, 0};                      // the zero-spin rule clears the moment sum
+                else { msb.x += mr.x; msb.y += mr.y; msb.z += mr.z; }
+                fnb += fnr; ktb += ktr; krb += krr;
             }
             for (uint64_t q = 0; q < K; ++q) {                   // _21 order: type-0 slots by slot
                 const uint64_t k = i * K + q;

@@ -44,6 +44,12 @@
 #ifndef RF_GRAPH_UNROLL
 #define RF_GRAPH_UNROLL 8         // explicit steps per iteration of the graph's WHILE loop
 #endif
+// outcome of one bond record, handed by the lane that evaluated it to its particle's lane
+// (bits 8-12: the record's row slot)
+#define RF_REC_DELETE 1u          // beyond the bond's keep distance: the slot is deleted (partner id in the force word)
+#define RF_REC_BROKE 2u           // the bond broke this step
+#define RF_REC_PARALLEL 4u        // the pair overlaps: the slot's contact was taken with the bond
+#define RF_REC_CLEAR 8u           // that contact's zero-spin rule cleared the particle's moment sum
 #ifndef RF_REBUILD_EACH_STEP_N
 #define RF_REBUILD_EACH_STEP_N (1u << 20)   // from this many particles the rebuild condition is evaluated every step
 #endif
@@ -1099,104 +1105,171 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     float fnabs = 0.f, kt = 0.f, kr = 0.f;
     uint32_t npair = 0;
 
-    double4 xi = make_double4(0, 0, 0, 1);
-    f3 vi = mk3(0.f, 0.f, 0.f), wi = vi;
     uint32_t live = 0, bond = 0, cm = 0, nbq = 0, bmask = 0, ncand = 0;
     unsigned long long mem = 0ull;
     if (valid) {
-        xi = P[i]; vi = f4to3(Vv[i]); wi = f4to3(Wv[i]);
         live = d.live[i]; bond = d.bond[i]; cm = d.cmask[i];
         mem = d.member[i]; ncand = d.cand_n[i];
         nbq = d.nbq[i]; bmask = d.bmask[i];
     }
-    const float ri = (float)xi.w;
-    const float mi = c.cmass * ri * ri * ri;
     const uint32_t live0 = live, bond0 = bond, cm0 = cm, bmask0 = bmask;
     const unsigned long long mem0 = mem;
     const size_t QN = (size_t)d.QB * N;
 
     f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
     uint32_t nbroken = 0;
-    const uint32_t* row = d.ids + (size_t)i * c.K;
-    const float* oin = d.cO[cur] + (size_t)i * c.K * 3;
-    float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
     // bond slots whose pair overlaps: their contact (in parallel with the bond) was taken
     // in the bond pass, with its tangential overlap kept in the slot's contact state
     uint32_t pc = 0;
     {
-        const uint32_t wb = __reduce_or_sync(FULL, bmask);
-        const uint32_t qend = 32u - __clz(wb);
-        // every load of a record is issued before the partner's gathers and the far-link
-        // test, so a record waits for two dependent latencies (id -> partner state), not three.
-        // FIRE mode reads the records' increment-start state and the motion since then.
-        const float4* src = MODE == 1 ? d.bst0 : d.bst;
-        double4 xi0 = xi, ri0 = make_double4(0, 0, 0, 0);
-        if (MODE == 1 && valid) { xi0 = d.x0[i]; ri0 = d.rot[i]; }
+        // Bond records, spread over the warp. The warp's active records are listed
+        // ordinal-major (every particle's first record, then every second one, ...; lane
+        // order within an ordinal), so consecutive lanes read consecutive entries of the
+        // [QB][N] record arrays, and in each round every lane takes one record whatever the
+        // 32 particles' bond counts. The lane that takes a record forms its force, moment
+        // and outcome from zero and hands them to the particle's lane through shared
+        // memory; the particle adds them in record order. FIRE mode reads the records'
+        // increment-start state and the motion since then.
+        constexpr int NO = MODE == 1 ? 10 : 7;        // words of one record's result
+        __shared__ float s_res[4][NO][32];
+        __shared__ uint32_t s_q0[4][32], s_qb[4][32];  // per ordinal: first list entry, lanes holding one
+        extern __shared__ __align__(16) unsigned char rf_step_smem[];
+        const uint32_t lane = threadIdx.x & 31u, wp = threadIdx.x >> 5;
+        const uint32_t lt = (1u << lane) - 1u;
+        const uint32_t wbase = i - lane;
+        uint16_t* lst = reinterpret_cast<uint16_t*>(rf_step_smem) + (size_t)wp * 32u * d.QB;
+        const uint32_t qend = 32u - __clz(__reduce_or_sync(FULL, bmask));
+        uint32_t T = 0;
         for (uint32_t q = 0; q < qend; ++q) {
-            if (!((bmask >> q) & 1u)) continue;
-            const size_t s = (size_t)q * N + i;
-            const uint32_t j = __ldg(&d.bj[s]);
-            const float4 s0 = src[s], s1 = src[s + QN], s2 = src[s + 2 * QN];
-            const float2 str = __ldg(&d.bstr[s]);
-            const double L0 = __ldg(&d.bL0[s]);
-            const double4 xj = ldg_d4(&P[j]);
-            const float4 vj = __ldg(&Vv[j]), wj = __ldg(&Wv[j]);
-            const double3 rd = dsub(xj, xi);
-            const double rr = dlen2(rd);
-            if (rr > bond_cut2_del(c, xi.w, xj.w, L0) || rr < 1e-10) {
-                delete_slot(d, c, i, d.bk[s], j, ncand, nbq, live, bond, cm, bmask, mem);
-                continue;
+            const bool has = (bmask >> q) & 1u;
+            const uint32_t bal = __ballot_sync(FULL, has);
+            if (has) lst[T + __popc(bal & lt)] = (uint16_t)(lane | (q << 5));
+            if (lane == q) { s_q0[wp][q] = T; s_qb[wp][q] = bal; }
+            T += __popc(bal);
+        }
+        __syncwarp();
+        const float4* src = MODE == 1 ? d.bst0 : d.bst;
+        uint32_t rem = bmask;                          // this particle's records not yet added
+        for (uint32_t base = 0; base < T; base += 32u) {
+            const uint32_t p = base + lane;
+            const uint32_t e = p < T ? (uint32_t)lst[p] : lane;
+            const uint32_t ol = e & 31u;
+            const uint32_t cmo = __shfl_sync(FULL, cm0, ol);   // the record's particle's step-start contacts
+            if (p < T) {
+                const uint32_t q = e >> 5, io = wbase + ol;
+                const size_t s = (size_t)q * N + io;
+                // every load of the record is issued before the partner's gathers
+                const uint32_t j = __ldg(&d.bj[s]);
+                const float4 s0 = src[s], s1 = src[s + QN], s2 = src[s + 2 * QN];
+                const float2 str = __ldg(&d.bstr[s]);
+                const double L0 = __ldg(&d.bL0[s]);
+                const uint32_t k = d.bk[s];
+                const double4 xo = ldg_d4(&P[io]);
+                const double4 xj = ldg_d4(&P[j]);
+                const float4 vj = __ldg(&Vv[j]), wj = __ldg(&Wv[j]);
+                const double3 rd = dsub(xj, xo);
+                const double rr = dlen2(rd);
+                uint32_t fl = k << 8;
+                f3 fr = mk3(0.f, 0.f, 0.f), mr = fr;
+                float fnr = 0.f, ktr = 0.f, krr = 0.f;
+                if (rr > bond_cut2_del(c, xo.w, xj.w, L0) || rr < 1e-10) {
+                    fl |= RF_REC_DELETE;
+                    fr.x = __uint_as_float(j);
+                } else {
+                    const float ro = (float)xo.w;
+                    BondExt b;
+                    b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ro, (float)xj.w);
+                    b.sc = str.x; b.tc = str.y; b.L0 = L0;
+                    if (MODE == 0 && c.ref_mode) {
+                        const float il = __ldg(&d.bil[s]);
+                        b.kn = c.refE * il; b.ks = c.refG * il; b.br = c.ref_br;
+                    }
+                    const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
+                    f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
+                    f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
+                    f3 vo = mk3(0.f, 0.f, 0.f), wo = vo;
+                    bool broke;
+                    if (MODE == 1) {
+                        const double4 xi0 = ldg_d4(&d.x0[io]), ri0 = ldg_d4(&d.rot[io]);
+                        const double4 xj0 = ldg_d4(&d.x0[j]), rj0 = ldg_d4(&d.rot[j]);
+                        const double hx = 0.5 * (ri0.x + rj0.x), hy = 0.5 * (ri0.y + rj0.y), hz = 0.5 * (ri0.z + rj0.z);
+                        const f3 du = mk3((float)(rd.x - (xj0.x - xi0.x) - (hy * rd.z - hz * rd.y)),
+                                          (float)(rd.y - (xj0.y - xi0.y) - (hz * rd.x - hx * rd.z)),
+                                          (float)(rd.z - (xj0.z - xi0.z) - (hx * rd.y - hy * rd.x)));
+                        broke = bond_slot_ext_total(b, r, rr, du, mk3((float)ri0.x, (float)ri0.y, (float)ri0.z),
+                                                    mk3((float)rj0.x, (float)rj0.y, (float)rj0.z), rij, oijt, mijn,
+                                                    mijt, rij, oijt, mijn, mijt, fr, mr, fnr, ktr, krr);
+                    } else {
+                        vo = f4to3(__ldg(&Vv[io])); wo = f4to3(__ldg(&Wv[io]));
+                        broke = bond_slot_ext(ep, b, r, rr, vo, f4to3(vj), wo, f4to3(wj), rij, oijt, mijn, mijt, fr,
+                                              mr, fnr, ktr, krr, c.ref_mode != 0);
+                    }
+                    d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
+                    d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
+                    d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
+                    if (broke) fl |= RF_REC_BROKE;
+                    // parallel contact (extended model, explicit steps): an overlapping bonded pair
+                    // also carries the Hertz-Mindlin contact, and a broken bond's slot keeps that
+                    // contact's state. Its overlap counts from min(r_i + r_j, L0), so a bond formed
+                    // between overlapping particles is force-free at its rest length. FIRE
+                    // relaxation leaves it out: its state would depend on the path.
+                    const double sr = fmin(xo.w + xj.w, L0);
+                    if (MODE == 0 && !c.ref_mode && rr < sr * sr) {
+                        const float rj = (float)xj.w;
+                        const size_t so = ((size_t)io * c.K + k) * 3;
+                        const float* oi = d.cO[cur] + so;
+                        f3 o = ((cmo >> k) & 1u) ? mk3(oi[0], oi[1], oi[2]) : mk3(0.f, 0.f, 0.f);
+                        if (contact_pair_ext(ep, r, rr, sr, ro, rj, c.cmass * ro * ro * ro, c.cmass * rj * rj * rj, vo,
+                                             f4to3(vj), wo, f4to3(wj), o, fr, mr, fnr, ktr, krr))
+                            fl |= RF_REC_CLEAR;
+                        float* oo = d.cO[nxt] + so;
+                        oo[0] = o.x; oo[1] = o.y; oo[2] = o.z;
+                        fl |= RF_REC_PARALLEL;
+                    }
+                }
+                s_res[wp][0][lane] = fr.x; s_res[wp][1][lane] = fr.y; s_res[wp][2][lane] = fr.z;
+                s_res[wp][3][lane] = mr.x; s_res[wp][4][lane] = mr.y; s_res[wp][5][lane] = mr.z;
+                s_res[wp][6][lane] = __uint_as_float(fl);
+                if (MODE == 1) { s_res[wp][7][lane] = fnr; s_res[wp][8][lane] = ktr; s_res[wp][9][lane] = krr; }
             }
-            BondExt b;
-            b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ri, (float)xj.w);
-            b.sc = str.x; b.tc = str.y; b.L0 = L0;
-            if (MODE == 0 && c.ref_mode) {
-                const float il = __ldg(&d.bil[s]);
-                b.kn = c.refE * il; b.ks = c.refG * il; b.br = c.ref_br;
-            }
-            const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
-            f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
-            f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
-            bool broke;
-            if (MODE == 1) {
-                const double4 xj0 = ldg_d4(&d.x0[j]), rj0 = ldg_d4(&d.rot[j]);
-                const double hx = 0.5 * (ri0.x + rj0.x), hy = 0.5 * (ri0.y + rj0.y), hz = 0.5 * (ri0.z + rj0.z);
-                const f3 du = mk3((float)(rd.x - (xj0.x - xi0.x) - (hy * rd.z - hz * rd.y)),
-                                  (float)(rd.y - (xj0.y - xi0.y) - (hz * rd.x - hx * rd.z)),
-                                  (float)(rd.z - (xj0.z - xi0.z) - (hx * rd.y - hy * rd.x)));
-                broke = bond_slot_ext_total(b, r, rr, du, mk3((float)ri0.x, (float)ri0.y, (float)ri0.z),
-                                            mk3((float)rj0.x, (float)rj0.y, (float)rj0.z), rij, oijt, mijn, mijt, rij,
-                                            oijt, mijn, mijt, fsb, msb, fnabs, kt, kr);
-            } else {
-                broke = bond_slot_ext(ep, b, r, rr, vi, f4to3(vj), wi, f4to3(wj), rij, oijt, mijn, mijt, fsb,
-                                      msb, fnabs, kt, kr, c.ref_mode != 0);
-            }
-            ++npair;
-            d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
-            d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
-            d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
-            const uint32_t k = d.bk[s];
-            if (broke) { bmask &= ~(1u << q); bond &= ~(1u << k); ++nbroken; }
-            // parallel contact (extended model, explicit steps): an overlapping bonded pair also
-            // carries the Hertz-Mindlin contact, and a broken bond's slot keeps that contact's
-            // state. Its overlap counts from min(r_i + r_j, L0), so a bond formed between
-            // overlapping particles is force-free at its rest length. FIRE relaxation leaves
-            // it out: its state would depend on the path.
-            const double sr = fmin(xi.w + xj.w, L0);
-            if (MODE == 0 && !c.ref_mode && rr < sr * sr) {
-                const uint32_t bit = 1u << k;
-                const float rj = (float)xj.w;
-                f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
-                contact_pair_ext(ep, r, rr, sr, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(vj), wi, f4to3(wj), o,
-                                 fsb, msb, fnabs, kt, kr);
+            __syncwarp();
+            // this particle's records that fell in this round, in record order
+            while (rem) {
+                const uint32_t q = __ffs(rem) - 1u;
+                const uint32_t x = s_q0[wp][q] + __popc(s_qb[wp][q] & lt) - base;
+                if (x >= 32u) break;
+                rem &= rem - 1u;
+                const uint32_t fl = __float_as_uint(s_res[wp][6][x]);
+                const uint32_t k = (fl >> 8) & 31u;
+                if (fl & RF_REC_DELETE) {
+                    delete_slot(d, c, i, k, __float_as_uint(s_res[wp][0][x]), ncand, nbq, live, bond, cm, bmask, mem);
+                    continue;
+                }
+                fsb.x += s_res[wp][0][x]; fsb.y += s_res[wp][1][x]; fsb.z += s_res[wp][2][x];
+                if (fl & RF_REC_CLEAR) {
+                    msb = mk3(0.f, 0.f, 0.f);       // the contact's zero-spin rule clears the moment sum
+                } else {
+                    msb.x += s_res[wp][3][x]; msb.y += s_res[wp][4][x]; msb.z += s_res[wp][5][x];
+                }
+                if (MODE == 1) { fnabs += s_res[wp][7][x]; kt += s_res[wp][8][x]; kr += s_res[wp][9][x]; }
                 ++npair;
-                oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
-                pc |= bit;
-            } else {
-                cm &= ~(1u << k);      // not in contact: the parallel contact's state ends here
+                if (fl & RF_REC_BROKE) { bmask &= ~(1u << q); bond &= ~(1u << k); ++nbroken; }
+                if (fl & RF_REC_PARALLEL) { pc |= 1u << k; ++npair; }
+                else cm &= ~(1u << k);       // not in contact: the parallel contact's state ends here
             }
+            __syncwarp();
         }
     }
+
+    // the particle's own state (the bond pass read it through the cache)
+    double4 xi = make_double4(0, 0, 0, 1);
+    f3 vi = mk3(0.f, 0.f, 0.f), wi = vi;
+    if (valid) { xi = P[i]; vi = f4to3(Vv[i]); wi = f4to3(Wv[i]); }
+    const float ri = (float)xi.w;
+    const float mi = c.cmass * ri * ri * ri;
+    const uint32_t* row = d.ids + (size_t)i * c.K;
+    const float* oin = d.cO[cur] + (size_t)i * c.K * 3;
+    float* oout = d.cO[nxt] + (size_t)i * c.K * 3;
 
     f3 fsc = mk3(0.f, 0.f, 0.f), msc = fsc;
     uint32_t cm_out = 0;
@@ -2074,7 +2147,7 @@ template <class T> rf_status dalloc(rf_engine* e, T** p, size_t n) {
 
 #define TRY(x) do { rf_status s__ = (x); if (s__ != RF_OK) return s__; } while (0)
 
-// Explicit extended-model step kernels compiled for 4, 5 or 6 CTAs per SM.
+// Explicit extended-model step kernels compiled for 5, 6 or 8 CTAs per SM.
 void* ext_step_variant(bool brazil, int minb) {
     switch (minb) {
         case 8: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 8> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 8>;
@@ -2082,6 +2155,10 @@ void* ext_step_variant(bool brazil, int minb) {
         default: return brazil ? (void*)k_step_ext<RF_TEST_BRAZIL, 0, 6> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 0, 6>;
     }
 }
+
+// dynamic shared memory of a step launch: the extended kernel's per-warp record list
+// (32 particles x QB records, 2 bytes each, 4 warps)
+unsigned step_smem(const rf_engine* e) { return e->c.ext ? 4u * 32u * e->d.QB * 2u : 0u; }
 
 void* step_kernel(const rf_engine* e) {
     const bool br = e->task.kind == RF_TEST_BRAZIL;
@@ -2173,6 +2250,7 @@ rf_status build_graph(rf_engine* e) {
         sargs[u][1] = &cs[u];
         cudaGraphNode_t step;
         kp = kparams(fn, e->nblocks, 128, sargs[u]);
+        kp.sharedMemBytes = step_smem(e);
         RF_CUDA(cudaGraphAddKernelNode(&step, body, &last, 1, &kp));
         last = step;
     }
@@ -2235,6 +2313,7 @@ rf_status build_fire_graph(rf_engine* e) {
     cudaGraphNode_t fnode, unode;
     void* ff = (e->task.kind == RF_TEST_BRAZIL) ? (void*)k_step_ext<RF_TEST_BRAZIL, 1> : (void*)k_step_ext<RF_TEST_UNIAXIAL, 1>;
     kp = kparams(ff, e->nblocks, 128);
+    kp.sharedMemBytes = step_smem(e);
     RF_CUDA(cudaGraphAddKernelNode(&fnode, body, &inode, 1, &kp));
     kp = kparams((void*)k_fire_update, e->nblocks, 128);
     RF_CUDA(cudaGraphAddKernelNode(&unode, body, &fnode, 1, &kp));
@@ -2261,7 +2340,7 @@ rf_status launch_stream_fire(rf_engine* e, uint64_t max_iter) {
             k_rb_scan_apply<<<e->cg_nb, 1024, 0, s>>>(d, c);
             k_rb_scatter<<<gN, 256, 0, s>>>(d, c);
             k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
-            RF_CUDA(cudaLaunchKernel(ff, dim3(e->nblocks), dim3(128), args, 0, s));
+            RF_CUDA(cudaLaunchKernel(ff, dim3(e->nblocks), dim3(128), args, step_smem(e), s));
             k_fire_update<<<e->nblocks, 128, 0, s>>>(d, c);
         }
         RF_CHECK_LAUNCH("engine stream FIRE");
@@ -2289,7 +2368,7 @@ rf_status launch_stream_steps(rf_engine* e, uint64_t nsteps) {
         k_rb_scatter<<<gN, 256, 0, s>>>(d, c);
         k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
         void* sargs[] = {&d, &c};
-        if (cudaLaunchKernel(step_kernel(e), dim3(e->nblocks), dim3(128), sargs, 0, s) != cudaSuccess) break;
+        if (cudaLaunchKernel(step_kernel(e), dim3(e->nblocks), dim3(128), sargs, step_smem(e), s) != cudaSuccess) break;
         k_stream_ungate<<<1, 32, 0, s>>>(d);
     }
     RF_CHECK_LAUNCH("engine stream steps");
@@ -3005,7 +3084,8 @@ rf_status rf_engine_autotune(rf_engine* e, int steps, int* choice, float* ms_out
             k_rb_cand<<<(c.N + 127) / 128, 128, 0, s>>>(d, c);
             k_set_target<<<1, 1, 0, s>>>(d.sc, (unsigned long long)steps);
             cudaEventRecord(a0, s);
-            for (int q = 0; q < steps && !ce; ++q) ce = cudaLaunchKernel(fn, dim3(e->nblocks), dim3(128), args, 0, s);
+            for (int q = 0; q < steps && !ce; ++q)
+                ce = cudaLaunchKernel(fn, dim3(e->nblocks), dim3(128), args, step_smem(e), s);
             cudaEventRecord(a1, s);
             if (!ce) ce = cudaEventSynchronize(a1);
             float ms = 0.f;

@@ -479,8 +479,9 @@ __device__ __forceinline__ bool bond_slot_ext_total(const BondExt& b, const f3 r
 }
 
 // Overlapping pair of the extended model. rr = |r|^2 and sr = r_i + r_j in double, with
-// rr < sr^2; the overlap is (sr^2 - rr) / (sr + |r|). mi, mj are the masses.
-__device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r, const double rr, const double sr,
+// rr < sr^2; the overlap is (sr^2 - rr) / (sr + |r|). mi, mj are the masses. Returns true
+// when the rolling resistance's zero-spin rule cleared the moment sum ms.
+__device__ __forceinline__ bool contact_pair_ext(const ExtParams& p, const f3 r, const double rr, const double sr,
                                                  const float ri, const float rj, const float mi, const float mj,
                                                  const f3 vi, const f3 vj, const f3 wi, const f3 wj, f3& Oijt, f3& fs,
                                                  f3& ms, float& fnabs, float& kt, float& kr) {
@@ -540,8 +541,10 @@ __device__ __forceinline__ void contact_pair_ext(const ExtParams& p, const f3 r,
             ms.x = fm(wi.x, cr, ms.x); ms.y = fm(wi.y, cr, ms.y); ms.z = fm(wi.z, cr, ms.z);
         } else {
             ms = mk3(0.f, 0.f, 0.f);
+            return true;
         }
     }
+    return false;
 }
 
 }  // namespace rf

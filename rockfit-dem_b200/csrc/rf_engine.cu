@@ -1073,13 +1073,6 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     const bool frozen = MODE == 0 && i < N && S->done != 0;
     const bool valid = i < N && !frozen;
     const uint32_t FULL = 0xffffffffu;
-    const double Top = c.ref_mode ? (double)(float)S->Top : S->Top;
-    const double Bottom = c.ref_mode ? (double)(float)S->Bottom : S->Bottom;
-    const double TopR = c.ref_mode ? (double)(float)S->TopR : S->TopR;
-    const double BottomR = c.ref_mode ? (double)(float)S->BottomR : S->BottomR;
-    const float vt = MODE == 0 ? (float)S->V : 0.f, RR = S->RR;
-    rf_float3 cc;
-    cc.x = S->center[0]; cc.y = S->center[1]; cc.z = S->center[2];
     if (frozen) {
         d.posd[nxt][i] = P[i];
         d.vel[nxt][i] = Vv[i];
@@ -1112,15 +1105,17 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         mem = d.member[i]; ncand = d.cand_n[i];
         nbq = d.nbq[i]; bmask = d.bmask[i];
     }
-    const uint32_t live0 = live, bond0 = bond, cm0 = cm, bmask0 = bmask;
-    const unsigned long long mem0 = mem;
     const size_t QN = (size_t)d.QB * N;
 
-    f3 fsb = mk3(0.f, 0.f, 0.f), msb = fsb;
-    uint32_t nbroken = 0;
+    bool dirty = false;          // live, bond, bmask or member changed
     // bond slots whose pair overlaps: their contact (in parallel with the bond) was taken
     // in the bond pass, with its tangential overlap kept in the slot's contact state
     uint32_t pc = 0;
+    const uint32_t cm0 = cm;
+    constexpr int NA = MODE == 1 ? 9 : 6;         // the particle's bond sums (float)
+    __shared__ float s_acc[4][NA][32];
+    __shared__ uint32_t s_msk[4][10][32];
+    enum { W_LIVE, W_BOND, W_CM, W_BMASK, W_PC, W_NB, W_MEMLO, W_MEMHI, W_NPAIR, W_DIRTY };
     {
         // Bond records, spread over the warp. The warp's active records are listed
         // ordinal-major (every particle's first record, then every second one, ...; lane
@@ -1128,8 +1123,10 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         // [QB][N] record arrays, and in each round every lane takes one record whatever the
         // 32 particles' bond counts. The lane that takes a record forms its force, moment
         // and outcome from zero and hands them to the particle's lane through shared
-        // memory; the particle adds them in record order. FIRE mode reads the records'
-        // increment-start state and the motion since then.
+        // memory; the particle adds them in record order. While the pass runs, each
+        // particle's sums and masks wait in shared memory, leaving the registers to the
+        // record arithmetic. FIRE mode reads the records' increment-start state and the
+        // motion since then.
         constexpr int NO = MODE == 1 ? 10 : 7;        // words of one record's result
         __shared__ float s_res[4][NO][32];
         __shared__ uint32_t s_q0[4][32], s_qb[4][32];  // per ordinal: first list entry, lanes holding one
@@ -1147,16 +1144,24 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             if (lane == q) { s_q0[wp][q] = T; s_qb[wp][q] = bal; }
             T += __popc(bal);
         }
+        uint32_t rem = bmask;                          // this particle's records not yet added
+#pragma unroll
+        for (int a = 0; a < NA; ++a) s_acc[wp][a][lane] = 0.f;   // (read back after the contact pass)
+        s_msk[wp][W_NB][lane] = 0u;
+        s_msk[wp][W_NPAIR][lane] = 0u;
+        if (T) {
+            s_msk[wp][W_LIVE][lane] = live; s_msk[wp][W_BOND][lane] = bond; s_msk[wp][W_CM][lane] = cm;
+            s_msk[wp][W_BMASK][lane] = bmask; s_msk[wp][W_PC][lane] = 0u;
+            s_msk[wp][W_MEMLO][lane] = (uint32_t)mem; s_msk[wp][W_MEMHI][lane] = (uint32_t)(mem >> 32);
+            s_msk[wp][W_DIRTY][lane] = 0u;
+        }
         __syncwarp();
         const float4* src = MODE == 1 ? d.bst0 : d.bst;
-        uint32_t rem = bmask;                          // this particle's records not yet added
         for (uint32_t base = 0; base < T; base += 32u) {
             const uint32_t p = base + lane;
-            const uint32_t e = p < T ? (uint32_t)lst[p] : lane;
-            const uint32_t ol = e & 31u;
-            const uint32_t cmo = __shfl_sync(FULL, cm0, ol);   // the record's particle's step-start contacts
             if (p < T) {
-                const uint32_t q = e >> 5, io = wbase + ol;
+                const uint32_t e = lst[p];
+                const uint32_t ol = e & 31u, q = e >> 5, io = wbase + ol;
                 const size_t s = (size_t)q * N + io;
                 // every load of the record is issued before the partner's gathers
                 const uint32_t j = __ldg(&d.bj[s]);
@@ -1218,6 +1223,9 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                         const float rj = (float)xj.w;
                         const size_t so = ((size_t)io * c.K + k) * 3;
                         const float* oi = d.cO[cur] + so;
+                        // the particle's contacts at the step's start (its own record's
+                        // bit is only cleared after this record is added)
+                        const uint32_t cmo = s_msk[wp][W_CM][ol];
                         f3 o = ((cmo >> k) & 1u) ? mk3(oi[0], oi[1], oi[2]) : mk3(0.f, 0.f, 0.f);
                         if (contact_pair_ext(ep, r, rr, sr, ro, rj, c.cmass * ro * ro * ro, c.cmass * rj * rj * rj, vo,
                                              f4to3(vj), wo, f4to3(wj), o, fr, mr, fnr, ktr, krr))
@@ -1242,29 +1250,58 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                 const uint32_t fl = __float_as_uint(s_res[wp][6][x]);
                 const uint32_t k = (fl >> 8) & 31u;
                 if (fl & RF_REC_DELETE) {
-                    delete_slot(d, c, i, k, __float_as_uint(s_res[wp][0][x]), ncand, nbq, live, bond, cm, bmask, mem);
+                    uint32_t lv = s_msk[wp][W_LIVE][lane], bd = s_msk[wp][W_BOND][lane];
+                    uint32_t cmm = s_msk[wp][W_CM][lane], bm = s_msk[wp][W_BMASK][lane];
+                    unsigned long long mm = (unsigned long long)s_msk[wp][W_MEMLO][lane] |
+                                            ((unsigned long long)s_msk[wp][W_MEMHI][lane] << 32);
+                    delete_slot(d, c, i, k, __float_as_uint(s_res[wp][0][x]), d.cand_n[i], d.nbq[i], lv, bd, cmm, bm,
+                                mm);
+                    s_msk[wp][W_LIVE][lane] = lv; s_msk[wp][W_BOND][lane] = bd;
+                    s_msk[wp][W_CM][lane] = cmm; s_msk[wp][W_BMASK][lane] = bm;
+                    s_msk[wp][W_MEMLO][lane] = (uint32_t)mm; s_msk[wp][W_MEMHI][lane] = (uint32_t)(mm >> 32);
+                    s_msk[wp][W_DIRTY][lane] = 1u;
                     continue;
                 }
-                fsb.x += s_res[wp][0][x]; fsb.y += s_res[wp][1][x]; fsb.z += s_res[wp][2][x];
-                if (fl & RF_REC_CLEAR) {
-                    msb = mk3(0.f, 0.f, 0.f);       // the contact's zero-spin rule clears the moment sum
+                s_acc[wp][0][lane] += s_res[wp][0][x];
+                s_acc[wp][1][lane] += s_res[wp][1][x];
+                s_acc[wp][2][lane] += s_res[wp][2][x];
+                if (fl & RF_REC_CLEAR) {       // the contact's zero-spin rule clears the moment sum
+                    s_acc[wp][3][lane] = 0.f; s_acc[wp][4][lane] = 0.f; s_acc[wp][5][lane] = 0.f;
                 } else {
-                    msb.x += s_res[wp][3][x]; msb.y += s_res[wp][4][x]; msb.z += s_res[wp][5][x];
+                    s_acc[wp][3][lane] += s_res[wp][3][x];
+                    s_acc[wp][4][lane] += s_res[wp][4][x];
+                    s_acc[wp][5][lane] += s_res[wp][5][x];
                 }
-                if (MODE == 1) { fnabs += s_res[wp][7][x]; kt += s_res[wp][8][x]; kr += s_res[wp][9][x]; }
-                ++npair;
-                if (fl & RF_REC_BROKE) { bmask &= ~(1u << q); bond &= ~(1u << k); ++nbroken; }
-                if (fl & RF_REC_PARALLEL) { pc |= 1u << k; ++npair; }
-                else cm &= ~(1u << k);       // not in contact: the parallel contact's state ends here
+                if (MODE == 1) {
+                    s_acc[wp][6][lane] += s_res[wp][7][x];
+                    s_acc[wp][7][lane] += s_res[wp][8][x];
+                    s_acc[wp][8][lane] += s_res[wp][9][x];
+                }
+                uint32_t np = 1;
+                if (fl & RF_REC_BROKE) {
+                    s_msk[wp][W_BMASK][lane] &= ~(1u << q);
+                    s_msk[wp][W_BOND][lane] &= ~(1u << k);
+                    s_msk[wp][W_NB][lane] += 1u;
+                    s_msk[wp][W_DIRTY][lane] = 1u;
+                }
+                if (fl & RF_REC_PARALLEL) { s_msk[wp][W_PC][lane] |= 1u << k; ++np; }
+                else s_msk[wp][W_CM][lane] &= ~(1u << k);    // not in contact: the parallel contact's state ends
+                if (MODE == 1) s_msk[wp][W_NPAIR][lane] += np;
             }
             __syncwarp();
         }
+        if (T) {
+            live = s_msk[wp][W_LIVE][lane]; bond = s_msk[wp][W_BOND][lane]; cm = s_msk[wp][W_CM][lane];
+            bmask = s_msk[wp][W_BMASK][lane]; pc = s_msk[wp][W_PC][lane];
+            mem = (unsigned long long)s_msk[wp][W_MEMLO][lane] | ((unsigned long long)s_msk[wp][W_MEMHI][lane] << 32);
+            dirty = s_msk[wp][W_DIRTY][lane] != 0u;
+        }
     }
 
-    // the particle's own state (the bond pass read it through the cache)
+    // the particle's own position (the bond pass read it through the cache; its velocity
+    // and spin are read where they are used)
     double4 xi = make_double4(0, 0, 0, 1);
-    f3 vi = mk3(0.f, 0.f, 0.f), wi = vi;
-    if (valid) { xi = P[i]; vi = f4to3(Vv[i]); wi = f4to3(Wv[i]); }
+    if (valid) xi = P[i];
     const float ri = (float)xi.w;
     const float mi = c.cmass * ri * ri * ri;
     const uint32_t* row = d.ids + (size_t)i * c.K;
@@ -1286,6 +1323,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             const double rr = dlen2(rd);
             if (with_delete && (rr > cut2_del(c, xi.w, xj.w) || rr < 1e-10)) {
                 delete_slot(d, c, i, k, j, ncand, nbq, live, bond, cm, bmask, mem);
+                dirty = true;
                 continue;
             }
             const float rj = (float)xj.w;
@@ -1295,8 +1333,9 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             // cm: step-start contacts minus slots deleted this step (a refilled slot starts at zero)
             f3 o = (cm & bit) ? mk3(oin[3 * k], oin[3 * k + 1], oin[3 * k + 2]) : mk3(0.f, 0.f, 0.f);
             const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
-            contact_pair_ext(ep, r, rr, sr, ri, rj, mi, c.cmass * rj * rj * rj, vi, f4to3(__ldg(&Vv[j])), wi,
-                             f4to3(__ldg(&Wv[j])), o, fsc, msc, fnc, ktc, krc);
+            contact_pair_ext(ep, r, rr, sr, ri, rj, mi, c.cmass * rj * rj * rj, f4to3(__ldg(&Vv[i])),
+                             f4to3(__ldg(&Vv[j])), f4to3(__ldg(&Wv[i])), f4to3(__ldg(&Wv[j])), o, fsc, msc, fnc, ktc,
+                             krc);
             ++npc;
             oout[3 * k] = o.x; oout[3 * k + 1] = o.y; oout[3 * k + 2] = o.z;
             cm_out |= bit;
@@ -1336,6 +1375,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
             d.ids[(size_t)i * c.K + k] = j;
             live |= 1u << k;
             mem |= 1ull << best_q;
+            dirty = true;
             const double4 xj = ldg_d4(&P[j]);
             const double sr = xi.w + xj.w;
             if (dlen2(dsub(xj, xi)) < sr * sr) replay = true;
@@ -1358,11 +1398,26 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
 #pragma unroll
     for (int q = 0; q < FIRE_SUMS; ++q) acc[q] = 0.0;
     if (valid) {
-        if (live != live0) d.live[i] = live;
-        if (bond != bond0) d.bond[i] = bond;
+        // the bond pass's sums, waiting in shared memory through the contact pass
+        const uint32_t wq = threadIdx.x >> 5, lq = threadIdx.x & 31u;
+        const f3 vi = f4to3(Vv[i]), wi = f4to3(Wv[i]);
+        const f3 fsb = mk3(s_acc[wq][0][lq], s_acc[wq][1][lq], s_acc[wq][2][lq]);
+        const f3 msb = mk3(s_acc[wq][3][lq], s_acc[wq][4][lq], s_acc[wq][5][lq]);
+        if (MODE == 1) {
+            fnabs += s_acc[wq][6][lq]; kt += s_acc[wq][7][lq]; kr += s_acc[wq][8][lq];
+            npair += s_msk[wq][W_NPAIR][lq];
+        }
+        if (dirty) { d.live[i] = live; d.bond[i] = bond; d.member[i] = mem; d.bmask[i] = bmask; }
         if (cm != cm0) d.cmask[i] = cm;
-        if (mem != mem0) d.member[i] = mem;
-        if (bmask != bmask0) d.bmask[i] = bmask;
+        // platens of this particle's specimen (with the reference constants their
+        // coordinates are rounded to float, as the reference's drivers pass them)
+        const double Top = c.ref_mode ? (double)(float)S->Top : S->Top;
+        const double Bottom = c.ref_mode ? (double)(float)S->Bottom : S->Bottom;
+        const double TopR = c.ref_mode ? (double)(float)S->TopR : S->TopR;
+        const double BottomR = c.ref_mode ? (double)(float)S->BottomR : S->BottomR;
+        const float vt = MODE == 0 ? (float)S->V : 0.f, RR = S->RR;
+        rf_float3 cc;
+        cc.x = S->center[0]; cc.y = S->center[1]; cc.z = S->center[2];
         float Fx = 0.0f + fsb.x, Fy = 0.0f + fsb.y, Fz = 0.0f + fsb.z;
         Fx += fsc.x; Fy += fsc.y; Fz += fsc.z;
         float Mx = 0.0f + msb.x, My = 0.0f + msb.y, Mz = 0.0f + msb.z;
@@ -1417,6 +1472,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         if (!hidden) e2max = e2;
         }
     }
+    const uint32_t nbroken = s_msk[threadIdx.x >> 5][W_NB][threadIdx.x & 31u];
     if (MODE == 0) {
         note_displacement(d, e2max);
         step_finish_ext<KIND>(d, c, sfb, sft, nbroken, moved, sI - sA);

@@ -46,6 +46,11 @@
 #endif
 // outcome of one bond record, handed by the lane that evaluated it to its particle's lane
 // (bits 8-12: the record's row slot)
+// margin buckets of the candidate lists: a candidate's margin (distance - list cutoff at
+// the build) below RF_CB1, RF_CB2, RF_CB3 skins, or above
+#define RF_CB1 0.05f
+#define RF_CB2 0.15f
+#define RF_CB3 0.3f
 #define RF_REC_DELETE 1u          // beyond the bond's keep distance: the slot is deleted (partner id in the force word)
 #define RF_REC_BROKE 2u           // the bond broke this step
 #define RF_REC_PARALLEL 4u        // the pair overlaps: the slot's contact was taken with the bond
@@ -158,6 +163,7 @@ struct Dev {
     unsigned long long* member;   // [N]
     float4* pos_ref;    // [N]
     float* cmargin;     // [N] smallest (distance - a_farcut) of the non-member candidates at the build
+    uint32_t* cbound;   // [N] ends of the candidates' margin buckets (bytes 0-2, see k_rb_cand)
     uint32_t* cg_key;   // [N]
     uint32_t* cg_count; // [cells+1]
     uint32_t* cg_start; // [cells+1]
@@ -331,6 +337,28 @@ __global__ void k_rb_cand(Dev d, Consts c) {
         }
         if (n > c.KC) n = c.KC;
         d.cand_n[i] = n;
+        // candidates in the order of their margin bucket (stable within a bucket): a scan
+        // needs no candidate of a bucket whose lower bound the displacements since this
+        // build cannot have closed (scan_limit)
+        {
+            uint32_t jl[64];
+            uint8_t bq[64];
+            uint32_t cnt[4] = {0u, 0u, 0u, 0u};
+            for (uint32_t q = 0; q < n; ++q) {
+                const uint32_t j = d.cand[(size_t)q * c.N + i];
+                const float4 xj = posf(d, c, cur, j);
+                const float ddx = xj.x - xi.x, ddy = xj.y - xi.y, ddz = xj.z - xi.z;
+                const float cut = c.lgap_f > 0.f ? fminf(c.acut_f, (xi.w + xj.w) + c.lgap_f) : c.acut_f;
+                const float mg = sqrtf(ddx * ddx + ddy * ddy + ddz * ddz) - cut;
+                const uint32_t b = mg < RF_CB1 * c.skin_f ? 0u : mg < RF_CB2 * c.skin_f ? 1u : mg < RF_CB3 * c.skin_f ? 2u : 3u;
+                jl[q] = j;
+                bq[q] = (uint8_t)b;
+                ++cnt[b];
+            }
+            uint32_t pos[4] = {0u, cnt[0], cnt[0] + cnt[1], cnt[0] + cnt[1] + cnt[2]};
+            d.cbound[i] = pos[1] | (pos[2] << 8) | (pos[3] << 16);
+            for (uint32_t q = 0; q < n; ++q) d.cand[(size_t)(pos[bq[q]]++) * c.N + i] = jl[q];
+        }
         // membership: candidates already in the row
         unsigned long long mem = 0ull;
         uint32_t live = d.live[i];
@@ -420,6 +448,23 @@ __device__ __forceinline__ bool scan_not_needed(const Dev& d, const Consts& c, u
     const float ex = x - pr.x, ey = y - pr.y, ez = z - pr.z;
     const float di = sqrtf(ex * ex + ey * ey + ez * ez);
     return di + d.sc->dmax < 0.9f * d.cmargin[i] - 1e-4f * c.acut_f;
+}
+
+// How many of particle i's candidates (in bucket order) a scan must test: the candidates
+// of a bucket whose smallest margin the displacements since the build cannot have closed
+// (the test of scan_not_needed, with the bucket's lower bound for cmargin) can be skipped.
+// After a deletion (cmargin 0) every candidate is tested.
+__device__ __forceinline__ uint32_t scan_limit(const Dev& d, const Consts& c, uint32_t i, float x, float y, float z,
+                                               uint32_t n) {
+    if (!(d.cmargin[i] > 0.f)) return n;
+    const float4 pr = d.pos_ref[i];
+    const float ex = x - pr.x, ey = y - pr.y, ez = z - pr.z;
+    const float reach = sqrtf(ex * ex + ey * ey + ez * ez) + d.sc->dmax + 1e-4f * c.acut_f;
+    const uint32_t b = d.cbound[i];
+    if (reach < 0.9f * RF_CB1 * c.skin_f) return b & 0xFFu;
+    if (reach < 0.9f * RF_CB2 * c.skin_f) return (b >> 8) & 0xFFu;
+    if (reach < 0.9f * RF_CB3 * c.skin_f) return (b >> 16) & 0xFFu;
+    return n;
 }
 
 // Largest squared displacement (since the last build) of the positions a step writes.
@@ -778,6 +823,13 @@ __global__ void __launch_bounds__(128, RF_STEP_MIN_BLOCKS) k_step(Dev d, Consts 
 __device__ __forceinline__ double4 ldg_d4(const double4* p) {
     const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
     return make_double4(a.x, a.y, b.x, b.y);
+}
+// A read of three floats that the compiler may not merge with an earlier read of the same
+// address: the value is fetched again (an L1 hit) instead of being held in registers.
+__device__ __forceinline__ f3 reload3(const float4* p) {
+    float x, y, z, w;
+    asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(x), "=f"(y), "=f"(z), "=f"(w) : "l"(p));
+    return mk3(x, y, z);
 }
 __device__ __forceinline__ double3 dsub(const double4 a, const double4 b) {
     return make_double3(a.x - b.x, a.y - b.y, a.z - b.z);
@@ -1181,9 +1233,16 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                     fl |= RF_REC_DELETE;
                     fr.x = __uint_as_float(j);
                 } else {
-                    const float ro = (float)xo.w;
+                    const float ro = (float)xo.w, rj = (float)xj.w;
+                    // parallel contact (extended model, explicit steps): an overlapping bonded pair
+                    // also carries the Hertz-Mindlin contact, and a broken bond's slot keeps that
+                    // contact's state. Its overlap counts from min(r_i + r_j, L0), so a bond formed
+                    // between overlapping particles is force-free at its rest length. FIRE
+                    // relaxation leaves it out: its state would depend on the path.
+                    const double sr = fmin(xo.w + xj.w, L0);
+                    const bool pcon = MODE == 0 && !c.ref_mode && rr < sr * sr;
                     BondExt b;
-                    b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ro, (float)xj.w);
+                    b.kn = c.kn; b.ks = c.ks; b.br = c.br_lambda * fminf(ro, rj);
                     b.sc = str.x; b.tc = str.y; b.L0 = L0;
                     if (MODE == 0 && c.ref_mode) {
                         const float il = __ldg(&d.bil[s]);
@@ -1192,7 +1251,6 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                     const f3 r = mk3((float)rd.x, (float)rd.y, (float)rd.z);
                     f3 rij = mk3(s0.x, s0.y, s0.z), oijt = mk3(s0.w, s1.x, s1.y);
                     f3 mijn = mk3(s1.z, s1.w, s2.x), mijt = mk3(s2.y, s2.z, s2.w);
-                    f3 vo = mk3(0.f, 0.f, 0.f), wo = vo;
                     bool broke;
                     if (MODE == 1) {
                         const double4 xi0 = ldg_d4(&d.x0[io]), ri0 = ldg_d4(&d.rot[io]);
@@ -1205,30 +1263,25 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
                                                     mk3((float)rj0.x, (float)rj0.y, (float)rj0.z), rij, oijt, mijn,
                                                     mijt, rij, oijt, mijn, mijt, fr, mr, fnr, ktr, krr);
                     } else {
-                        vo = f4to3(__ldg(&Vv[io])); wo = f4to3(__ldg(&Wv[io]));
-                        broke = bond_slot_ext(ep, b, r, rr, vo, f4to3(vj), wo, f4to3(wj), rij, oijt, mijn, mijt, fr,
-                                              mr, fnr, ktr, krr, c.ref_mode != 0);
+                        broke = bond_slot_ext(ep, b, r, rr, f4to3(__ldg(&Vv[io])), f4to3(vj), f4to3(__ldg(&Wv[io])),
+                                              f4to3(wj), rij, oijt, mijn, mijt, fr, mr, fnr, ktr, krr, c.ref_mode != 0);
                     }
                     d.bst[s] = make_float4(rij.x, rij.y, rij.z, oijt.x);
                     d.bst[s + QN] = make_float4(oijt.y, oijt.z, mijn.x, mijn.y);
                     d.bst[s + 2 * QN] = make_float4(mijn.z, mijt.x, mijt.y, mijt.z);
                     if (broke) fl |= RF_REC_BROKE;
-                    // parallel contact (extended model, explicit steps): an overlapping bonded pair
-                    // also carries the Hertz-Mindlin contact, and a broken bond's slot keeps that
-                    // contact's state. Its overlap counts from min(r_i + r_j, L0), so a bond formed
-                    // between overlapping particles is force-free at its rest length. FIRE
-                    // relaxation leaves it out: its state would depend on the path.
-                    const double sr = fmin(xo.w + xj.w, L0);
-                    if (MODE == 0 && !c.ref_mode && rr < sr * sr) {
-                        const float rj = (float)xj.w;
+                    if (pcon) {
+                        // the pair's velocities and spins are read again (cache hits) rather
+                        // than held through the bond arithmetic
                         const size_t so = ((size_t)io * c.K + k) * 3;
                         const float* oi = d.cO[cur] + so;
                         // the particle's contacts at the step's start (its own record's
                         // bit is only cleared after this record is added)
                         const uint32_t cmo = s_msk[wp][W_CM][ol];
                         f3 o = ((cmo >> k) & 1u) ? mk3(oi[0], oi[1], oi[2]) : mk3(0.f, 0.f, 0.f);
-                        if (contact_pair_ext(ep, r, rr, sr, ro, rj, c.cmass * ro * ro * ro, c.cmass * rj * rj * rj, vo,
-                                             f4to3(vj), wo, f4to3(wj), o, fr, mr, fnr, ktr, krr))
+                        if (contact_pair_ext(ep, r, rr, sr, ro, rj, c.cmass * ro * ro * ro, c.cmass * rj * rj * rj,
+                                             reload3(&Vv[io]), reload3(&Vv[j]), reload3(&Wv[io]), reload3(&Wv[j]), o,
+                                             fr, mr, fnr, ktr, krr))
                             fl |= RF_REC_CLEAR;
                         float* oo = d.cO[nxt] + so;
                         oo[0] = o.x; oo[1] = o.y; oo[2] = o.z;
@@ -1349,10 +1402,11 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         bool have_cells = false;
         Octant oc;
         const f3 xif = mk3((float)xi.x, (float)xi.y, (float)xi.z);
+        const uint32_t qlim = scan_limit(d, c, i, xif.x, xif.y, xif.z, ncand);
         for (;;) {
             unsigned long long best = ~0ull;
             uint32_t best_q = 0;
-            for (uint32_t q = 0; q < ncand; ++q) {
+            for (uint32_t q = 0; q < qlim; ++q) {
                 if ((tried >> q) & 1ull) continue;
                 const uint32_t j = __ldg(&d.cand[(size_t)q * N + i]);
                 const double4 xj = ldg_d4(&P[j]);
@@ -2590,7 +2644,7 @@ rf_status engine_create_impl(const rf_task* t, const float* h_R, const double* h
         (st = dalloc(e, &d.live, N)) || (st = dalloc(e, &d.bond, N)) || (st = dalloc(e, &d.cmask, N)) ||
         (st = dalloc(e, &d.nbq, N)) || (st = dalloc(e, &d.bmask, N)) || (st = dalloc(e, &e->maxq_dev, 1)) ||
         (st = dalloc(e, &d.cand, (size_t)c.KC * N)) || (st = dalloc(e, &d.cand_n, N)) || (st = dalloc(e, &d.member, N)) ||
-        (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cmargin, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
+        (st = dalloc(e, &d.pos_ref, N)) || (st = dalloc(e, &d.cmargin, N)) || (st = dalloc(e, &d.cbound, N)) || (st = dalloc(e, &d.cg_key, N)) || (st = dalloc(e, &d.cg_count, cells + 1)) ||
         (st = dalloc(e, &d.cg_start, cells + 1)) || (st = dalloc(e, &d.cg_fill, cells + 1)) ||
         (st = dalloc(e, &d.cg_bsum, e->cg_nb)) || (st = dalloc(e, &d.cg_sorted, N)) ||
         (st = dalloc(e, &d.partial, e->nblocks)) || (st = dalloc(e, &d.partial2, e->nblocks)) ||

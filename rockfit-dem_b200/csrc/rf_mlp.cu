@@ -493,6 +493,17 @@ rf_status mlp_reserve(rf_mlp* m, int rows) {
     RF_CUDA(cudaMalloc(&m->dY, (size_t)need * 16 * sizeof(float)));
     RF_CUDA(cudaMalloc(&m->loss_part, 1024 * sizeof(double)));
     RF_CUDA(cudaMalloc(&m->Tres, (size_t)need * NOUT * sizeof(float)));
+    // zero everything once: the padding rows past a call's row count are never written by
+    // the forward pass, but the weight gradients sum over them (with zero output gradients),
+    // and 0 * NaN from uninitialised memory would poison the sums
+    for (int l = 0; l < NL; ++l) {
+        RF_CUDA(cudaMemsetAsync(m->H[l], 0, (size_t)need * DIN[l] * 2, m->stream));
+        RF_CUDA(cudaMemsetAsync(m->HT[l], 0, (size_t)need * DIN[l] * 2, m->stream));
+        RF_CUDA(cudaMemsetAsync(m->dZ[l], 0, (size_t)need * DOUT[l] * 2, m->stream));
+        RF_CUDA(cudaMemsetAsync(m->dZT[l], 0, (size_t)need * DOUT[l] * 2, m->stream));
+    }
+    RF_CUDA(cudaMemsetAsync(m->Y, 0, (size_t)need * 16 * sizeof(float), m->stream));
+    RF_CUDA(cudaMemsetAsync(m->dY, 0, (size_t)need * 16 * sizeof(float), m->stream));
     m->rows_cap = need;
     return RF_OK;
 }

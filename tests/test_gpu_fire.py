@@ -66,3 +66,55 @@ def test_fire_exact_warm_start_cuts_iterations(cuda):
     assert b.iterations * 2 < a.iterations
     assert abs(b.stress - a.stress) <= 1e-3 * a.stress
     A.close(); B.close()
+
+
+def test_mlp_warm_start_behind_its_gate(cuda):
+    """The MLP warm start on a loaded specimen (three engines in lockstep until the
+    evaluation): trained on plain-FIRE pairs of its own history, the gated MLP start relaxes
+    every evaluated increment to the plain run's stress, in fewer iterations than plain
+    FIRE; the gate lets the MLP predict an increment only after its error on the previous
+    one was below the gate times the last-increment motion's error. The last-increment
+    start is run beside it for reference."""
+    from rfdem.warm import WarmStart
+    N, r0 = 4000, 0.25
+    R0, rad, D, H, mo = rfdem.pack_cylinder(N, r0, aspect=2.0, phi=0.58, seed=0xB2000000 + 78)
+    x = extspec.stiff_params()
+    t, R = rfdem.make_test_ext(rfdem.RF_TEST_UNIAXIAL, R0, rad, r0, min_stress=1e3)
+    A, B, Cn = (rfdem.Engine(mc.clone(t), R, ext=x, radius=rad) for _ in range(3))
+    p = A.relax_params(max_iter=60000)
+    ws = WarmStart(N, p.strain_inc, seed=0xB2000000 + 79)
+    loaded = 0
+    for k in range(30):                      # until the platen carries load
+        rs = [E.load_increment(p) for E in (A, B, Cn)]
+        if rs[0].stress > 1e-7 and rs[0].converged:
+            loaded += 1
+        if loaded >= 2:
+            break
+    assert loaded >= 2
+    for k in range(4):                       # training pairs from the plain engine
+        ws.features(A)
+        for E in (A, B, Cn):
+            E.load_increment(p)
+        ws.collect(A)
+    losses = ws.train(steps=300)
+    assert losses[-1] < losses[0]
+    it = {"plain": 0, "mlp": 0, "last": 0}
+    for k in range(5):
+        a = A.load_increment(p)
+        b = B.load_increment_pred(p, ws.predict(B), 16)
+        ratio = ws.observe(B)
+        c = Cn.load_increment_pred(p, ws.predict(Cn, use_mlp=False), 16)
+        print("increment %d: iterations plain %d, MLP %d (used %d, error / last-increment error %.3f), "
+              "last increment %d" % (k, a.iterations, b.iterations, ws.log[-1][1], ratio, c.iterations))
+        assert a.converged == 1 and b.converged == 1 and c.converged == 1
+        assert abs(b.stress - a.stress) <= 1e-3 * abs(a.stress)
+        assert abs(c.stress - a.stress) <= 1e-3 * abs(a.stress)
+        it["plain"] += a.iterations
+        it["mlp"] += b.iterations
+        it["last"] += c.iterations
+    print("iterations over 5 increments:", it)
+    assert it["mlp"] < it["plain"]
+    for (r_prev, _), (_, used) in zip(ws.log[:-1], ws.log[1:]):
+        assert used == (r_prev < ws.gate)
+    ws.close()
+    A.close(); B.close(); Cn.close()

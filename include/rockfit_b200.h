@@ -436,14 +436,26 @@ rf_status rf_relax_default_params(rf_relax_params* p, const rf_task* t);
    (the rotation as the first iteration's angular velocity, rotation / dt0). */
 rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const float* warm,
                                    rf_relax_result* r);
+/* One load increment of every specimen of a batch engine (rf_engine_create_batch; also
+   accepts a one-specimen engine). Each specimen's platen advances by strain_inc times its
+   own initial size and its relaxation runs on its own FIRE scalars (dt, alpha, positive
+   count, convergence); a specimen whose relaxation stopped stays where it is until the
+   others stop, so each specimen ends as its run alone would. warm (device, may be NULL):
+   float[N][ldw], columns 0-5 as for rf_engine_load_increment, or, with scaled != 0, in
+   the warm-start target units of each particle's own specimen. results: one per
+   specimen (broken_bonds: the batch's total). No counterpart in the reference: its
+   quasi-static path is the north star's FIRE extension, here batched. */
+rf_status rf_engine_load_increment_batch(rf_engine* e, const rf_relax_params* p, const float* warm, int ldw,
+                                         int scaled, rf_relax_result* results);
 /* The last increment's start positions, relaxed displacement and accumulated rotation,
    each double[N][3] (host; any may be NULL): training pairs for the warm start. */
 rf_status rf_engine_increment_fields(rf_engine* e, double* x0, double* dx, double* rot);
 
 /*
- * Warm-start features and targets (device buffers). Features of each particle for the
- * next increment of size strain_inc, from the last increment's motion: bf16 [rows][64],
- * rows = N rounded up to 128 (padding rows zero). With D = strain_inc * initial size:
+ * Warm-start features and targets (device buffers; a batch engine's particles each use
+ * their own specimen's sizes). Features of each particle for the next increment of size
+ * strain_inc, from the last increment's motion: bf16 [rows][64], rows = N rounded up to
+ * 128 (padding rows zero). With D = strain_inc * the specimen's initial size:
  *   0-2 displacement / D; 3-5 rotation * r / D; 6 position along the load axis and
  *   7 distance from it, both relative to the specimen's half sizes; 8-55 up to 12
  *   intact bonds in record order: the partner's displacement minus this one's / D

@@ -174,7 +174,8 @@ struct Dev {
     // FIRE relaxation (allocated on first use)
     float4* frc;        // [N] net force after the platen clamp
     float4* mom;        // [N] net moment
-    double* fpart;      // [blocks][FIRE_SUMS] FP64 block partial sums
+    double* fpart;      // [blocks][FIRE_SUMS] FP64 block partial sums (of a CTA's first specimen)
+    double* fpart2;     // [blocks][FIRE_SUMS] the same for a CTA's second specimen (batches)
     double4* rot;       // [N] accumulated rotation of the increment (sum of w dt)
     double4* x0;        // [N] positions at the start of the increment
     unsigned long long n_particles;
@@ -829,6 +830,7 @@ __device__ __forceinline__ double4 ldg_d4(const double4* p) {
 __device__ __forceinline__ f3 reload3(const float4* p) {
     float x, y, z, w;
     asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(x), "=f"(y), "=f"(z), "=f"(w) : "l"(p));
+    (void)w;
     return mk3(x, y, z);
 }
 __device__ __forceinline__ double3 dsub(const double4 a, const double4 b) {
@@ -1095,7 +1097,8 @@ __device__ __forceinline__ void step_finish_ext(const Dev& d, const Consts& c, d
 #define FIRE_SUMS 9     // F.v + M.w, |F|^2, |v|^2, |M|^2, |w|^2, sum |f_n|, pair count, platen sums (2)
 
 template <int KIND>
-__device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c, double (&acc)[FIRE_SUMS]);
+__device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c, double (&acc)[FIRE_SUMS],
+                                                  uint32_t second);
 
 // MODE 0: explicit step (Verlet increments, platen moving at V). MODE 1: force evaluation
 // of one FIRE iteration: the same forces with the FIRE time step, platens at rest; net
@@ -1122,7 +1125,8 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     const SpecGeom& G = d.geom[sI];
     const DevScalars* S = d.spec + sI;
     // a finished specimen of a batch is frozen: its state is carried to the next buffer
-    const bool frozen = MODE == 0 && i < N && S->done != 0;
+    // (explicit steps: it reached its stop rule; FIRE: its relaxation of this increment stopped)
+    const bool frozen = i < N && (MODE == 0 ? S->done != 0 : S->fstop != 0);
     const bool valid = i < N && !frozen;
     const uint32_t FULL = 0xffffffffu;
     if (frozen) {
@@ -1143,7 +1147,7 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
         // FIRE minimises the conservative part of the model: its own velocity mixing
         // and restarts replace the viscous contact damping, and the constant-torque
         // rolling resistance (a set-valued term at rest) is left out.
-        ep.dt = (float)sc->fdt;
+        ep.dt = (float)S->fdt;
         ep.p_A = 0.f;
         ep.mur = 0.f;
     }
@@ -1533,33 +1537,84 @@ __global__ void __launch_bounds__(128, MINB) k_step_ext(Dev d, Consts c) {
     } else {
         const uint32_t nb = __reduce_add_sync(FULL, nbroken);
         if ((threadIdx.x & 31) == 0 && nb) atomicAdd(&sc->broken, (unsigned long long)nb);
-        fire_force_finish<KIND>(d, c, acc);
+        fire_force_finish<KIND>(d, c, acc, sI - sA);
     }
 }
 
-// Block sums of the FIRE accumulators (fixed tree); the last block adds the block
-// partials in block order and makes the FIRE decision (Bitzek et al. 2006), in FP64:
-//   residual = sqrt(sum |F_i|^2 / N) / (mean normal pair force); converged when <= tol;
+// The FIRE decision of one specimen from its sums tot (FP64; n its particle count), by
+// the last CTA's thread 0 (Bitzek et al. 2006):
+//   residual = sqrt(sum |F_i|^2 / n) / (mean normal pair force); converged when <= tol;
 //   P = F.v + M.w > 0: mixing v <- (1-a) v + a (|v|/|F|) F (same for w with M), and after
 //   n_delay such steps dt <- min(dt f_inc, dt_max), a <- a f_alpha;
 //   P <= 0: dt <- max(dt f_dec, dt_min), a <- a0, v = w = 0.
+__device__ __forceinline__ void fire_decide(DevScalars* S, const Consts& c, const double* tot, uint32_t n) {
+    const double P = tot[0], FF = tot[1], VV = tot[2], MM = tot[3], WW = tot[4], FN = tot[5], NP = tot[6];
+    const double mean = NP > 0.0 ? FN / NP : 0.0;
+    const double rms = sqrt(FF / (double)n);
+    S->fmean = mean;
+    S->fresidual = mean > 0.0 ? rms / mean : (FF > 0.0 ? 1e300 : 0.0);
+    S->fpower = P;
+    // platen stress of this configuration (SumForcesULoading's formula)
+    const double a1 = (double)S->_1d_Area;
+    S->Stress = 0.5 * (fabs(tot[7]) + fabs(tot[8])) * a1;
+    S->fiter += 1;
+    S->fiter_total += 1;
+    if (S->fresidual <= S->ftol) { S->fconverged = 1; S->fstop = 1; return; }
+    if (S->fiter >= S->fmax_iter) { S->fstop = 1; return; }
+    if (S->fwarm) {
+        // first pass of an increment: the velocities only carried the start motion into
+        // the state; the dynamics starts from rest
+        S->fwarm = 0;
+        S->fuphill = 1;
+        S->fnpos = 0;
+        S->fcv = 0.0; S->fcf = 0.0; S->fcm = 0.0;
+    } else if (P > 0.0) {
+        const double a = S->falpha;
+        S->fcv = 1.0 - a;
+        S->fcf = FF > 0.0 ? a * sqrt(VV / FF) : 0.0;
+        S->fcm = MM > 0.0 ? a * sqrt(WW / MM) : 0.0;
+        S->fuphill = 0;
+        S->fnpos += 1;
+        if (S->fnpos > S->fndelay) {
+            S->fdt = fmin(S->fdt * S->finc, S->fdtmax);
+            S->falpha = a * S->fshrink;
+        }
+    } else {
+        S->fnpos = 0;
+        S->fdt = fmax(S->fdt * S->fdec, S->fdtmin);
+        S->falpha = S->falpha0;
+        S->fuphill = 1;
+        S->fcv = 0.0; S->fcf = 0.0; S->fcm = 0.0;
+    }
+}
+
+// Block sums of the FIRE accumulators (fixed tree, per specimen); the last block adds
+// each specimen's block partials in block order and makes its FIRE decision.
 template <int KIND>
-__device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c, double (&acc)[FIRE_SUMS]) {
+__device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c, double (&acc)[FIRE_SUMS],
+                                                  uint32_t second) {
     DevScalars* sc = d.sc;
     const uint32_t FULL = 0xffffffffu;
-    __shared__ double s_acc[4][FIRE_SUMS];
+    __shared__ double s_acc[4][FIRE_SUMS], s_acc2[4][FIRE_SUMS];
     __shared__ bool s_last;
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    // a CTA touches at most two specimens: its sums are kept apart per specimen
 #pragma unroll
     for (int q = 0; q < FIRE_SUMS; ++q) {
-        double v = acc[q];
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-        if (l == 0) s_acc[w][q] = v;
+        double v = second ? 0.0 : acc[q], v2 = second ? acc[q] : 0.0;
+        for (int o = 16; o; o >>= 1) {
+            v += __shfl_xor_sync(FULL, v, o);
+            v2 += __shfl_xor_sync(FULL, v2, o);
+        }
+        if (l == 0) { s_acc[w][q] = v; s_acc2[w][q] = v2; }
     }
     __syncthreads();
     if (threadIdx.x < FIRE_SUMS) {
         const int q = threadIdx.x;
         d.fpart[(size_t)blockIdx.x * FIRE_SUMS + q] = (s_acc[0][q] + s_acc[1][q]) + (s_acc[2][q] + s_acc[3][q]);
+        if (d.fpart2)
+            d.fpart2[(size_t)blockIdx.x * FIRE_SUMS + q] =
+                (s_acc2[0][q] + s_acc2[1][q]) + (s_acc2[2][q] + s_acc2[3][q]);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1569,54 +1624,32 @@ __device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c,
     __syncthreads();
     if (!s_last) return;
     __threadfence();
+    // the last CTA: per specimen still relaxing, its sums over its CTAs in CTA order, then
+    // its FIRE decision
     __shared__ double tot[FIRE_SUMS];
-    if (threadIdx.x < FIRE_SUMS) {
-        double v = 0.0;
-        for (uint32_t b = 0; b < gridDim.x; ++b) v += __ldcg(&d.fpart[(size_t)b * FIRE_SUMS + threadIdx.x]);
-        tot[threadIdx.x] = v;
+    bool all_stopped = true;
+    for (uint32_t sp = 0; sp < d.nspec; ++sp) {
+        DevScalars* S = d.spec + sp;
+        if (S->fstop) continue;                               // uniform across the CTA
+        const SpecGeom& G = d.geom[sp];
+        if (threadIdx.x < FIRE_SUMS) {
+            double v = 0.0;
+#pragma unroll 8
+            for (uint32_t b = G.b0; b <= G.b1; ++b) {
+                const double* src = (d.blk_spec == nullptr || d.blk_spec[b] == sp) ? d.fpart : d.fpart2;
+                v += __ldcg(&src[(size_t)b * FIRE_SUMS + threadIdx.x]);
+            }
+            tot[threadIdx.x] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) fire_decide(S, c, tot, G.p1 - G.p0);
+        __syncthreads();
+        if (!S->fstop) all_stopped = false;
     }
-    __syncthreads();
     if (threadIdx.x != 0) return;
     sc->fcounter = 0;
-    const double P = tot[0], FF = tot[1], VV = tot[2], MM = tot[3], WW = tot[4], FN = tot[5], NP = tot[6];
-    const double mean = NP > 0.0 ? FN / NP : 0.0;
-    const double rms = sqrt(FF / (double)c.N);
-    sc->fmean = mean;
-    sc->fresidual = mean > 0.0 ? rms / mean : (FF > 0.0 ? 1e300 : 0.0);
-    sc->fpower = P;
-    // platen stress of this configuration (SumForcesULoading's formula)
-    const double a1 = (double)sc->_1d_Area;
-    sc->Stress = 0.5 * (fabs(tot[7]) + fabs(tot[8])) * a1;
-    sc->fiter += 1;
-    sc->fiter_total += 1;
     sc->steps += 1;                     // buffer parity: the update works on what this pass wrote
-    if (sc->fresidual <= sc->ftol) { sc->fconverged = 1; sc->fstop = 1; return; }
-    if (sc->fiter >= sc->fmax_iter) { sc->fstop = 1; return; }
-    if (sc->fwarm) {
-        // first pass of an increment: the velocities only carried the start motion into
-        // the state; the dynamics starts from rest
-        sc->fwarm = 0;
-        sc->fuphill = 1;
-        sc->fnpos = 0;
-        sc->fcv = 0.0; sc->fcf = 0.0; sc->fcm = 0.0;
-    } else if (P > 0.0) {
-        const double a = sc->falpha;
-        sc->fcv = 1.0 - a;
-        sc->fcf = FF > 0.0 ? a * sqrt(VV / FF) : 0.0;
-        sc->fcm = MM > 0.0 ? a * sqrt(WW / MM) : 0.0;
-        sc->fuphill = 0;
-        sc->fnpos += 1;
-        if (sc->fnpos > sc->fndelay) {
-            sc->fdt = fmin(sc->fdt * sc->finc, sc->fdtmax);
-            sc->falpha = a * sc->fshrink;
-        }
-    } else {
-        sc->fnpos = 0;
-        sc->fdt = fmax(sc->fdt * sc->fdec, sc->fdtmin);
-        sc->falpha = sc->falpha0;
-        sc->fuphill = 1;
-        sc->fcv = 0.0; sc->fcf = 0.0; sc->fcm = 0.0;
-    }
+    if (d.nspec > 1) sc->fstop = all_stopped ? 1u : 0u;      // (with one specimen sc == spec)
 }
 
 // FIRE update of one iteration, in place on the buffers the force pass wrote:
@@ -1627,21 +1660,25 @@ __global__ void k_fire_update(Dev d, Consts c) {
     const uint32_t cur = (uint32_t)(sc->steps & 1ull);
     const bool stop = sc->fstop != 0;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    // the particle's specimen (a batch's specimens relax on their own FIRE scalars; one
+    // whose relaxation stopped stays where it is)
+    const uint32_t sA = d.blk_spec ? (uint32_t)d.blk_spec[blockIdx.x] : 0u;
+    const DevScalars* S = d.spec + ((i < c.N && i >= d.geom[sA].p1) ? sA + 1u : sA);
     uint32_t moved = 0;
     float e2max = 0.f;
-    if (!stop && i < c.N) {
+    if (!stop && i < c.N && !S->fstop) {
         double4 x = d.posd[cur][i];
         float4 v = d.vel[cur][i], w = d.ang[cur][i];
         const float4 F = d.frc[i], M = d.mom[i];
-        const float dt = (float)sc->fdt;
+        const float dt = (float)S->fdt;
         const double dtd = (double)dt;
-        if (sc->fuphill) {
+        if (S->fuphill) {
             // stop (no half step back: the bond and contact state integrates v dt, so every
             // position change must be a v dt of the force pass that follows)
             v = make_float4(0.f, 0.f, 0.f, 0.f);
             w = v;
         } else {
-            const float cv = (float)sc->fcv, cf = (float)sc->fcf, cm = (float)sc->fcm;
+            const float cv = (float)S->fcv, cf = (float)S->fcf, cm = (float)S->fcm;
             v.x = cv * v.x + cf * F.x; v.y = cv * v.y + cf * F.y; v.z = cv * v.z + cf * F.z;
             w.x = cv * w.x + cm * M.x; w.y = cv * w.y + cm * M.y; w.z = cv * w.z + cm * M.z;
         }
@@ -1700,25 +1737,33 @@ __global__ void k_fire_update(Dev d, Consts c) {
 // initial angular velocity (so the first iteration's bond and contact state advance
 // by that rotation).
 template <int KIND>
-__global__ void k_qs_begin_scalars(Dev d, Consts c, double delta) {
-    DevScalars* sc = d.sc;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
-        sc->V = 0.0;
-        sc->size_d[ax] -= delta;
-        sc->Top -= delta;
-        sc->TopR = sc->Top - 2.0 * c.p_r_d;
-        sc->size[ax] = (float)sc->size_d[ax];
-        sc->sized2[ax] = (float)(0.5 * sc->size_d[ax]);
-        sc->center_d[ax] -= delta;
-        sc->center[ax] = (float)sc->center_d[ax];
-        sc->Hd2 = sc->sized2[ax];
-        sc->Strain = (sc->size_d[ax] - sc->Size0) / sc->Size0;
-        sc->fdt = sc->fdt0;
-        sc->falpha = sc->falpha0;
-        sc->fnpos = 0; sc->fiter = 0; sc->fuphill = 0; sc->fconverged = 0; sc->fstop = 0; sc->fcounter = 0;
-        sc->fcv = 1.0; sc->fcf = 0.0; sc->fcm = 0.0;
-        sc->fwarm = 1;
+__global__ void k_qs_begin_scalars(Dev d, Consts c, double sinc) {
+    const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
+    for (uint32_t sp = threadIdx.x; sp < d.nspec; sp += blockDim.x) {
+        DevScalars* S = d.spec + sp;
+        const double delta = sinc * S->Size0;      // the specimen's platen advance
+        S->V = 0.0;
+        S->size_d[ax] -= delta;
+        S->Top -= delta;
+        S->TopR = S->Top - 2.0 * c.p_r_d;
+        S->size[ax] = (float)S->size_d[ax];
+        S->sized2[ax] = (float)(0.5 * S->size_d[ax]);
+        S->center_d[ax] -= delta;
+        S->center[ax] = (float)S->center_d[ax];
+        S->Hd2 = S->sized2[ax];
+        S->Strain = (S->size_d[ax] - S->Size0) / S->Size0;
+        S->fdt = S->fdt0;
+        S->falpha = S->falpha0;
+        S->fnpos = 0; S->fiter = 0; S->fuphill = 0; S->fconverged = 0; S->fstop = 0;
+        S->fcv = 1.0; S->fcf = 0.0; S->fcm = 0.0;
+        S->fwarm = 1;
+        S->done = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DevScalars* sc = d.sc;     // (with one specimen sc == spec)
+        sc->fstop = 0;
+        sc->fcounter = 0;
         sc->done = 0;
         sc->dmax = 3.0e38f;        // the increment moves particles (platen, warm start): the first pass scans
         sc->d2max_next = 0;
@@ -1726,15 +1771,22 @@ __global__ void k_qs_begin_scalars(Dev d, Consts c, double delta) {
     }
 }
 template <int KIND>
-__global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int ldw, int scaled, double D) {
-    DevScalars* sc = d.sc;
+__global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int ldw, int scaled, double sinc) {
+    const DevScalars* sc = d.sc;
     const uint32_t cur = (uint32_t)(sc->steps & 1ull);
-    const float idt0 = (float)(1.0 / sc->fdt0);
-    const double Top = sc->Top, Bottom = sc->Bottom, TopR = sc->TopR, BottomR = sc->BottomR;
-    const float RR = sc->RR;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;      // one particle per thread, 128-thread CTAs
+    if (i >= c.N) return;
+    const uint32_t sA = d.blk_spec ? (uint32_t)d.blk_spec[blockIdx.x] : 0u;
+    const uint32_t sI = i >= d.geom[sA].p1 ? sA + 1u : sA;
+    const DevScalars* S = d.spec + sI;
+    const double zcut = (double)d.geom[sI].zcut;
+    const float idt0 = (float)(1.0 / S->fdt0);
+    const double D = sinc * S->Size0;                          // the specimen's platen advance
+    const double Top = S->Top, Bottom = S->Bottom, TopR = S->TopR, BottomR = S->BottomR;
+    const float RR = S->RR;
     rf_float3 cc;
-    cc.x = sc->center[0]; cc.y = sc->center[1]; cc.z = sc->center[2];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+    cc.x = S->center[0]; cc.y = S->center[1]; cc.z = S->center[2];
+    {
         double4 x = d.posd[cur][i];
         d.x0[i] = x;
         float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1758,7 +1810,7 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int 
             const double a0 = KIND == RF_TEST_BRAZIL ? x.y : x.z;
             const float q0 = (float)(x.x - cc.x), q1 = KIND == RF_TEST_BRAZIL ? (float)(x.z - cc.z) : (float)(x.y - cc.y);
             const bool zone = q0 * q0 + q1 * q1 < RR && (KIND == RF_TEST_BRAZIL ? (double)(float)(x.z - cc.z) : a0) <
-                                                          (double)c.zcut;
+                                                          zcut;
             const bool at_top = zone && a0 + off - (Top + D) > -1e-9;
             const bool at_bottom = zone && a0 - off - Bottom < 1e-9;
             x.x += (double)u[0]; x.y += (double)u[1]; x.z += (double)u[2];
@@ -1775,10 +1827,10 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int 
         double sb = 0.0, st = 0.0;
         if (KIND == RF_TEST_BRAZIL)
             brazil_particle_ext(x.x, x.y, x.z, v0, v1, v2, f0, f1, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f,
-                                (double)c.zcut, x.w - c.p_r_d, sb, st, false);
+                                zcut, x.w - c.p_r_d, sb, st, false);
         else
             uniaxial_particle_ext(x.x, x.y, x.z, v0, v1, v2, f0, f1, f2, cc, RR, Top, Bottom, TopR, BottomR, 0.f,
-                                  (double)c.zcut, x.w - c.p_r_d, sb, st, false);
+                                  zcut, x.w - c.p_r_d, sb, st, false);
         d.posd[cur][i] = x;
         d.vel[cur][i] = make_float4(v0, v1, v2, 0.f);
         d.ang[cur][i] = w;
@@ -1786,14 +1838,21 @@ __global__ void k_qs_begin(Dev d, Consts c, const float* __restrict__ warm, int 
     }
 }
 
+// The specimen of particle i in a kernel of 128-thread CTAs, one particle per thread.
+__device__ __forceinline__ const DevScalars* spec_of(const Dev& d, uint32_t i) {
+    const uint32_t sA = d.blk_spec ? (uint32_t)d.blk_spec[blockIdx.x] : 0u;
+    return d.spec + (i >= d.geom[sA].p1 ? sA + 1u : sA);
+}
+
 // Warm-start features of each particle from the last increment's motion (layout in the
-// header); D = strain_inc * initial size, sinc = strain_inc.
+// header); sinc = strain_inc, D = sinc * the specimen's initial size (its platen advance).
 template <int KIND>
-__global__ void k_warm_features(Dev d, Consts c, double D, double sinc, __nv_bfloat16* __restrict__ feat) {
-    const DevScalars* sc = d.sc;
-    const uint32_t cur = (uint32_t)(sc->steps & 1ull);
+__global__ void k_warm_features(Dev d, Consts c, double sinc, __nv_bfloat16* __restrict__ feat) {
+    const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
+    const DevScalars* sc = spec_of(d, i);
+    const double D = sinc * sc->Size0;
     const int ax = (KIND == RF_TEST_BRAZIL) ? 1 : 2;
     const double iD = 1.0 / D;
     const double4 x = d.posd[cur][i], x0 = d.x0[i], r = d.rot[i];
@@ -1843,10 +1902,11 @@ __global__ void k_warm_features(Dev d, Consts c, double D, double sinc, __nv_bfl
 }
 
 // Targets of the last increment: displacement / D and rotation * r / D.
-__global__ void k_warm_targets(Dev d, Consts c, double D, float* __restrict__ t) {
+__global__ void k_warm_targets(Dev d, Consts c, double sinc, float* __restrict__ t) {
     const uint32_t cur = (uint32_t)(d.sc->steps & 1ull);
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
+    const double D = sinc * spec_of(d, i)->Size0;
     const double iD = 1.0 / D;
     const double4 x = d.posd[cur][i], x0 = d.x0[i], r = d.rot[i];
     float* o = t + (size_t)i * 6;
@@ -3014,6 +3074,7 @@ rf_status fire_setup(rf_engine* e) {
     rf_status st;
     if ((st = dalloc(e, &d.frc, N)) || (st = dalloc(e, &d.mom, N)) ||
         (st = dalloc(e, &d.fpart, (size_t)e->nblocks * FIRE_SUMS)) || (st = dalloc(e, &d.rot, N)) ||
+        (d.nspec > 1 && (st = dalloc(e, &d.fpart2, (size_t)e->nblocks * FIRE_SUMS))) ||
         (st = dalloc(e, &d.x0, N)) || (st = dalloc(e, &d.bst0, 3 * (size_t)d.QB * N)))
         return st;
     e->cf = e->c;
@@ -3028,52 +3089,62 @@ rf_status fire_setup(rf_engine* e) {
     return RF_OK;
 }
 
+// One quasi-static load increment of every specimen of the engine (a batch relaxes its
+// specimens together, each on its own FIRE scalars, and a specimen whose relaxation
+// stopped stays put until the others stop). r: one result per specimen.
 rf_status load_increment(rf_engine* e, const rf_relax_params* p, const float* warm, int ldw, int scaled,
                          rf_relax_result* r) {
     if (!e || !p) { set_error("rf_engine_load_increment: bad arguments"); return RF_ERR_INVALID; }
     if (!e->c.ext) { set_error("rf_engine_load_increment: quasi-static relaxation needs the extended model"); return RF_ERR_STATE; }
-    if (e->d.nspec > 1) { set_error("rf_engine_load_increment: quasi-static relaxation runs one specimen per engine"); return RF_ERR_STATE; }
     if (e->c.ref_mode) { set_error("rf_engine_load_increment: the reference-constants mode runs explicit steps only"); return RF_ERR_STATE; }
     if (!(p->dt0 > 0) || !(p->dt_max >= p->dt0) || !(p->dt_min > 0) || !(p->dt_min <= p->dt0) || !(p->tol > 0) ||
-        p->max_iter == 0 || !(p->alpha0 >= 0 && p->alpha0 < 1) || !(p->f_inc >= 1) || !(p->f_dec > 0 && p->f_dec < 1)) {
+        p->max_iter == 0 || !(p->alpha0 >= 0 && p->alpha0 < 1) || !(p->f_inc >= 1) || !(p->f_dec > 0 && p->f_dec < 1) ||
+        !(p->strain_inc > 0)) {
         set_error("rf_engine_load_increment: bad FIRE parameters");
         return RF_ERR_INVALID;
     }
     cudaStream_t s = e->stream;
     Dev& d = e->d;
-    const uint32_t N = e->c.N;
+    const uint32_t N = e->c.N, ns = d.nspec;
     if (rf_status st = fire_setup(e)) return st;
-    // FIRE constants into the scalar block (host read-modify-write, stream ordered)
-    DevScalars h;
-    RF_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    // FIRE constants into every specimen's scalar block (host read-modify-write, stream ordered)
+    std::vector<DevScalars> hs(ns);
+    RF_CUDA(cudaMemcpyAsync(hs.data(), d.spec, ns * sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
     RF_CUDA(cudaStreamSynchronize(s));
-    h.fdt0 = p->dt0; h.fdtmax = p->dt_max; h.fdtmin = p->dt_min; h.falpha0 = p->alpha0; h.finc = p->f_inc;
-    h.fdec = p->f_dec; h.fshrink = p->f_alpha; h.fndelay = p->n_delay; h.ftol = p->tol; h.fmax_iter = p->max_iter;
-    RF_CUDA(cudaMemcpyAsync(d.sc, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-    const double delta = p->strain_inc * h.Size0;
+    for (DevScalars& h : hs) {
+        h.fdt0 = p->dt0; h.fdtmax = p->dt_max; h.fdtmin = p->dt_min; h.falpha0 = p->alpha0; h.finc = p->f_inc;
+        h.fdec = p->f_dec; h.fshrink = p->f_alpha; h.fndelay = p->n_delay; h.ftol = p->tol; h.fmax_iter = p->max_iter;
+    }
+    RF_CUDA(cudaMemcpyAsync(d.spec, hs.data(), ns * sizeof(DevScalars), cudaMemcpyHostToDevice, s));
     // the bond records' state at the start of the increment (FIRE mode computes from it)
     RF_CUDA(cudaMemcpyAsync(d.bst0, d.bst, 3 * (size_t)d.QB * N * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+    const unsigned nb = (N + 127) / 128;
     if (e->task.kind == RF_TEST_BRAZIL) {
-        k_qs_begin_scalars<RF_TEST_BRAZIL><<<1, 32, 0, s>>>(d, e->cf, delta);
-        k_qs_begin<RF_TEST_BRAZIL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm, ldw, scaled, delta);
+        k_qs_begin_scalars<RF_TEST_BRAZIL><<<1, 32, 0, s>>>(d, e->cf, p->strain_inc);
+        k_qs_begin<RF_TEST_BRAZIL><<<nb, 128, 0, s>>>(d, e->cf, warm, ldw, scaled, p->strain_inc);
     } else {
-        k_qs_begin_scalars<RF_TEST_UNIAXIAL><<<1, 32, 0, s>>>(d, e->cf, delta);
-        k_qs_begin<RF_TEST_UNIAXIAL><<<(N + 255) / 256, 256, 0, s>>>(d, e->cf, warm, ldw, scaled, delta);
+        k_qs_begin_scalars<RF_TEST_UNIAXIAL><<<1, 32, 0, s>>>(d, e->cf, p->strain_inc);
+        k_qs_begin<RF_TEST_UNIAXIAL><<<nb, 128, 0, s>>>(d, e->cf, warm, ldw, scaled, p->strain_inc);
     }
     RF_CHECK_LAUNCH("k_qs_begin");
     if (e->cf.use_graph) RF_CUDA(cudaGraphLaunch(e->fexec, s));
     else if (rf_status st = launch_stream_fire(e, p->max_iter)) return st;
-    RF_CUDA(cudaMemcpyAsync(&h, d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    DevScalars g;
+    RF_CUDA(cudaMemcpyAsync(hs.data(), d.spec, ns * sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
+    RF_CUDA(cudaMemcpyAsync(&g, d.sc, sizeof(g), cudaMemcpyDeviceToHost, s));
     RF_CUDA(cudaStreamSynchronize(s));
     if (r) {
-        r->iterations = h.fiter;
-        r->converged = (int32_t)h.fconverged;
-        r->residual = h.fresidual;
-        r->mean_force = h.fmean;
-        r->stress = h.Stress;
-        r->strain = h.Strain;
-        r->broken_bonds = h.broken;
-        r->error = (rf_status)h.err;
+        for (uint32_t k = 0; k < ns; ++k) {
+            const DevScalars& h = hs[k];
+            r[k].iterations = h.fiter;
+            r[k].converged = (int32_t)h.fconverged;
+            r[k].residual = h.fresidual;
+            r[k].mean_force = h.fmean;
+            r[k].stress = h.Stress;
+            r[k].strain = h.Strain;
+            r[k].broken_bonds = g.broken;         // (the engine's total)
+            r[k].error = (rf_status)g.err;
+        }
     }
     return RF_OK;
 }
@@ -3083,30 +3154,34 @@ rf_status load_increment(rf_engine* e, const rf_relax_params* p, const float* wa
 extern "C" {
 
 rf_status rf_engine_load_increment(rf_engine* e, const rf_relax_params* p, const float* warm, rf_relax_result* r) {
+    if (e && e->d.nspec > 1) { set_error("rf_engine_load_increment: a batch takes rf_engine_load_increment_batch"); return RF_ERR_STATE; }
     return load_increment(e, p, warm, 6, 0, r);
+}
+
+rf_status rf_engine_load_increment_batch(rf_engine* e, const rf_relax_params* p, const float* warm, int ldw,
+                                         int scaled, rf_relax_result* results) {
+    if (warm && ldw < 6) { set_error("rf_engine_load_increment_batch: bad warm-start buffer"); return RF_ERR_INVALID; }
+    return load_increment(e, p, warm, ldw, scaled ? 1 : 0, results);
 }
 
 rf_status rf_engine_load_increment_pred(rf_engine* e, const rf_relax_params* p, const float* pred, int ldp,
                                         rf_relax_result* r) {
     if (!pred || ldp < 6) { set_error("rf_engine_load_increment_pred: bad prediction buffer"); return RF_ERR_INVALID; }
+    if (e && e->d.nspec > 1) { set_error("rf_engine_load_increment_pred: a batch takes rf_engine_load_increment_batch"); return RF_ERR_STATE; }
     return load_increment(e, p, pred, ldp, 1, r);
 }
 
 rf_status rf_engine_warm_features(rf_engine* e, double strain_inc, void* feat) {
     if (!e || !feat || !(strain_inc > 0)) { set_error("rf_engine_warm_features: bad arguments"); return RF_ERR_INVALID; }
-    if (!e->c.ext || e->d.nspec > 1) { set_error("rf_engine_warm_features: needs a one-specimen extended-model engine"); return RF_ERR_STATE; }
+    if (!e->c.ext) { set_error("rf_engine_warm_features: needs an extended-model engine"); return RF_ERR_STATE; }
     if (rf_status st = fire_setup(e)) return st;
     const uint32_t N = e->c.N, rows = (N + 127) / 128 * 128;
     cudaStream_t s = e->stream;
-    DevScalars h;
-    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
-    RF_CUDA(cudaStreamSynchronize(s));
-    const double D = strain_inc * h.Size0;
     if (rows > N) RF_CUDA(cudaMemsetAsync((__nv_bfloat16*)feat + (size_t)N * 64, 0, (size_t)(rows - N) * 64 * 2, s));
     if (e->task.kind == RF_TEST_BRAZIL)
-        k_warm_features<RF_TEST_BRAZIL><<<(N + 127) / 128, 128, 0, s>>>(e->d, e->cf, D, strain_inc, (__nv_bfloat16*)feat);
+        k_warm_features<RF_TEST_BRAZIL><<<(N + 127) / 128, 128, 0, s>>>(e->d, e->cf, strain_inc, (__nv_bfloat16*)feat);
     else
-        k_warm_features<RF_TEST_UNIAXIAL><<<(N + 127) / 128, 128, 0, s>>>(e->d, e->cf, D, strain_inc, (__nv_bfloat16*)feat);
+        k_warm_features<RF_TEST_UNIAXIAL><<<(N + 127) / 128, 128, 0, s>>>(e->d, e->cf, strain_inc, (__nv_bfloat16*)feat);
     RF_CHECK_LAUNCH("k_warm_features");
     return RF_OK;
 }
@@ -3115,10 +3190,7 @@ rf_status rf_engine_warm_targets(rf_engine* e, double strain_inc, float* targets
     if (!e || !targets || !(strain_inc > 0)) { set_error("rf_engine_warm_targets: bad arguments"); return RF_ERR_INVALID; }
     if (!e->fire_ready) { set_error("rf_engine_warm_targets: no load increment run yet"); return RF_ERR_STATE; }
     cudaStream_t s = e->stream;
-    DevScalars h;
-    RF_CUDA(cudaMemcpyAsync(&h, e->d.sc, sizeof(h), cudaMemcpyDeviceToHost, s));
-    RF_CUDA(cudaStreamSynchronize(s));
-    k_warm_targets<<<(e->c.N + 127) / 128, 128, 0, s>>>(e->d, e->cf, strain_inc * h.Size0, targets);
+    k_warm_targets<<<(e->c.N + 127) / 128, 128, 0, s>>>(e->d, e->cf, strain_inc, targets);
     RF_CHECK_LAUNCH("k_warm_targets");
     return RF_OK;
 }

@@ -202,6 +202,7 @@ _proto = {
     "rf_engine_warm_features": (i32, [P, f64, P]),
     "rf_engine_warm_targets": (i32, [P, f64, P]),
     "rf_engine_load_increment_pred": (i32, [P, C.POINTER(RelaxParams), P, i32, C.POINTER(RelaxResult)]),
+    "rf_engine_load_increment_batch": (i32, [P, C.POINTER(RelaxParams), P, i32, i32, C.POINTER(RelaxResult)]),
     "rf_specimen_lattice_cylinder": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
     "rf_specimen_lattice_disc": (i32, [u64, f64, f64, f64, f64, f64, P, P, u64, P]),
 }
@@ -617,6 +618,18 @@ class BatchEngine(Engine):
         self.N = int(sum(t.N for t in tasks))
         self.K = int(tasks[0].K)
         self.task = tasks[0]
+
+    def load_increment(self, params, warm=None, ldw=6, scaled=False):
+        """One quasi-static load increment of every specimen (rf_engine_load_increment_batch);
+        warm: device tensor float32 [N, ldw] or None. Returns one RelaxResult per specimen."""
+        rs = (RelaxResult * self.nspec)()
+        check(lib.rf_engine_load_increment_batch(self.h, C.byref(params), ptr(warm), ldw, 1 if scaled else 0, rs),
+              "rf_engine_load_increment_batch")
+        return list(rs)
+
+    def load_increment_pred(self, params, pred, ldp=16):
+        """A load increment of every specimen from a WarmStart prediction [rows, ldp]."""
+        return self.load_increment(params, pred, ldp, scaled=True)
 
     def spec_info(self, s):
         first, count, off = C.c_uint64(0), C.c_uint64(0), C.c_double(0)

@@ -132,3 +132,40 @@ def test_sharded_run_matches_the_batch(cuda):
         assert [float(getattr(r, f)) for f in RESULT_FIELDS] == table[q].tolist()
     e.close()
     assert table[1][0] < 200 and table[0][0] == table[2][0] == 200
+
+
+def test_fire_batch_matches_single_specimens(cuda):
+    """Quasi-static load increments of a batch (rf_engine_load_increment_batch): every
+    specimen relaxes on its own FIRE scalars and ends each increment where its run alone
+    ends (a one-specimen engine on the same placed specimen), up to the order of the FP64
+    sums: a batch groups a specimen's particles into CTAs differently."""
+    specs = _specimens()
+    e = rfdem.BatchEngine([s[0] for s in specs], [s[3] for s in specs], [s[1] for s in specs], [s[2] for s in specs])
+    p = e.relax_params(max_iter=40000, strain_inc=1e-4)
+    n = 4
+    res = [e.load_increment(p) for _ in range(n)]
+    Rall = e.positions_f64()
+    iters = [[r.iterations for r in rk] for rk in res]
+    print("batch iterations per increment and specimen:", iters)
+    assert len({tuple(row) for row in zip(*iters)}) > 1 or n == 1   # the specimens stop at their own counts
+    for q, (t, R, rad, x) in enumerate(specs):
+        first, m, off, tq = e.spec_info(q)
+        Rq = R.reshape(3, m).copy()
+        Rq[0] += off
+        Rq = Rq.reshape(-1)
+        a = rfdem.Engine(mc.clone(tq), Rq, ext=x, radius=rad)
+        ra = [a.load_increment(p) for _ in range(n)]
+        Ra = a.positions_f64()
+        a.close()
+        Re = Rall.reshape(3, e.N)[:, first:first + m].reshape(-1)
+        ext = float(np.ptp(Rq.reshape(3, m)[2]))
+        for k in range(n):
+            rb = res[k][q]
+            print("specimen %d increment %d: iterations batch %d alone %d, stress batch %.9e alone %.9e" %
+                  (q, k, rb.iterations, ra[k].iterations, rb.stress, ra[k].stress))
+            assert rb.error == 0 and rb.converged == 1 and ra[k].converged == 1
+            assert abs(rb.stress - ra[k].stress) <= 1e-6 * abs(ra[k].stress) + 1e-15
+            assert abs(rb.iterations - ra[k].iterations) <= 0.1 * ra[k].iterations + 5
+        assert ra[-1].stress > 0
+        assert np.max(np.abs(Re - Ra)) < 1e-7 * ext, (q, np.abs(Re - Ra).max())
+    e.close()

@@ -60,6 +60,7 @@ N_PARTICLES, RMIN, RMAX, RADII = 4000000, 0.5, 1.5, "log-uniform"
 LIST_GAP = 0.25                          # x r0
 PRESTRAIN = (0.2, 0.2, -0.03)            # lateral, lateral, axial
 FIRE_PARTICLES = 1000000                 # the quasi-static configuration (radii U[0.8, 1.2] x r0)
+FIRE_BATCH_SPECIMENS, FIRE_BATCH_INC = 8, 3   # quasi-static batch: specimens, timed increments
 FIRE_PRE, FIRE_COLLECT, FIRE_EVAL = 1, 2, 20
 SAMPLE_N = 65536                         # particles of the committed specimen sample
 SAMPLE_FILE = os.path.join(ROOT, "oracle", "data", "bench_sample_4m.npz")
@@ -325,6 +326,68 @@ def run_fire(rfdem, torch, seed, n_eval):
             "training_pairs": ws.pairs(), "training_loss": [losses[0], losses[-1]], "training_s": t_train,
             "warm_start_includes": "feature build + last-increment motion + MLP forward (tcgen05 BF16) + gate "
                                    "scoring per load step"}
+
+
+def run_fire_batch(rfdem, torch, seed):
+    """Quasi-static load steps of a batch: FIRE_BATCH_SPECIMENS uniaxial cylinders (particle
+    counts log-uniform in [50k, 200k], radii U[0.8, 1.2] x 0.25 mm, own seeds) relaxed
+    together (rf_engine_load_increment_batch, each specimen on its own FIRE scalars), plain
+    and warm-started by each particle's last-increment motion, against the same specimens
+    one engine each, one after the other. Wall time per load step of the whole set."""
+    from rfdem.warm import WarmStart
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(50000), np.log(200000), FIRE_BATCH_SPECIMENS)).astype(int)
+    tasks, params, Rs, rads = [], [], [], []
+    x = rfdem.ext_params_si()
+    x.list_gap = LIST_GAP * R0_MM
+    t0 = time.perf_counter()
+    for q in range(FIRE_BATCH_SPECIMENS):
+        t, R, rad, D, H = ext_specimen(rfdem, int(counts[q]), seed + q, "uniform", 0.8, 1.2)
+        tasks.append(t); params.append(x); Rs.append(R); rads.append(rad)
+    t_pack = time.perf_counter() - t0
+    ntot = int(sum(int(t.N) for t in tasks))
+    P = rfdem.BatchEngine(tasks, params, Rs, rads)          # plain
+    W = rfdem.BatchEngine(tasks, params, Rs, rads)          # warm-started
+    p = P.relax_params(max_iter=60000)
+    ws = WarmStart(ntot, p.strain_inc, seed=seed)
+    for E in (P, W):
+        E.load_increment(p)                                # one increment before: the warm start's base
+    plain, warm = [], []
+    for k in range(FIRE_BATCH_INC):
+        t0 = time.perf_counter()
+        rp = P.load_increment(p)
+        plain.append((time.perf_counter() - t0, [r.iterations for r in rp], min(r.converged for r in rp)))
+        t0 = time.perf_counter()
+        rw = W.load_increment_pred(p, ws.predict(W, use_mlp=False), 16)
+        warm.append((time.perf_counter() - t0, [r.iterations for r in rw], min(r.converged for r in rw)))
+    P.close(); W.close(); ws.close()
+    seq, seq_it, seq_conv = 0.0, [], 1
+    for q in range(FIRE_BATCH_SPECIMENS):
+        e = rfdem.Engine(rfdem.Task.from_buffer_copy(tasks[q]), Rs[q], ext=params[q], radius=rads[q])
+        e.load_increment(p)
+        its = []
+        for k in range(FIRE_BATCH_INC):
+            t0 = time.perf_counter()
+            r = e.load_increment(p)
+            seq += time.perf_counter() - t0
+            its.append(r.iterations)
+            seq_conv = min(seq_conv, r.converged)
+        seq_it.append(its)
+        e.close()
+    tb = sum(a[0] for a in plain) / FIRE_BATCH_INC
+    tw = sum(a[0] for a in warm) / FIRE_BATCH_INC
+    ts = seq / FIRE_BATCH_INC
+    return {"workload": "%d uniaxial cylinders, %d particles in all (%d to %d each, log-uniform), quasi-static load "
+                        "steps of strain %.1e, FIRE to RMS net force <= 1e-6 x mean normal pair force"
+                        % (FIRE_BATCH_SPECIMENS, ntot, int(counts.min()), int(counts.max()), p.strain_inc),
+            "evaluated_increments": FIRE_BATCH_INC, "packing_s": t_pack,
+            "wall_s_per_load_step_batched_plain": tb, "wall_s_per_load_step_batched_warm": tw,
+            "wall_s_per_load_step_one_engine_each": ts,
+            "speedup_batched_vs_one_engine_each": ts / tb, "speedup_batched_warm_vs_one_engine_each": ts / tw,
+            "iterations_batched_plain": [a[1] for a in plain], "iterations_batched_warm": [a[1] for a in warm],
+            "iterations_one_engine_each": seq_it,
+            "all_converged": int(min([a[2] for a in plain] + [a[2] for a in warm] + [seq_conv])),
+            "warm_start": "each particle's last-increment motion (WarmStart.predict(use_mlp=False))"}
 
 
 class Clocks:
@@ -670,6 +733,7 @@ def run_engine(args):
     fire = None
     if rank == 0 and ws == 1 and not args.no_fire:
         fire = run_fire(rfdem, torch, 0xB2000000 + 3000, args.fire_eval)
+        fire["batch"] = run_fire_batch(rfdem, torch, 0xB2000000 + 5000)
     if rank != 0:
         return
     out = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,

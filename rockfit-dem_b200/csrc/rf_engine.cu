@@ -1632,14 +1632,26 @@ __device__ __forceinline__ void fire_force_finish(const Dev& d, const Consts& c,
         DevScalars* S = d.spec + sp;
         if (S->fstop) continue;                               // uniform across the CTA
         const SpecGeom& G = d.geom[sp];
+        // fixed order: each thread a CTA-strided share of the blocks, then the warp trees,
+        // then the four warps
+        double v[FIRE_SUMS];
+#pragma unroll
+        for (int q = 0; q < FIRE_SUMS; ++q) v[q] = 0.0;
+        for (uint32_t b = G.b0 + threadIdx.x; b <= G.b1; b += blockDim.x) {
+            const double* src = (d.blk_spec == nullptr || d.blk_spec[b] == sp) ? d.fpart : d.fpart2;
+#pragma unroll
+            for (int q = 0; q < FIRE_SUMS; ++q) v[q] += __ldcg(&src[(size_t)b * FIRE_SUMS + q]);
+        }
+#pragma unroll
+        for (int q = 0; q < FIRE_SUMS; ++q) {
+            double x = v[q];
+            for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+            if (l == 0) s_acc[w][q] = x;
+        }
+        __syncthreads();
         if (threadIdx.x < FIRE_SUMS) {
-            double v = 0.0;
-#pragma unroll 8
-            for (uint32_t b = G.b0; b <= G.b1; ++b) {
-                const double* src = (d.blk_spec == nullptr || d.blk_spec[b] == sp) ? d.fpart : d.fpart2;
-                v += __ldcg(&src[(size_t)b * FIRE_SUMS + threadIdx.x]);
-            }
-            tot[threadIdx.x] = v;
+            const int q = threadIdx.x;
+            tot[q] = (s_acc[0][q] + s_acc[1][q]) + (s_acc[2][q] + s_acc[3][q]);
         }
         __syncthreads();
         if (threadIdx.x == 0) fire_decide(S, c, tot, G.p1 - G.p0);

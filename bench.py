@@ -328,6 +328,39 @@ def run_fire(rfdem, torch, seed, n_eval):
                                    "scoring per load step"}
 
 
+def run_fire_long(n_inc):
+    """A long quasi-static run of the FIRE specimen: one plain increment, then n_inc
+    increments warm-started by each particle's last-increment motion; per increment its
+    iterations, convergence, platen stress (MPa) and wall time."""
+    import torch
+    import rfdem
+    from rfdem.warm import WarmStart
+    seed = 0xB2000000 + 3000
+    t, R, rad, D, H = ext_specimen(rfdem, FIRE_PARTICLES, seed, "uniform", 0.8, 1.2)
+    x = rfdem.ext_params_si()
+    x.list_gap = LIST_GAP * R0_MM
+    e = rfdem.Engine(rfdem.Task.from_buffer_copy(t), R, ext=x, radius=rad)
+    p = e.relax_params(max_iter=60000)
+    ws = WarmStart(int(t.N), p.strain_inc, seed=seed)
+    r0 = e.load_increment(p)
+    rows = []
+    t_all = time.perf_counter()
+    for k in range(n_inc):
+        t0 = time.perf_counter()
+        r = e.load_increment_pred(p, ws.predict(e, use_mlp=False), 16)
+        rows.append((r.iterations, r.converged, r.stress * rfdem.STRESS * 1e-6, time.perf_counter() - t0))
+    wall = time.perf_counter() - t_all
+    e.close(); ws.close()
+    print(json.dumps({"record": "quasi-static run, last-increment warm start",
+                      "workload": "%d-particle cylinder (radii U[0.8,1.2] x 0.25 mm, D %.1f x H %.1f mm), %d increments "
+                                  "of strain %.1e after one plain increment (%d iterations)"
+                                  % (int(t.N), D, H, n_inc, p.strain_inc, r0.iterations),
+                      "increments": n_inc, "wall_s": wall, "wall_s_per_increment": wall / n_inc,
+                      "all_converged": int(min(a[1] for a in rows)),
+                      "iterations": [a[0] for a in rows], "stress_mpa": [round(a[2], 6) for a in rows],
+                      "iterations_total": sum(a[0] for a in rows)}))
+
+
 def run_fire_batch(rfdem, torch, seed):
     """Quasi-static load steps of a batch: FIRE_BATCH_SPECIMENS uniaxial cylinders (particle
     counts log-uniform in [50k, 200k], radii U[0.8, 1.2] x 0.25 mm, own seeds) relaxed
@@ -800,6 +833,9 @@ def main():
                     help="homogeneous pre-strain x y z applied before the warm-up (0 0 0: none)")
     ap.add_argument("--write-sample", default=None, help="write the specimen's sample block to this .npz")
     ap.add_argument("--fit", action="store_true", help="time one material-fitter step (12 runs to fracture)")
+    ap.add_argument("--fire-long", type=int, default=0,
+                    help="only this many quasi-static increments of the 1M FIRE specimen, warm-started by the "
+                         "last increment's motion; prints their iterations (a record run, not a bench line)")
     ap.add_argument("--batch-full", action="store_true",
                     help="run the 64-disc batch to every specimen's post-peak drop instead of the timed window")
     args = ap.parse_args()
@@ -812,6 +848,8 @@ def main():
     STEPS_PER_BENCH_STEP = max(1, args.explicit_steps)
     if args.impl == "reference":
         run_reference(args)
+    elif args.fire_long > 0:
+        run_fire_long(args.fire_long)
     else:
         run_engine(args)
 

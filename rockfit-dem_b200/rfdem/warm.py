@@ -5,7 +5,9 @@ applies it (rf_engine_load_increment_pred) and FIRE then relaxes to the same res
 tolerance as plain FIRE, so a prediction only changes how many iterations that takes.
 
 The base prediction is the last increment's motion, taken exactly (float) from the
-engine (rf_engine_warm_targets before the increment). The MLP (rf_mlp_*, tensor-core
+engine (rf_engine_warm_targets before the increment), with a particle's translation
+capped at base_cap platen advances (a particle that rearranged in the last increment
+is not thrown as far again). The MLP (rf_mlp_*, tensor-core
 BF16 forward and backward) learns the correction to it: training pairs are the
 per-particle features before a plain increment (rf_engine_warm_features) and the
 increment's relaxed motion less the last increment's. A correction is clamped
@@ -23,7 +25,7 @@ from . import MLP
 
 
 class WarmStart:
-    def __init__(self, n_particles, strain_inc, seed=0xB2000000, clamp=4.0, gate=0.8):
+    def __init__(self, n_particles, strain_inc, seed=0xB2000000, clamp=4.0, gate=0.8, base_cap=2.0):
         import torch
         self.torch = torch
         self.N = int(n_particles)
@@ -31,6 +33,7 @@ class WarmStart:
         self.strain_inc = float(strain_inc)
         self.clamp = float(clamp)
         self.gate = float(gate)
+        self.base_cap = float(base_cap)
         self.mlp = MLP(seed)
         self.mlp.set_residual(False)
         self.feat = torch.zeros(self.rows, 64, dtype=torch.bfloat16, device="cuda")
@@ -91,6 +94,11 @@ class WarmStart:
         rotations; 1759 plain). The engine and the MLP run on their own streams: each
         hand-over synchronises."""
         self.features(engine)
+        if self.base_cap > 0:
+            # a particle that rearranged in the last increment (moved further than base_cap
+            # platen advances) is not thrown that far again: its base motion is scaled down
+            n = self.L[:, :3].norm(dim=1, keepdim=True)
+            self.L[:, :3] *= self.torch.clamp(self.base_cap / self.torch.clamp(n, min=1e-30), max=1.0)
         use = self.use_mlp if use_mlp is None else bool(use_mlp)
         if use_mlp is False:
             self.corr = None                  # the base alone: no forward pass
